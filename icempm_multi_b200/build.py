@@ -1,0 +1,63 @@
+"""Build recipe for the in-tree native libraries.
+
+``build()`` compiles ``libicempm_b200.so`` (CUDA kernels for sm_100a + the
+C-ABI of ``include/icempm.h`` + the host-side C++ of ``csrc/``) into this
+package directory with nvcc, so the shared object travels with the source
+tree.  Run ``python -m icempm_multi_b200.build``.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libicempm_b200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CUDA_SOURCES = ["capi.cu", "instance.cu"]
+CXX_SOURCES = ["params.cpp", "scene.cpp"]
+
+
+def _sources():
+    return [os.path.join(CSRC, s) for s in CUDA_SOURCES + CXX_SOURCES]
+
+
+def _deps():
+    out = []
+    for d in (CSRC, os.path.join(ROOT, "include")):
+        for f in os.listdir(d):
+            if f.endswith((".cu", ".cuh", ".cpp", ".h", ".hpp")):
+                out.append(os.path.join(d, f))
+    return out
+
+
+def needs_build():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(f) > t for f in _deps())
+
+
+def build(verbose=False, force=False):
+    if not force and not needs_build():
+        return LIB
+    nvcc = os.environ.get("NVCC", "nvcc")
+    cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+           "-Xptxas", "-v" if verbose else "-O3",
+           "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp", *_sources(), "-lcudart"]
+    if verbose:
+        print(" ".join(cmd))
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose or r.returncode != 0:
+        sys.stdout.write(r.stdout)
+        sys.stderr.write(r.stderr)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed building libicempm_b200.so")
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose="-v" in sys.argv, force=True)
+    print(LIB)

@@ -1,0 +1,46 @@
+// instance.cuh -- device state of one simulation instance (one domain, one GPU).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/icempm.h"
+#include "mpm_math.cuh"
+
+struct icy_mpm {
+    int device = 0;
+    int precision = ICY_PRECISION_FP64;
+    icy_sim_params prm{};
+    cudaStream_t stream = nullptr, own_stream = nullptr;
+
+    // particles: 16 lines of `pitch` doubles (HSSOA line order)
+    unsigned capacity = 0, n = 0;
+    long pitch = 0;
+    double *d_pts = nullptr;
+
+    // grid: nodes gx in [-halo, GridX+halo), gy in [0, GridY), column gx+halo,
+    // five arrays of n_nodes doubles: m, px, py (accumulated), vx, vy (updated)
+    long n_nodes = 0;
+    double *d_grid = nullptr;
+
+    double *d_acc = nullptr;      // indenter force bins, 2*n_indenter_subdivisions
+    int *d_status = nullptr;      // device error code (reference codes 70..73, 5)
+    int *h_status = nullptr;      // pinned host mirror
+
+    int64_t launches = 0;
+};
+
+icy_dev::StepParams icy_step_params(const icy_sim_params &p);
+void icy_set_error(const char *where, cudaError_t e);
+void icy_set_error_msg(const std::string &m);
+
+int icy_instance_allocate(icy_mpm *h, unsigned capacity);
+void icy_instance_free(icy_mpm *h);
+int icy_instance_upload(icy_mpm *h, const double *hssoa, unsigned cap, unsigned size);
+int icy_instance_download(icy_mpm *h, double *hssoa, unsigned cap);
+int icy_phase_reset_grid(icy_mpm *h);
+int icy_phase_p2g(icy_mpm *h);
+int icy_phase_update(icy_mpm *h, double ind_x, double ind_y);
+int icy_phase_g2p(icy_mpm *h, bool recordPQ);
+int icy_instance_steps(icy_mpm *h, int step0, int nsteps, double *sim_time);

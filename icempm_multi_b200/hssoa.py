@@ -1,0 +1,106 @@
+"""Host-side particle SoA in the reference layout.
+
+Mirror of ``HostSideSOA`` (simulation/hssoa/host_side_soa.h:52-74): one buffer
+of 16 lines x ``capacity`` doubles, ``size`` points in use, line 0 holding the
+64-bit utility word bit-cast into a double.  The buffer can be page-locked
+(through torch, which is used here only as the pinned-memory allocator) so
+that uploads and downloads run at full PCIe/C2C speed.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (BP00, FE00, IDX_JP_INV, IDX_P, IDX_Q, N_PTS_ARRAYS, POSX, STATUS_CRUSHED, STATUS_DISABLED,
+                   STATUS_LIQUID, VELX, check, lib)
+
+
+class HostSideSOA:
+    def __init__(self, capacity, pinned=False):
+        self.capacity = int(capacity)
+        self.size = 0
+        self._keep = None
+        if pinned:
+            import torch
+            t = torch.zeros((N_PTS_ARRAYS, self.capacity), dtype=torch.float64).pin_memory()
+            self._keep = t
+            self.buf = t.numpy()
+        else:
+            self.buf = np.zeros((N_PTS_ARRAYS, self.capacity), dtype=np.float64)
+
+    # --- access -----------------------------------------------------------
+    @property
+    def ptr(self):
+        return self.buf.ctypes.data_as(C.c_void_p)
+
+    def line(self, k):
+        return self.buf[k, :self.size]
+
+    @property
+    def utility(self):
+        return self.buf[0, :self.size].view(np.int64)
+
+    @property
+    def pos(self):
+        return self.buf[POSX:POSX + 2, :self.size]
+
+    @property
+    def vel(self):
+        return self.buf[VELX:VELX + 2, :self.size]
+
+    @property
+    def Fe(self):
+        return self.buf[FE00:FE00 + 4, :self.size]
+
+    @property
+    def Bp(self):
+        return self.buf[BP00:BP00 + 4, :self.size]
+
+    @property
+    def Jp_inv(self):
+        return self.buf[IDX_JP_INV, :self.size]
+
+    @property
+    def PQ(self):
+        return self.buf[IDX_P:IDX_Q + 1, :self.size]
+
+    def crushed(self):
+        return (self.utility & STATUS_CRUSHED) != 0
+
+    def disabled(self):
+        return (self.utility & STATUS_DISABLED) != 0
+
+    def liquid(self):
+        return (self.utility & STATUS_LIQUID) != 0
+
+    def grains(self):
+        return (self.utility & 0xFFFF).astype(np.int64)
+
+    def copy_from(self, other):
+        n = other.size
+        assert n <= self.capacity
+        self.buf[:, :n] = other.buf[:, :n]
+        self.size = n
+        return self
+
+    def clone(self, pinned=False):
+        c = HostSideSOA(max(self.size, 1), pinned=pinned)
+        return c.copy_from(self)
+
+    def active_count(self):
+        """Non-disabled points (simulation/gpu_implementation5.cpp:399-405)."""
+        return int((~self.disabled()).sum())
+
+
+def make_block(params, block_w, block_h, ppc=4, seed=1, n_grains=0, extra_space=0.0, pinned=False):
+    """Seeded synthetic ice block placed as LoadRawPoints places a cloud
+    (simulation/snapshotmanager.cpp:29-121).  Updates ``params`` in place
+    (nPtsTotal, Volume, ParticleVolume, indenter start, derived constants)."""
+    n = lib().icy_scene_block_count(C.byref(params), block_w, block_h, ppc)
+    cap = int(n * (1 + extra_space)) if extra_space else int(n)
+    soa = HostSideSOA(max(cap, 1), pinned=pinned)
+    out_n = C.c_uint(0)
+    rc = lib().icy_scene_block(C.byref(params), block_w, block_h, ppc, seed, n_grains, soa.ptr, soa.capacity,
+                               C.byref(out_n))
+    check(rc, "icy_scene_block")
+    soa.size = out_n.value
+    return soa

@@ -1,0 +1,233 @@
+/*
+ * icempm.h -- C-ABI of the B200-native MLS-MPM step library (libicempm_b200.so).
+ *
+ * The library replaces the per-step hot path of iceMPM_multi run as ONE
+ * partition on ONE GPU: grid reset, P2G scatter, grid-node update with the
+ * rigid indenter, G2P gather fused with the Drucker-Prager return mapping.
+ * Every entry point returns an int status: 0 = OK, otherwise one of the
+ * ICY_ERR_* codes below.  No C++ exception crosses this boundary; the C++
+ * host layer (icempm_multi_b200/host) turns non-zero codes into
+ * std::runtime_error, as the reference does for every CUDA failure
+ * (simulation/gpu_partition.cu:19-20,151-156 and similar).
+ *
+ * Particle data uses the reference HSSOA layout: 16 lines of doubles, line
+ * stride = capacity (simulation/hssoa/host_side_soa.h:52-74), line order as
+ * in simulation/parameters_sim.h:27-35.  Line 0 holds the 64-bit utility word
+ * bit-cast into a double (grain id bits 0-15, crushed 0x10000, disabled
+ * 0x20000, liquid 0x40000; simulation/kernels.cuh:12-14).
+ */
+#ifndef ICEMPM_H
+#define ICEMPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* status codes                                                         */
+/* ------------------------------------------------------------------ */
+enum {
+    ICY_OK = 0,
+    /* device error byte values kept from the reference
+       (simulation/kernels.cuh:94-97 and :506) */
+    ICY_ERR_NO_SPACE = 5,          /* capacity exceeded                        */
+    ICY_ERR_OUT_OF_GRID_XLO = 70,  /* particle stencil left the grid: x < -halo */
+    ICY_ERR_OUT_OF_GRID_YLO = 71,  /* y < 0                                     */
+    ICY_ERR_OUT_OF_GRID_XHI = 72,  /* x > GridX + halo - 3                      */
+    ICY_ERR_OUT_OF_GRID_YHI = 73,  /* y > GridY - 3                             */
+    /* host-side errors of this library */
+    ICY_ERR_INVALID_ARGUMENT = 100,
+    ICY_ERR_CUDA = 101,            /* a CUDA runtime call failed                */
+    ICY_ERR_OUT_OF_MEMORY = 102,   /* device allocation refused or over budget  */
+    ICY_ERR_JSON = 103,            /* configuration text is not a JSON object   */
+    ICY_ERR_CONFIG_MISSING = 104,  /* "InputRawPoints" missing                  */
+    ICY_ERR_FILE = 105,            /* configuration file not found / unreadable */
+    ICY_ERR_CAPACITY = 106,        /* host HSSOA capacity too small             */
+    ICY_ERR_POINT_COUNT = 107,     /* active point count changed                */
+    ICY_ERR_TIMEOUT = 108,         /* a bounded device wait gave up             */
+    ICY_ERR_NOT_SUPPORTED = 109
+};
+
+/* ------------------------------------------------------------------ */
+/* SimParams                                                            */
+/* ------------------------------------------------------------------ */
+/*
+ * Field-for-field mirror of icy::SimParams (simulation/parameters_sim.h:37-85):
+ * same names, types and order, so the structs have the same layout and a
+ * caller holding an icy::SimParams may pass a pointer to it directly
+ * (the layout is checked by static_assert in oracle/ref_driver_common.h).
+ */
+typedef struct icy_sim_params {
+    int n_indenter_subdivisions;
+    int tpb_P2G, tpb_Upd, tpb_G2P;
+    int nPtsTotal;
+    int GridXTotal, GridY, GridTotal;
+    double GridXDimension;
+    double InitialTimeStep, SimulationEndTime;
+    int UpdateEveryNthStep;
+    int SimulationStep;
+    double SimulationTime;
+    double Gravity, Density, WaterDensity, PoissonsRatio, YoungsModulus;
+    double lambda, mu, kappa;
+    double IceCompressiveStrength, IceTensileStrength, IceShearStrength, IceTensileStrength2;
+    double NACC_beta, NACC_M, NACC_Msq;
+    double DP_tan_phi, DP_threshold_p;
+    double IndDiameter, IndRSq, IndVelocity, IndDepth;
+    double cellsize, cellsize_inv, Dp_inv;
+    double xmin, xmax, ymin, ymax;
+    int nxmin, nxmax, nymin, nymax;
+    double ParticleVolume, ParticleMass, WaterParticleMass, ParticleViewSize;
+    double indenter_x, indenter_x_initial, indenter_y, indenter_y_initial;
+    double Volume;
+    int SetupType;
+    double GrainVariability;
+    int GridHaloSize;
+    double ExtraSpaceForIncomingPoints;
+    double PointsTransferBufferFraction;
+    double RebalanceThresholdFreeSpaceRemaining;
+    double RebalanceThresholdDisabledPercentage;
+    int PointTransferFrequency;
+    int nPartitions;
+    int VectorCapacity_transfer;
+    double dt_vol_Dpinv, dt_Gravity, vmax, vmax_squared;
+    int gbOffset;
+} icy_sim_params;
+
+/* HSSOA line indices (simulation/parameters_sim.h:27-35) */
+enum {
+    ICY_IDX_UTILITY = 0, ICY_IDX_P = 1, ICY_IDX_Q = 2, ICY_IDX_JP_INV = 3,
+    ICY_POSX = 4, ICY_VELX = 6, ICY_FE00 = 8, ICY_BP00 = 12, ICY_N_PTS_ARRAYS = 16
+};
+/* utility-word status bits (simulation/kernels.cuh:12-14) */
+#define ICY_STATUS_CRUSHED  0x10000LL
+#define ICY_STATUS_DISABLED 0x20000LL
+#define ICY_STATUS_LIQUID   0x40000LL
+
+/* SimParams::Reset -- defaults (simulation/parameters_sim.cpp:5-60). */
+void icy_params_reset(icy_sim_params *p);
+/* SimParams::ComputeLame (simulation/parameters_sim.cpp:128-133). */
+void icy_params_compute_lame(icy_sim_params *p);
+/* SimParams::ComputeCamClayParams2 (simulation/parameters_sim.cpp:155-165). */
+void icy_params_compute_camclay(icy_sim_params *p);
+/* SimParams::ComputeHelperVariables (simulation/parameters_sim.cpp:135-153). */
+void icy_params_compute_helpers(icy_sim_params *p);
+/*
+ * SimParams::ParseFile on in-memory JSON text (simulation/parameters_sim.cpp:63-126):
+ * the same keys, DP_phi in degrees converted to DP_tan_phi, then
+ * ComputeCamClayParams2 + ComputeHelperVariables.  The "InputRawPoints"
+ * string is copied into raw_points (NUL-terminated, truncated to cap-1).
+ * Returns ICY_ERR_JSON if the text is not a JSON object and
+ * ICY_ERR_CONFIG_MISSING if "InputRawPoints" is absent (the parameters are
+ * still updated in that case, as in the reference, which throws after parsing).
+ */
+int icy_params_parse_json(icy_sim_params *p, const char *json_text,
+                          char *raw_points, size_t cap);
+/* SimParams::ParseFile on a file path (ICY_ERR_FILE if it does not exist). */
+int icy_params_parse_file(icy_sim_params *p, const char *path,
+                          char *raw_points, size_t cap);
+
+/* ------------------------------------------------------------------ */
+/* scene set-up (host only)                                             */
+/* ------------------------------------------------------------------ */
+/*
+ * Seeded synthetic ice block, replacing the HDF5 point cloud read by
+ * SnapshotManager::LoadRawPoints (simulation/snapshotmanager.cpp:29-121):
+ * a block of block_w x block_h metres, ppc particles per cell of size
+ * p->cellsize, each jittered uniformly inside its cell by a counter-based
+ * hash of (seed, cell, k); grain ids from a seeded Voronoi partition with
+ * n_grains sites (0 = all grain 0).  Writes x, y and the utility word into
+ * the HSSOA (line stride = capacity), then applies LoadRawPoints' placement
+ * rules: block centred in x and lifted by 2h (:71-78), points sorted by
+ * cell (:81, host_side_soa.cpp:50-61), Fe = I and Jp_inv = 1 (:82,
+ * host_side_soa.cpp:94-105), indenter start (:84-105), ParticleVolume =
+ * Volume/N and ComputeHelperVariables (:108-109).  On return *n_points holds N.
+ * Returns ICY_ERR_CAPACITY if N > capacity.
+ */
+int icy_scene_block(icy_sim_params *p, double block_w, double block_h, int ppc,
+                    uint64_t seed, int n_grains, double *hssoa, unsigned capacity,
+                    unsigned *n_points);
+/* Number of points icy_scene_block would create (for sizing the HSSOA). */
+unsigned icy_scene_block_count(const icy_sim_params *p, double block_w, double block_h, int ppc);
+
+/* ------------------------------------------------------------------ */
+/* one simulation instance on one device                                */
+/* ------------------------------------------------------------------ */
+typedef struct icy_mpm icy_mpm;
+
+/* Precision of the device state. */
+enum { ICY_PRECISION_FP64 = 0, ICY_PRECISION_FP32_SPLIT = 1 };
+
+/*
+ * GPU_Partition::initialize + allocate for a single partition
+ * (simulation/gpu_partition.cu:113-197): creates the stream, device particle
+ * SoA for `capacity` points, the grid covering x in [-halo, GridX+halo) and
+ * y in [0, GridY), the indenter accumulator and the status word.
+ */
+int icy_mpm_create(const icy_sim_params *p, int device, unsigned capacity,
+                   int precision, icy_mpm **out);
+/* GPU_Partition::~GPU_Partition (simulation/gpu_partition.cu:88-111). */
+int icy_mpm_destroy(icy_mpm *h);
+/* Run the instance's work on an external cudaStream_t (NULL = own stream). */
+int icy_mpm_set_stream(icy_mpm *h, void *cuda_stream);
+void *icy_mpm_get_stream(icy_mpm *h);
+/* GPU_Partition::update_constants (simulation/gpu_partition.cu:200-208):
+   copy the parameters and clear the device error code. */
+int icy_mpm_update_constants(icy_mpm *h, const icy_sim_params *p);
+/* GPU_Implementation5::transfer_ponts_to_device for one partition
+   (simulation/gpu_implementation5.cpp:346-356, gpu_partition.cu:49-68). */
+int icy_mpm_transfer_points_to_device(icy_mpm *h, const double *hssoa,
+                                      unsigned capacity, unsigned size);
+/*
+ * GPU_Implementation5::transfer_from_device for one partition
+ * (simulation/gpu_implementation5.cpp:360-436, gpu_partition.cu:16-46):
+ * copies the 16 lines back in the order they were uploaded, the indenter
+ * accumulator (2*n_indenter_subdivisions doubles, may be NULL) and the device
+ * error code; synchronises.  Returns the device error code if it is set and
+ * ICY_ERR_POINT_COUNT if the number of non-disabled points differs from
+ * p->nPtsTotal.  *size receives the number of points.
+ */
+int icy_mpm_transfer_from_device(icy_mpm *h, double *hssoa, unsigned capacity,
+                                 unsigned *size, double *indenter_force_bins);
+/* GPU_Partition::reset_indenter_force_accumulator (gpu_partition.cu:212-217). */
+int icy_mpm_reset_indenter_force_accumulator(icy_mpm *h);
+/* Sum of the indenter accumulator bins, read back synchronously (force[2]). */
+int icy_mpm_indenter_force(icy_mpm *h, double *force_xy, double *bins);
+
+/* Per-phase calls of GPU_Implementation5 (simulation/gpu_implementation5.h:44-51). */
+int icy_mpm_reset_grid(icy_mpm *h);                         /* gpu_partition.cu:221-228 */
+int icy_mpm_p2g(icy_mpm *h);                                /* gpu_partition.cu:230-242 */
+int icy_mpm_receive_halos(icy_mpm *h);                      /* no-op: one partition     */
+int icy_mpm_update_nodes(icy_mpm *h, double indenter_x,
+                         double indenter_y, double simulation_time); /* :244-257 */
+int icy_mpm_g2p(icy_mpm *h, int recordPQ, int enablePointTransfer); /* :259-293;
+                                   enablePointTransfer must be 0 (one domain) */
+int icy_mpm_receive_points(icy_mpm *h);                     /* no-op: one partition     */
+
+/*
+ * The sub-step loop of icy::Model::Step (simulation/model.cpp:38-54) on the
+ * device, with no host synchronisation: for k = 0..nsteps-1,
+ *   t += dt;  indenter_x = indenter_x_initial + t*IndVelocity;
+ *   reset grid; P2G; grid update(indenter at (indenter_x, indenter_y));
+ *   G2P(recordPQ = ((step0 + k) % UpdateEveryNthStep == 0)).
+ * `*sim_time` is advanced in place.  Work is queued on the instance stream
+ * (use icy_mpm_synchronize or a download to wait).
+ */
+int icy_mpm_step(icy_mpm *h, int step0, int nsteps, double *sim_time);
+int icy_mpm_synchronize(icy_mpm *h);
+/* Read (synchronously) and return the device error code (0 if none). */
+int icy_mpm_status(icy_mpm *h);
+/* Number of kernels this instance launched since creation. */
+int64_t icy_mpm_kernel_launches(icy_mpm *h);
+
+/* Library build description, e.g. "icempm_b200 sm_100a". */
+const char *icy_version(void);
+/* Text of the last error recorded on the calling thread ("" if none). */
+const char *icy_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ICEMPM_H */
