@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark of the MLS-MPM hot path (particle-steps/s) on one or more B200s.
+
+Workload: the single large instance -- grid 4096 x 2048 cells at h = 0.05 m,
+an ice block of 150 m x 40 m at 4 points per cell (9.6 M points, 1.23 GB of
+FP64 particle state), dt = 2e-5 s, E = 1 GPa, nu = 0.3, rho = 980, friction
+angle 62 deg, cohesion 0, gravity 9.81, indenter radius 1 m at 1 m/s.  The
+points are seeded synthetic (no point-cloud files are available).  One bench
+step = one MPM sub-step (grid reset, P2G, grid update, G2P + return mapping)
+over the whole instance.  The particle state (1.23 GB) is larger than L2, so
+no extra flush is done between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank runs its own replica (the instances are
+independent: weak scaling, no collective on the data path); the reported time
+is the maximum over ranks of the device-timed region.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from icempm_multi_b200.workloads import LARGE as WORKLOAD  # noqa: E402
+from icempm_multi_b200.workloads import make_workload as _make, workload_params  # noqa: E402
+
+METRIC = "particle-steps/s"
+# algorithmic bytes per particle-step of the FP64 path, per kernel (FP64 HSSOA fields
+# each phase must touch): P2G reads utility, pos, vel, Fe, Bp = 13 doubles; G2P reads
+# utility, pos, Fe, Jp = 8 doubles and writes 14 doubles
+ALG_BYTES = {"k_p2g_simple": 13 * 8, "k_g2p_simple": (8 + 14) * 8}
+
+
+def make_workload(pinned):
+    return _make(WORKLOAD, pinned=pinned)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.out = ""
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_setup(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def max_over_ranks(pg, value, local):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, local):
+    if pg is not None:
+        import torch
+        pg.barrier(device_ids=[local])
+
+
+def cpu_reference_rate(p, soa, target_s=15.0, max_steps=50, min_steps=2):
+    """The reference's own kernels compiled for the host (oracle/_ref, OpenMP on all
+    host cores) on the same workload; returns (particle-steps/s, steps, threads, seconds)."""
+    from oracle.oracle import RefHost
+    ref = RefHost()
+    threads = ref.max_threads()
+    work = soa.clone()
+    t0 = time.perf_counter()
+    ref.run(p, work, 0, 1, 0.0, threads=threads)
+    t1 = time.perf_counter() - t0
+    steps = int(max(min_steps, min(max_steps, target_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    err, _, _ = ref.run(p, work, 1, steps, p.InitialTimeStep, threads=threads)
+    dt = time.perf_counter() - t0
+    return soa.size * steps / dt, steps, threads, dt, err
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    p, soa = make_workload(pinned=False)
+    from oracle.oracle import RefHost
+    ref = RefHost()
+    threads = ref.max_threads()
+    work = soa.clone()
+    # one sub-step of the full instance, to size the sample
+    t0 = time.perf_counter()
+    ref.run(p, work, 0, 1, 0.0, threads=threads)
+    t_step = time.perf_counter() - t0
+    budget = 150.0
+    frac = min(1.0, budget / max((args.steps + args.warmup) * t_step, 1e-9))
+    sample = soa
+    desc = f"full instance ({soa.size} points) per step"
+    if frac < 1.0:
+        # a narrower block of the same grid, density and material (bounded sample)
+        from icempm_multi_b200 import make_block
+        w = dict(WORKLOAD)
+        w["block_w"] = max(2.0, WORKLOAD["block_w"] * frac)
+        pp = workload_params(w)
+        sample = make_block(pp, w["block_w"], w["block_h"], ppc=w["ppc"], seed=w["seed"], n_grains=w["n_grains"])
+        p = pp
+        desc = f"{w['block_w']:.2f} m x {w['block_h']} m block ({sample.size} points) per step"
+    work = sample.clone()
+    t = 0.0
+    _, t, _ = ref.run(p, work, 0, args.warmup, t, threads=threads)
+    t0 = time.perf_counter()
+    err, t, _ = ref.run(p, work, args.warmup, args.steps, t, threads=threads)
+    el = time.perf_counter() - t0
+    v = sample.size * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "error_code": err,
+        "config": {"workload": "single large FP64 instance, grid 4096x2048 h=0.05, 150x40 m block, 4 ppc",
+                   "points": soa.size, "dt": WORKLOAD["dt"]},
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
+                         "sample": desc + ", reference kernels (simulation/kernels.cuh) built for the host, OpenMP"},
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import numpy as np
+    import torch
+    from icempm_multi_b200 import GPUImplementation
+    from icempm_multi_b200._lib import lib
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    p, soa = make_workload(pinned=True)
+    n = soa.size
+    stream = torch.cuda.Stream(device=local)
+    g = GPUImplementation(p, soa, device=local)
+    g.set_stream(stream.cuda_stream)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.reset_indenter_force_accumulator()
+    t_sim = 0.0
+    with torch.cuda.stream(stream):
+        t_sim = g.run_steps(0, args.warmup, t_sim)
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region --------------------------------------------------
+    barrier(pg, local)
+    torch.cuda.synchronize()
+    l0 = g.kernel_launches()
+    g.profile(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            t_sim = g.run_steps(args.warmup, args.steps, t_sim)
+            ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(pg, local)
+    ms_local = ev0.elapsed_time(ev1)
+    launches = g.kernel_launches() - l0
+    prof = g.profile_read()
+    g.profile(False)
+    ms = max_over_ranks(pg, ms_local, local)
+    value = n * args.steps * world / (ms / 1e3)
+
+    # ---- end to end through the C-ABI with host buffers ----------------------------------
+    # upload the HSSOA from pinned host memory, run the steps with the reference's
+    # frame structure (a full HSSOA download every UpdateEveryNthStep sub-steps and
+    # at the end), all inside the timed region
+    frame = p.UpdateEveryNthStep
+    host = soa
+    barrier(pg, local)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    downloads = 0
+    w0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        g.transfer_ponts_to_device()
+        done = 0
+        t2 = 0.0
+        while done < args.steps:
+            k = min(frame, args.steps - done)
+            t2 = g.run_steps(done, k, t2)
+            done += k
+            g.transfer_from_device()     # synchronous download, as Model::Step does
+            downloads += 1
+        e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    ms_e2e = max_over_ranks(pg, max(e0.elapsed_time(e1), wall * 1e3), local)
+    e2e_value = n * args.steps * world / (ms_e2e / 1e3)
+    h2d = 16 * 8 * n / args.steps
+    d2h = 16 * 8 * n * downloads / args.steps
+
+    # ---- roofline of the dominant kernel ------------------------------------------------
+    peak, peak_kind = peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][0]) if prof else (None, (0, 0))
+    name, (tot_ms, cnt) = dom
+    per_launch_ms = tot_ms / max(cnt, 1)
+    alg = ALG_BYTES.get(name, 0) * n
+    achieved = alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get(name)
+        except Exception:
+            traffic = None
+
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "single large FP64 instance: grid 4096x2048 h=0.05 m, 150x40 m block, 4 ppc, "
+                               "dt=2e-5, E=1e9, phi=62, indenter r=1 m at 1 m/s",
+                   "points": n, "precision": "fp64", "l2": "inputs larger than L2 (1.23 GB particle state)",
+                   "replicas": world},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "frame_steps": frame, "downloads": downloads},
+        "gpu_launches": int(launches),
+        "kernels": {k: {"ms_total": v[0], "launches": v[1], "ms_per_launch": v[0] / max(v[1], 1)}
+                    for k, v in prof.items()},
+        "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None, "traffic": traffic,
+                     "peak_kind": peak_kind, "alg_bytes_per_launch": alg},
+        "clocks": clk.summary(),
+    }
+    g.close()
+
+    # ---- reference kernels built for sm_100a on the same GPU (a few steps) -----------------
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        try:
+            from oracle.oracle import RefCuda
+            work = soa.clone(pinned=False)
+            k = min(args.steps, 50)
+            err, _, _, rms = RefCuda().run(p, work, 0, k, 0.0)
+            out["reference_sm100a"] = {"value": n * k / (rms / 1e3), "unit": METRIC, "steps": k,
+                                       "error_code": err,
+                                       "what": "reference kernels.cuh built for sm_100a, one partition"}
+        except Exception as e:  # informational only
+            out["reference_sm100a"] = {"unavailable": str(e)[:200]}
+
+    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------------------------
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, steps, threads, secs, err = cpu_reference_rate(p, soa)
+            out["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
+                                   "sample": f"{steps} sub-steps of the full {n}-point instance "
+                                             f"({secs:.1f} s), reference kernels built for the host, OpenMP"}
+        except Exception as e:
+            out["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

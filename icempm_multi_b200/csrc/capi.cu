@@ -233,3 +233,99 @@ int icy_mpm_status(icy_mpm *h)
 int64_t icy_mpm_kernel_launches(icy_mpm *h) { return h ? h->launches : 0; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- profiling
+const char *const icy_kernel_names[K_N_KERNELS] = {
+    "k_p2g_simple", "k_update_simple", "k_g2p_simple", "memset_grid",
+};
+
+static cudaEvent_t pool_get(icy_mpm *h)
+{
+    if (h->event_pool.empty()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        return e;
+    }
+    cudaEvent_t e = h->event_pool.back();
+    h->event_pool.pop_back();
+    return e;
+}
+
+void icy_prof_begin(icy_mpm *h, int kernel)
+{
+    if (!h->profiling) return;
+    icy_mpm::ProfRec r{kernel, pool_get(h), pool_get(h)};
+    if (!r.a || !r.b) return;
+    cudaEventRecord(r.a, h->stream);
+    h->prof_recs.push_back(r);
+}
+
+void icy_prof_end(icy_mpm *h)
+{
+    if (!h->profiling || h->prof_recs.empty()) return;
+    cudaEventRecord(h->prof_recs.back().b, h->stream);
+}
+
+int icy_prof_resolve(icy_mpm *h)
+{
+    if (h->prof_recs.empty()) return ICY_OK;
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->prof_ms.size() != K_N_KERNELS) { h->prof_ms.assign(K_N_KERNELS, 0.0); h->prof_n.assign(K_N_KERNELS, 0); }
+    for (auto &r : h->prof_recs) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            h->prof_ms[r.kernel] += ms;
+            h->prof_n[r.kernel] += 1;
+        }
+        h->event_pool.push_back(r.a);
+        h->event_pool.push_back(r.b);
+    }
+    h->prof_recs.clear();
+    return ICY_OK;
+}
+
+void icy_prof_free(icy_mpm *h)
+{
+    for (auto &r : h->prof_recs) { h->event_pool.push_back(r.a); h->event_pool.push_back(r.b); }
+    h->prof_recs.clear();
+    for (auto e : h->event_pool) cudaEventDestroy(e);
+    h->event_pool.clear();
+}
+
+extern "C" {
+
+int icy_mpm_profile(icy_mpm *h, int enable)
+{
+    if (!h) return ICY_ERR_INVALID_ARGUMENT;
+    if (set_device(h)) return ICY_ERR_CUDA;
+    if (enable) {
+        int rc = icy_prof_resolve(h);
+        if (rc) return rc;
+        h->prof_ms.assign(K_N_KERNELS, 0.0);
+        h->prof_n.assign(K_N_KERNELS, 0);
+    }
+    h->profiling = enable != 0;
+    return ICY_OK;
+}
+
+int icy_mpm_profile_read(icy_mpm *h, int max, char *names, double *ms_total, int64_t *launches, int *count)
+{
+    if (!h || max < 0) return ICY_ERR_INVALID_ARGUMENT;
+    if (set_device(h)) return ICY_ERR_CUDA;
+    int rc = icy_prof_resolve(h);
+    if (rc) return rc;
+    int c = 0;
+    for (int k = 0; k < (int)h->prof_n.size(); k++) {
+        if (h->prof_n[k] == 0) continue;
+        if (c < max) {
+            if (names) { std::strncpy(names + 48 * c, icy_kernel_names[k], 47); names[48 * c + 47] = 0; }
+            if (ms_total) ms_total[c] = h->prof_ms[k];
+            if (launches) launches[c] = h->prof_n[k];
+        }
+        c++;
+    }
+    if (count) *count = c;
+    return ICY_OK;
+}
+
+}  // extern "C"

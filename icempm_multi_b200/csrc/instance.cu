@@ -63,6 +63,7 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
 
 void icy_instance_free(icy_mpm *h)
 {
+    icy_prof_free(h);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
     if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
     cudaFree(h->d_pts);
@@ -96,7 +97,9 @@ int icy_instance_download(icy_mpm *h, double *hssoa, unsigned cap)
 
 int icy_phase_reset_grid(icy_mpm *h)
 {
+    icy_prof_begin(h, K_MEMSET_GRID);
     CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 3 * h->n_nodes, h->stream));
+    icy_prof_end(h);
     return ICY_OK;
 }
 
@@ -105,8 +108,10 @@ int icy_phase_p2g(icy_mpm *h)
     if (!h->n) return ICY_OK;
     StepParams P = icy_step_params(h->prm);
     const int tpb = 256;
+    icy_prof_begin(h, K_P2G_SIMPLE);
     k_p2g_simple<<<(h->n + tpb - 1) / tpb, tpb, 0, h->stream>>>(P, h->d_pts, h->pitch, (int)h->n, grid_view(h),
                                                                 h->d_status);
+    icy_prof_end(h);
     CK_LAUNCH("k_p2g_simple");
     return ICY_OK;
 }
@@ -116,8 +121,10 @@ int icy_phase_update(icy_mpm *h, double ind_x, double ind_y)
     StepParams P = icy_step_params(h->prm);
     const int tpb = 256;
     const long nb = (h->n_nodes + tpb - 1) / tpb;
+    icy_prof_begin(h, K_UPDATE_SIMPLE);
     k_update_simple<<<(unsigned)nb, tpb, sizeof(double) * 2 * P.nsub, h->stream>>>(P, grid_view(h), h->n_nodes,
                                                                                  ind_x, ind_y, h->d_acc);
+    icy_prof_end(h);
     CK_LAUNCH("k_update_simple");
     return ICY_OK;
 }
@@ -127,8 +134,10 @@ int icy_phase_g2p(icy_mpm *h, bool recordPQ)
     if (!h->n) return ICY_OK;
     StepParams P = icy_step_params(h->prm);
     const int tpb = 128;
+    icy_prof_begin(h, K_G2P_SIMPLE);
     k_g2p_simple<<<(h->n + tpb - 1) / tpb, tpb, 0, h->stream>>>(P, h->d_pts, h->pitch, (int)h->n, grid_view(h),
                                                                 recordPQ ? 1 : 0, h->d_status);
+    icy_prof_end(h);
     CK_LAUNCH("k_g2p_simple");
     return ICY_OK;
 }

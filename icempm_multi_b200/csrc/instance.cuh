@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/icempm.h"
 #include "mpm_math.cuh"
@@ -29,7 +30,26 @@ struct icy_mpm {
     int *h_status = nullptr;      // pinned host mirror
 
     int64_t launches = 0;
+
+    // per-kernel event profiling (icy_mpm_profile)
+    struct ProfRec { int kernel; cudaEvent_t a, b; };
+    bool profiling = false;
+    std::vector<ProfRec> prof_recs;
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<double> prof_ms;
+    std::vector<int64_t> prof_n;
 };
+
+// kernel ids for profiling
+enum IcyKernel {
+    K_P2G_SIMPLE = 0, K_UPDATE_SIMPLE, K_G2P_SIMPLE, K_MEMSET_GRID,
+    K_N_KERNELS
+};
+extern const char *const icy_kernel_names[K_N_KERNELS];
+void icy_prof_begin(icy_mpm *h, int kernel);
+void icy_prof_end(icy_mpm *h);
+int icy_prof_resolve(icy_mpm *h);
+void icy_prof_free(icy_mpm *h);
 
 icy_dev::StepParams icy_step_params(const icy_sim_params &p);
 void icy_set_error(const char *where, cudaError_t e);

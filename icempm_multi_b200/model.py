@@ -105,6 +105,25 @@ class GPUImplementation:
     def kernel_launches(self):
         return lib().icy_mpm_kernel_launches(self._h)
 
+    def profile(self, enable):
+        """Start (clearing) or stop per-kernel CUDA-event timing on the instance stream."""
+        check(lib().icy_mpm_profile(self._h, int(bool(enable))), "icy_mpm_profile")
+
+    def profile_read(self):
+        """{kernel name: (total ms, launches)} recorded since profiling was enabled."""
+        mx = 32
+        names = C.create_string_buffer(48 * mx)
+        ms = np.zeros(mx)
+        n = np.zeros(mx, dtype=np.int64)
+        cnt = C.c_int(0)
+        check(lib().icy_mpm_profile_read(self._h, mx, names, ms.ctypes.data_as(C.c_void_p),
+                                         n.ctypes.data_as(C.c_void_p), C.byref(cnt)), "icy_mpm_profile_read")
+        out = {}
+        for k in range(min(cnt.value, mx)):
+            name = names.raw[48 * k:48 * (k + 1)].split(b"\0", 1)[0].decode()
+            out[name] = (float(ms[k]), int(n[k]))
+        return out
+
     # --- fused multi-step path ------------------------------------------------
     def run_steps(self, step0, nsteps, sim_time):
         """Queue nsteps sub-steps of Model::Step on the device; returns the new time."""

@@ -221,6 +221,20 @@ int icy_mpm_synchronize(icy_mpm *h);
 int icy_mpm_status(icy_mpm *h);
 /* Number of kernels this instance launched since creation. */
 int64_t icy_mpm_kernel_launches(icy_mpm *h);
+/*
+ * Per-kernel timing with CUDA events recorded on the instance stream around
+ * every kernel launch (the event pairs of GPU_Partition::record_timings,
+ * simulation/gpu_partition.cu:344-401, but per kernel and read only on
+ * request).  enable=1 clears and starts recording, enable=0 stops.
+ */
+int icy_mpm_profile(icy_mpm *h, int enable);
+/*
+ * Synchronises and returns up to `max` kernel entries: names (max x 48 chars,
+ * NUL-terminated), total milliseconds and launch counts; *count receives the
+ * number of distinct kernels recorded.
+ */
+int icy_mpm_profile_read(icy_mpm *h, int max, char *names, double *ms_total,
+                         int64_t *launches, int *count);
 
 /* Library build description, e.g. "icempm_b200 sm_100a". */
 const char *icy_version(void);

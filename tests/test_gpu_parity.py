@@ -1,0 +1,165 @@
+"""GPU parity: the CUDA library against the CPU oracle (and the reference's own
+CUDA kernels), called through the C-ABI.
+
+FP64 results differ from the oracle only by FMA contraction and the order of
+floating-point atomic sums, so the comparison uses per-field relative errors
+with the tolerances written below.  All cases keep every particle well inside
+the grid (checked on the oracle's trajectory before the reference's CUDA
+kernels, which do not stop at out-of-grid particles, are run).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from icempm_multi_b200 import GPUImplementation, Model
+from icempm_multi_b200._lib import ICY_ERR_OUT_OF_GRID, PRECISION_FP64, IcyError, lib
+from scenarios import standard, stress
+
+pytestmark = pytest.mark.gpu
+
+# FP64 tolerances (relative L2 over all non-disabled points)
+TOL = {"pos": 1e-12, "vel": 1e-7, "Fe": 1e-9, "Bp": 1e-6, "Jp": 1e-9}
+STATUS_MISMATCH_MAX = 0.01   # fraction of points whose crushed bit may differ
+
+
+@pytest.fixture(scope="module")
+def oracle(built):
+    from oracle.oracle import Oracle
+    return Oracle()
+
+
+def field_errors(a, b):
+    """Relative L2 errors of the GPU result a against the oracle result b."""
+    m = ~b.disabled()
+    def rel(x, y, shift=0.0):
+        den = np.linalg.norm(y - shift)
+        return float(np.linalg.norm(x - y) / (den if den > 0 else 1.0))
+    I = np.array([1.0, 0.0, 0.0, 1.0])[:, None]
+    return {
+        "pos": rel(a.pos[:, m], b.pos[:, m]),
+        "vel": rel(a.vel[:, m], b.vel[:, m]),
+        "Fe": rel(a.Fe[:, m] - I, b.Fe[:, m] - I),
+        "Bp": rel(a.Bp[:, m], b.Bp[:, m]),
+        "Jp": rel(a.Jp_inv[m] - 1.0, b.Jp_inv[m] - 1.0),
+        "status": float(np.mean(a.utility[m] != b.utility[m])),
+    }
+
+
+def run_gpu(p, soa, steps, phases=False):
+    out = soa.clone()
+    g = GPUImplementation(p, out)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.reset_indenter_force_accumulator()
+    t = 0.0
+    if phases:
+        for k in range(steps):   # the per-phase calls of icy::Model::Step (model.cpp:40-49)
+            t += p.InitialTimeStep
+            ix = p.indenter_x_initial + t * p.IndVelocity
+            g.reset_grid()
+            g.p2g()
+            g.receive_halos()
+            g.update_nodes(t, ix, p.indenter_y)
+            g.g2p(k % p.UpdateEveryNthStep == 0)
+            g.receive_points()
+    else:
+        t = g.run_steps(0, steps, 0.0)
+    g.transfer_from_device()
+    bins = g.indenter_bins.copy()
+    launches = g.kernel_launches()
+    g.close()
+    return out, t, bins, launches
+
+
+def assert_close(errs, tol=TOL):
+    for k, v in tol.items():
+        assert errs[k] <= v, (k, errs)
+    assert errs["status"] <= STATUS_MISMATCH_MAX, errs
+
+
+@pytest.mark.parametrize("make,steps", [(standard, 100), (stress, 40)])
+def test_step_matches_oracle(oracle, make, steps):
+    p, soa = make()
+    ref = soa.clone()
+    err, t_ref, bins_ref = oracle.run(p, ref, 0, steps)
+    assert err == 0
+    out, t, bins, launches = run_gpu(p, soa, steps)
+    assert t == t_ref
+    assert launches > 0
+    errs = field_errors(out, ref)
+    print(make.__name__, errs)
+    assert_close(errs)
+    # indenter force: total over bins
+    fr, fo = bins_ref.reshape(-1, 2).sum(0), bins.reshape(-1, 2).sum(0)
+    assert np.allclose(fo, fr, rtol=1e-6, atol=1e-6 * (np.abs(fr).max() + 1))
+
+
+def test_phase_api_matches_step_api(oracle):
+    p, soa = standard(seed=3)
+    a, _, ba, _ = run_gpu(p, soa, 50, phases=True)
+    b, _, bb, _ = run_gpu(p, soa, 50, phases=False)
+    errs = field_errors(a, b)
+    assert_close(errs)
+
+
+def test_larger_block_matches_oracle(oracle):
+    p, soa = standard(n_cells_x=96, n_cells_y=24, grid=(192, 64), seed=5)
+    ref = soa.clone()
+    err, _, _ = oracle.run(p, ref, 0, 150)
+    assert err == 0
+    out, _, _, _ = run_gpu(p, soa, 150)
+    errs = field_errors(out, ref)
+    print("larger", soa.size, errs)
+    assert_close(errs)
+
+
+def test_reference_cuda_kernels_match_oracle(oracle):
+    """The reference's own kernels built for sm_100a agree with the oracle to
+    the same tolerance (parity check against the reference GPU build)."""
+    from oracle.oracle import RefCuda
+    p, soa = standard(seed=6)
+    ref = soa.clone()
+    err, _, _ = oracle.run(p, ref, 0, 80)
+    assert err == 0
+    # every point stays > 4 cells inside the grid along the oracle trajectory
+    h = p.cellsize
+    assert ref.pos[0].min() > 4 * h and ref.pos[0].max() < (p.GridXTotal - 4) * h
+    assert ref.pos[1].min() > 2 * h and ref.pos[1].max() < (p.GridY - 4) * h
+    out = soa.clone()
+    rc, _, _, ms = RefCuda().run(p, out, 0, 80)
+    assert rc == 0
+    assert_close(field_errors(out, ref))
+
+
+def test_model_frame_loop(oracle):
+    """icy::Model::Step: one frame = UpdateEveryNthStep sub-steps + download,
+    force averaged over the frame (model.cpp:27-114)."""
+    p, soa = standard(seed=8)
+    log = []
+    m = Model(p, soa.clone(), force_log=log)
+    m.gpu.transfer_ponts_to_device()
+    m.Prepare()
+    m.Step()
+    m.Step()
+    n = 2 * p.UpdateEveryNthStep
+    assert p.SimulationStep == n and len(log) == 2
+    ref = soa.clone()
+    oracle.run(p, ref, 0, n)
+    assert_close(field_errors(m.gpu.hssoa, ref))
+    m.gpu.close()
+
+
+def test_out_of_grid_reports_reference_code(oracle):
+    """A point whose stencil leaves the grid yields the reference's error code
+    (70..73) at download instead of a memory fault: the kernels skip it."""
+    p, soa = standard(seed=2)
+    soa.pos[1, 0] = -0.6 * p.cellsize    # (int)(y/h - 0.5) = -1 < 0  -> code 71
+    g = GPUImplementation(p, soa.clone())
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.run_steps(0, 2, 0.0)
+    with pytest.raises(IcyError) as e:
+        g.transfer_from_device()
+    assert e.value.code in ICY_ERR_OUT_OF_GRID
+    g.close()
