@@ -232,11 +232,28 @@ int icy_mpm_status(icy_mpm *h)
 
 int64_t icy_mpm_kernel_launches(icy_mpm *h) { return h ? h->launches : 0; }
 
+int icy_mpm_set_option(icy_mpm *h, const char *name, double value)
+{
+    if (!h || !name) return ICY_ERR_INVALID_ARGUMENT;
+    const std::string k(name);
+    if (k == "resort_every") {
+        if (value < 0) return ICY_ERR_INVALID_ARGUMENT;
+        h->resort_every = (int)value;
+    } else if (k == "tiled") {
+        h->tiled = value != 0;
+        h->primed = false;
+    } else {
+        return ICY_ERR_INVALID_ARGUMENT;
+    }
+    return ICY_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------- profiling
 const char *const icy_kernel_names[K_N_KERNELS] = {
     "k_p2g_simple", "k_update_simple", "k_g2p_simple", "memset_grid",
+    "bin_sort", "k_tile_g2p2g", "k_tile_p2g", "k_tile_g2p", "k_update_tiles", "k_unpermute",
 };
 
 static cudaEvent_t pool_get(icy_mpm *h)

@@ -1,9 +1,11 @@
-// instance.cu -- allocation, host<->device transfer and the step loop of one
-// simulation instance.
+// instance.cu -- allocation, host<->device transfer, binning and the step loop
+// of one simulation instance.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "instance.cuh"
-#include "kernels_simple.cuh"
+#include "kernels_tiled.cuh"
 
 using namespace icy_dev;
 
@@ -32,6 +34,14 @@ static GridView grid_view(icy_mpm *h)
     return g;
 }
 
+static TileGeom tile_geom(icy_mpm *h) { return TileGeom{h->ntx, h->nty, h->ntiles}; }
+
+template <typename T>
+static cudaError_t dalloc(T **p, size_t count)
+{
+    return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
+}
+
 int icy_instance_allocate(icy_mpm *h, unsigned capacity)
 {
     if (h->precision != ICY_PRECISION_FP64) return ICY_ERR_NOT_SUPPORTED;
@@ -40,23 +50,46 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     h->stream = h->own_stream;
     h->capacity = capacity;
     h->pitch = ((long)capacity + 31) / 32 * 32;
-    h->n_nodes = (long)h->prm.GridY * (h->prm.GridXTotal + 2 * h->prm.GridHaloSize);
+    const int nx = h->prm.GridXTotal + 2 * h->prm.GridHaloSize;
+    h->n_nodes = (long)h->prm.GridY * nx;
+    h->ntx = (nx + TX - 1) / TX;
+    h->nty = (h->prm.GridY + TY - 1) / TY;
+    h->ntiles = h->ntx * h->nty;
     cudaError_t e;
-    if ((e = cudaMalloc(&h->d_pts, sizeof(double) * 16 * h->pitch)) != cudaSuccess) {
+    if ((e = dalloc(&h->d_pts, 16 * h->pitch)) != cudaSuccess || (e = dalloc(&h->d_pts_alt, 16 * h->pitch)) != cudaSuccess) {
         icy_set_error("cudaMalloc(particles)", e);
         return ICY_ERR_OUT_OF_MEMORY;
     }
-    if ((e = cudaMalloc(&h->d_grid, sizeof(double) * 5 * h->n_nodes)) != cudaSuccess) {
+    if ((e = dalloc(&h->d_grid, 5 * h->n_nodes)) != cudaSuccess) {
         icy_set_error("cudaMalloc(grid)", e);
         return ICY_ERR_OUT_OF_MEMORY;
     }
-    CK(cudaMalloc(&h->d_acc, sizeof(double) * 2 * h->prm.n_indenter_subdivisions));
-    CK(cudaMalloc(&h->d_status, sizeof(int)));
+    CK(dalloc(&h->d_oidx, h->pitch));
+    CK(dalloc(&h->d_oidx_alt, h->pitch));
+    CK(dalloc(&h->d_keys, h->pitch));
+    CK(dalloc(&h->d_ranks, h->pitch));
+    CK(dalloc(&h->d_counts, h->ntiles + 1));
+    CK(dalloc(&h->d_start, h->ntiles + 2));
+    CK(dalloc(&h->d_active, h->ntiles));
+    CK(dalloc(&h->d_nactive, 1));
+    CK(dalloc(&h->d_flags, h->ntiles));
+    CK(dalloc(&h->d_moved, 1));
+    CK(dalloc(&h->d_acc, 2 * h->prm.n_indenter_subdivisions));
+    CK(dalloc(&h->d_status, 1));
     CK(cudaMallocHost(&h->h_status, sizeof(int)));
     CK(cudaMemsetAsync(h->d_pts, 0, sizeof(double) * 16 * h->pitch, h->stream));
     CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 5 * h->n_nodes, h->stream));
+    CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
+    CK(cudaMemsetAsync(h->d_nactive, 0, sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_moved, 0, sizeof(unsigned long long), h->stream));
     CK(cudaMemsetAsync(h->d_acc, 0, sizeof(double) * 2 * h->prm.n_indenter_subdivisions, h->stream));
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
+    // persistent grid sizes
+    int sms = 0, per_sm = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<true, true, false>, TILE_THREADS, 0));
+    h->tile_grid = std::max(1, sms * std::max(per_sm, 1));
+    h->update_grid = std::max(1, std::min(h->ntiles, sms * 8));
     CK(cudaStreamSynchronize(h->stream));
     return ICY_OK;
 }
@@ -66,14 +99,17 @@ void icy_instance_free(icy_mpm *h)
     icy_prof_free(h);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
     if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
-    cudaFree(h->d_pts);
-    cudaFree(h->d_grid);
-    cudaFree(h->d_acc);
-    cudaFree(h->d_status);
+    void *ptrs[] = {h->d_pts, h->d_pts_alt, h->d_grid, h->d_oidx, h->d_oidx_alt, h->d_keys, h->d_ranks,
+                    h->d_counts, h->d_start, h->d_active, h->d_nactive, h->d_flags, h->d_moved, h->d_acc,
+                    h->d_status};
+    for (void *p : ptrs) cudaFree(p);
     cudaFreeHost(h->h_status);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
-    h->d_pts = h->d_grid = h->d_acc = nullptr;
-    h->d_status = h->h_status = nullptr;
+    h->d_pts = h->d_pts_alt = h->d_grid = h->d_acc = nullptr;
+    h->d_oidx = h->d_oidx_alt = h->d_keys = h->d_ranks = h->d_counts = h->d_start = nullptr;
+    h->d_active = h->d_nactive = h->d_status = h->h_status = nullptr;
+    h->d_flags = nullptr;
+    h->d_moved = nullptr;
     h->own_stream = h->stream = nullptr;
 }
 
@@ -84,14 +120,113 @@ int icy_instance_upload(icy_mpm *h, const double *hssoa, unsigned cap, unsigned 
         CK(cudaMemcpy2DAsync(h->d_pts, sizeof(double) * h->pitch, hssoa, sizeof(double) * cap,
                              sizeof(double) * size, 16, cudaMemcpyHostToDevice, h->stream));
     h->n = size;
+    h->binned = false;
+    h->permuted = false;
+    h->primed = false;
+    if (size) {
+        k_iota<<<(size + 255) / 256, 256, 0, h->stream>>>(h->d_oidx, (int)size);
+        CK_LAUNCH("k_iota");
+    }
     return ICY_OK;
 }
 
 int icy_instance_download(icy_mpm *h, double *hssoa, unsigned cap)
 {
-    if (h->n)
-        CK(cudaMemcpy2DAsync(hssoa, sizeof(double) * cap, h->d_pts, sizeof(double) * h->pitch,
-                             sizeof(double) * h->n, 16, cudaMemcpyDeviceToHost, h->stream));
+    if (!h->n) return ICY_OK;
+    const double *src = h->d_pts;
+    if (h->permuted) {
+        icy_prof_begin(h, K_UNPERMUTE);
+        k_unpermute<<<(h->n + 255) / 256, 256, 0, h->stream>>>(h->d_pts, h->d_pts_alt, h->pitch, (int)h->n,
+                                                               h->d_oidx);
+        icy_prof_end(h);
+        CK_LAUNCH("k_unpermute");
+        src = h->d_pts_alt;
+    }
+    CK(cudaMemcpy2DAsync(hssoa, sizeof(double) * cap, src, sizeof(double) * h->pitch, sizeof(double) * h->n, 16,
+                         cudaMemcpyDeviceToHost, h->stream));
+    return ICY_OK;
+}
+
+// Counting sort of the points by tile (stable per warp, not globally):
+// count -> scan (+ list of non-empty tiles) -> scatter into the second buffer.
+int icy_instance_bin(icy_mpm *h)
+{
+    if (!h->n) { h->binned = true; return ICY_OK; }
+    StepParams P = icy_step_params(h->prm);
+    const int nb = (h->n + 255) / 256;
+    icy_prof_begin(h, K_BIN);
+    CK(cudaMemsetAsync(h->d_counts, 0, sizeof(int) * (h->ntiles + 1), h->stream));
+    k_bin_count<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_pts, h->pitch, (int)h->n, h->d_keys, h->d_ranks,
+                                           h->d_counts, h->d_status);
+    CK_LAUNCH("k_bin_count");
+    k_bin_scan<<<1, 1024, 0, h->stream>>>(h->d_counts, h->ntiles, h->d_start, h->d_active, h->d_nactive);
+    CK_LAUNCH("k_bin_scan");
+    k_bin_scatter<<<nb, 256, 0, h->stream>>>(h->d_pts, h->d_pts_alt, h->pitch, (int)h->n, h->d_keys, h->d_ranks,
+                                             h->d_start, h->d_oidx, h->d_oidx_alt);
+    CK_LAUNCH("k_bin_scatter");
+    icy_prof_end(h);
+    std::swap(h->d_pts, h->d_pts_alt);
+    std::swap(h->d_oidx, h->d_oidx_alt);
+    h->binned = true;
+    h->permuted = true;
+    h->steps_since_bin = 0;
+    return ICY_OK;
+}
+
+static TileArgs tile_args(icy_mpm *h, bool record)
+{
+    TileArgs A;
+    A.P = icy_step_params(h->prm);
+    A.G = tile_geom(h);
+    A.g = grid_view(h);
+    A.pts = h->d_pts;
+    A.pitch = h->pitch;
+    A.tile_start = h->d_start;
+    A.active = h->d_active;
+    A.n_active = h->d_nactive;
+    A.flags = h->d_flags;
+    A.status = h->d_status;
+    A.moved = h->d_moved;
+    A.record_pq = record ? 1 : 0;
+    return A;
+}
+
+// which: 0 = G2P+P2G, 1 = P2G only, 2 = G2P only (writes vel and Bp)
+static int launch_tile(icy_mpm *h, int which, bool record)
+{
+    if (!h->n) return ICY_OK;
+    if (!h->binned) {
+        int rc = icy_instance_bin(h);
+        if (rc) return rc;
+    }
+    TileArgs A = tile_args(h, record);
+    switch (which) {
+    case 0:
+        icy_prof_begin(h, K_TILE_G2P2G);
+        k_tile<true, true, false><<<h->tile_grid, TILE_THREADS, 0, h->stream>>>(A);
+        break;
+    case 1:
+        icy_prof_begin(h, K_TILE_P2G);
+        k_tile<false, true, false><<<h->tile_grid, TILE_THREADS, 0, h->stream>>>(A);
+        break;
+    default:
+        icy_prof_begin(h, K_TILE_G2P);
+        k_tile<true, false, true><<<h->tile_grid, TILE_THREADS, 0, h->stream>>>(A);
+        break;
+    }
+    icy_prof_end(h);
+    CK_LAUNCH("k_tile");
+    return ICY_OK;
+}
+
+static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y)
+{
+    StepParams P = icy_step_params(h->prm);
+    icy_prof_begin(h, K_UPDATE_TILES);
+    k_update_tiles<<<h->update_grid, TT, sizeof(double) * 2 * P.nsub, h->stream>>>(
+        P, tile_geom(h), grid_view(h), h->d_flags, ind_x, ind_y, h->d_acc);
+    icy_prof_end(h);
+    CK_LAUNCH("k_update_tiles");
     return ICY_OK;
 }
 
@@ -100,12 +235,15 @@ int icy_phase_reset_grid(icy_mpm *h)
     icy_prof_begin(h, K_MEMSET_GRID);
     CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 3 * h->n_nodes, h->stream));
     icy_prof_end(h);
+    if (h->tiled) CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
+    h->primed = false;
     return ICY_OK;
 }
 
 int icy_phase_p2g(icy_mpm *h)
 {
     if (!h->n) return ICY_OK;
+    if (h->tiled) return launch_tile(h, 1, false);
     StepParams P = icy_step_params(h->prm);
     const int tpb = 256;
     icy_prof_begin(h, K_P2G_SIMPLE);
@@ -118,6 +256,7 @@ int icy_phase_p2g(icy_mpm *h)
 
 int icy_phase_update(icy_mpm *h, double ind_x, double ind_y)
 {
+    if (h->tiled) return launch_update_tiles(h, ind_x, ind_y);
     StepParams P = icy_step_params(h->prm);
     const int tpb = 256;
     const long nb = (h->n_nodes + tpb - 1) / tpb;
@@ -132,6 +271,8 @@ int icy_phase_update(icy_mpm *h, double ind_x, double ind_y)
 int icy_phase_g2p(icy_mpm *h, bool recordPQ)
 {
     if (!h->n) return ICY_OK;
+    h->primed = false;
+    if (h->tiled) return launch_tile(h, 2, recordPQ);
     StepParams P = icy_step_params(h->prm);
     const int tpb = 128;
     icy_prof_begin(h, K_G2P_SIMPLE);
@@ -146,16 +287,40 @@ int icy_instance_steps(icy_mpm *h, int step0, int nsteps, double *sim_time)
 {
     double t = *sim_time;
     const icy_sim_params &p = h->prm;
+    int rc;
+    if (!h->tiled) {
+        for (int k = 0; k < nsteps; k++) {
+            // icy::Model::Step sub-step (simulation/model.cpp:40-49)
+            t += p.InitialTimeStep;
+            const double ind_x = p.indenter_x_initial + t * p.IndVelocity;
+            if ((rc = icy_phase_reset_grid(h))) return rc;
+            if ((rc = icy_phase_p2g(h))) return rc;
+            if ((rc = icy_phase_update(h, ind_x, p.indenter_y))) return rc;
+            const bool rec = ((step0 + k) % p.UpdateEveryNthStep) == 0;
+            if ((rc = icy_phase_g2p(h, rec))) return rc;
+        }
+        *sim_time = t;
+        return ICY_OK;
+    }
+    if (nsteps == 0) return ICY_OK;
+    // tiled path: P2G(first), then [update(k); G2P(k)+P2G(k+1)] ..., last G2P alone
+    if (!h->primed) {
+        if ((rc = launch_tile(h, 1, false))) return rc;
+        h->primed = true;
+    }
     for (int k = 0; k < nsteps; k++) {
-        // icy::Model::Step sub-step (simulation/model.cpp:40-49)
         t += p.InitialTimeStep;
         const double ind_x = p.indenter_x_initial + t * p.IndVelocity;
-        int rc;
-        if ((rc = icy_phase_reset_grid(h))) return rc;
-        if ((rc = icy_phase_p2g(h))) return rc;
-        if ((rc = icy_phase_update(h, ind_x, p.indenter_y))) return rc;
+        if ((rc = launch_update_tiles(h, ind_x, p.indenter_y))) return rc;
         const bool rec = ((step0 + k) % p.UpdateEveryNthStep) == 0;
-        if ((rc = icy_phase_g2p(h, rec))) return rc;
+        if (k == nsteps - 1) {
+            if ((rc = launch_tile(h, 2, rec))) return rc;
+            h->primed = false;
+        } else {
+            if ((rc = launch_tile(h, 0, rec))) return rc;
+            if (h->resort_every > 0 && ++h->steps_since_bin >= h->resort_every)
+                if ((rc = icy_instance_bin(h))) return rc;
+        }
     }
     *sim_time = t;
     return ICY_OK;

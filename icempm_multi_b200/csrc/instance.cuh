@@ -25,6 +25,22 @@ struct icy_mpm {
     long n_nodes = 0;
     double *d_grid = nullptr;
 
+    // binning by tile (tiled path): second particle buffer for the permutation,
+    // upload index of every slot, sort scratch, tile ranges, node-tile marks
+    double *d_pts_alt = nullptr;
+    int *d_oidx = nullptr, *d_oidx_alt = nullptr, *d_keys = nullptr, *d_ranks = nullptr;
+    int *d_counts = nullptr, *d_start = nullptr, *d_active = nullptr, *d_nactive = nullptr;
+    unsigned *d_flags = nullptr;
+    unsigned long long *d_moved = nullptr;
+    int ntx = 0, nty = 0, ntiles = 0;
+    int tile_grid = 0, update_grid = 0;
+    bool binned = false;        // points sorted by tile since the last upload
+    bool permuted = false;      // device order differs from upload order
+    bool primed = false;        // accumulators hold P2G of the current state
+    int steps_since_bin = 0;
+    int resort_every = 64;      // re-bin interval in steps (0 = never)
+    bool tiled = true;          // tiled kernels (false: one-thread-per-item kernels)
+
     double *d_acc = nullptr;      // indenter force bins, 2*n_indenter_subdivisions
     int *d_status = nullptr;      // device error code (reference codes 70..73, 5)
     int *h_status = nullptr;      // pinned host mirror
@@ -43,6 +59,7 @@ struct icy_mpm {
 // kernel ids for profiling
 enum IcyKernel {
     K_P2G_SIMPLE = 0, K_UPDATE_SIMPLE, K_G2P_SIMPLE, K_MEMSET_GRID,
+    K_BIN, K_TILE_G2P2G, K_TILE_P2G, K_TILE_G2P, K_UPDATE_TILES, K_UNPERMUTE,
     K_N_KERNELS
 };
 extern const char *const icy_kernel_names[K_N_KERNELS];
@@ -64,3 +81,4 @@ int icy_phase_p2g(icy_mpm *h);
 int icy_phase_update(icy_mpm *h, double ind_x, double ind_y);
 int icy_phase_g2p(icy_mpm *h, bool recordPQ);
 int icy_instance_steps(icy_mpm *h, int step0, int nsteps, double *sim_time);
+int icy_instance_bin(icy_mpm *h);

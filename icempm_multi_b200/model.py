@@ -105,6 +105,10 @@ class GPUImplementation:
     def kernel_launches(self):
         return lib().icy_mpm_kernel_launches(self._h)
 
+    def set_option(self, name, value):
+        """Instance tuning option (include/icempm.h: icy_mpm_set_option)."""
+        check(lib().icy_mpm_set_option(self._h, name.encode(), float(value)), "icy_mpm_set_option")
+
     def profile(self, enable):
         """Start (clearing) or stop per-kernel CUDA-event timing on the instance stream."""
         check(lib().icy_mpm_profile(self._h, int(bool(enable))), "icy_mpm_profile")

@@ -219,6 +219,15 @@ int icy_mpm_step(icy_mpm *h, int step0, int nsteps, double *sim_time);
 int icy_mpm_synchronize(icy_mpm *h);
 /* Read (synchronously) and return the device error code (0 if none). */
 int icy_mpm_status(icy_mpm *h);
+/*
+ * Tuning options of an instance (no counterpart in the reference, whose
+ * launch shapes come from tpb_* in SimParams):
+ *   "resort_every"  re-bin the points by tile every N steps (0 = only after upload)
+ *   "tiled"         1 = binned, tile-staged kernels (default); 0 = one thread per
+ *                   point / node, unsorted (the reference's kernel structure)
+ */
+int icy_mpm_set_option(icy_mpm *h, const char *name, double value);
+
 /* Number of kernels this instance launched since creation. */
 int64_t icy_mpm_kernel_launches(icy_mpm *h);
 /*
