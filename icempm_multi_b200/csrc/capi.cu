@@ -253,7 +253,7 @@ int icy_mpm_set_option(icy_mpm *h, const char *name, double value)
 // ---------------------------------------------------------------- profiling
 const char *const icy_kernel_names[K_N_KERNELS] = {
     "k_p2g_simple", "k_update_simple", "k_g2p_simple", "memset_grid",
-    "bin_sort", "k_tile_g2p2g", "k_tile_p2g", "k_tile_g2p", "k_update_tiles", "k_unpermute",
+    "bin_sort", "k_tile_g2p2g", "k_tile_p2g", "k_tile_g2p", "k_update_nodes", "k_unpermute",
 };
 
 static cudaEvent_t pool_get(icy_mpm *h)

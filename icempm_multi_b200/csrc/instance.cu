@@ -68,8 +68,11 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(dalloc(&h->d_oidx_alt, h->pitch));
     CK(dalloc(&h->d_keys, h->pitch));
     CK(dalloc(&h->d_ranks, h->pitch));
-    CK(dalloc(&h->d_counts, h->ntiles + 1));
-    CK(dalloc(&h->d_start, h->ntiles + 2));
+    const long nkeys = (long)h->ntiles * TT + 1;   // cells + the disabled / out-of-grid bucket
+    h->scan_blocks = (int)((nkeys + SCAN_BLOCK - 1) / SCAN_BLOCK);
+    CK(dalloc(&h->d_counts, nkeys));
+    CK(dalloc(&h->d_start, nkeys + 1));
+    CK(dalloc(&h->d_block_sums, h->scan_blocks));
     CK(dalloc(&h->d_active, h->ntiles));
     CK(dalloc(&h->d_nactive, 1));
     CK(dalloc(&h->d_flags, h->ntiles));
@@ -87,9 +90,11 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     // persistent grid sizes
     int sms = 0, per_sm = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<true, true, false>, TILE_THREADS, 0));
+    CK(cudaFuncSetAttribute(k_tile<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_DYN_SMEM));
+    CK(cudaFuncSetAttribute(k_tile<false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_DYN_SMEM));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<true, true, false>, TILE_THREADS, TILE_DYN_SMEM));
     h->tile_grid = std::max(1, sms * std::max(per_sm, 1));
-    h->update_grid = std::max(1, std::min(h->ntiles, sms * 8));
+    h->update_grid = (int)std::max(1L, std::min((h->n_nodes + 255) / 256, (long)sms * 16));
     CK(cudaStreamSynchronize(h->stream));
     return ICY_OK;
 }
@@ -101,13 +106,13 @@ void icy_instance_free(icy_mpm *h)
     if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->d_pts, h->d_pts_alt, h->d_grid, h->d_oidx, h->d_oidx_alt, h->d_keys, h->d_ranks,
                     h->d_counts, h->d_start, h->d_active, h->d_nactive, h->d_flags, h->d_moved, h->d_acc,
-                    h->d_status};
+                    h->d_status, h->d_block_sums};
     for (void *p : ptrs) cudaFree(p);
     cudaFreeHost(h->h_status);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     h->d_pts = h->d_pts_alt = h->d_grid = h->d_acc = nullptr;
     h->d_oidx = h->d_oidx_alt = h->d_keys = h->d_ranks = h->d_counts = h->d_start = nullptr;
-    h->d_active = h->d_nactive = h->d_status = h->h_status = nullptr;
+    h->d_active = h->d_nactive = h->d_status = h->h_status = h->d_block_sums = nullptr;
     h->d_flags = nullptr;
     h->d_moved = nullptr;
     h->own_stream = h->stream = nullptr;
@@ -154,13 +159,20 @@ int icy_instance_bin(icy_mpm *h)
     if (!h->n) { h->binned = true; return ICY_OK; }
     StepParams P = icy_step_params(h->prm);
     const int nb = (h->n + 255) / 256;
+    const int nkeys = h->ntiles * TT + 1;
     icy_prof_begin(h, K_BIN);
-    CK(cudaMemsetAsync(h->d_counts, 0, sizeof(int) * (h->ntiles + 1), h->stream));
+    CK(cudaMemsetAsync(h->d_counts, 0, sizeof(int) * nkeys, h->stream));
     k_bin_count<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_pts, h->pitch, (int)h->n, h->d_keys, h->d_ranks,
                                            h->d_counts, h->d_status);
     CK_LAUNCH("k_bin_count");
-    k_bin_scan<<<1, 1024, 0, h->stream>>>(h->d_counts, h->ntiles, h->d_start, h->d_active, h->d_nactive);
-    CK_LAUNCH("k_bin_scan");
+    k_scan_reduce<<<h->scan_blocks, SCAN_NT, 0, h->stream>>>(h->d_counts, nkeys, h->d_block_sums);
+    CK_LAUNCH("k_scan_reduce");
+    k_scan_blocks<<<1, 1024, 0, h->stream>>>(h->d_block_sums, h->scan_blocks);
+    CK_LAUNCH("k_scan_blocks");
+    k_scan_apply<<<h->scan_blocks, SCAN_NT, 0, h->stream>>>(h->d_counts, nkeys, h->d_block_sums, h->d_start);
+    CK_LAUNCH("k_scan_apply");
+    k_tiles_active<<<1, 1024, 0, h->stream>>>(h->d_start, h->ntiles, h->d_active, h->d_nactive);
+    CK_LAUNCH("k_tiles_active");
     k_bin_scatter<<<nb, 256, 0, h->stream>>>(h->d_pts, h->d_pts_alt, h->pitch, (int)h->n, h->d_keys, h->d_ranks,
                                              h->d_start, h->d_oidx, h->d_oidx_alt);
     CK_LAUNCH("k_bin_scatter");
@@ -181,7 +193,7 @@ static TileArgs tile_args(icy_mpm *h, bool record)
     A.g = grid_view(h);
     A.pts = h->d_pts;
     A.pitch = h->pitch;
-    A.tile_start = h->d_start;
+    A.cell_start = h->d_start;
     A.active = h->d_active;
     A.n_active = h->d_nactive;
     A.flags = h->d_flags;
@@ -203,11 +215,11 @@ static int launch_tile(icy_mpm *h, int which, bool record)
     switch (which) {
     case 0:
         icy_prof_begin(h, K_TILE_G2P2G);
-        k_tile<true, true, false><<<h->tile_grid, TILE_THREADS, 0, h->stream>>>(A);
+        k_tile<true, true, false><<<h->tile_grid, TILE_THREADS, TILE_DYN_SMEM, h->stream>>>(A);
         break;
     case 1:
         icy_prof_begin(h, K_TILE_P2G);
-        k_tile<false, true, false><<<h->tile_grid, TILE_THREADS, 0, h->stream>>>(A);
+        k_tile<false, true, false><<<h->tile_grid, TILE_THREADS, TILE_DYN_SMEM, h->stream>>>(A);
         break;
     default:
         icy_prof_begin(h, K_TILE_G2P);
@@ -223,10 +235,11 @@ static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y)
 {
     StepParams P = icy_step_params(h->prm);
     icy_prof_begin(h, K_UPDATE_TILES);
-    k_update_tiles<<<h->update_grid, TT, sizeof(double) * 2 * P.nsub, h->stream>>>(
-        P, tile_geom(h), grid_view(h), h->d_flags, ind_x, ind_y, h->d_acc);
+    k_update_nodes<<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
+        P, tile_geom(h), grid_view(h), h->d_flags, h->n_nodes, ind_x, ind_y, h->d_acc);
     icy_prof_end(h);
-    CK_LAUNCH("k_update_tiles");
+    CK_LAUNCH("k_update_nodes");
+    CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
     return ICY_OK;
 }
 

@@ -30,6 +30,8 @@ struct icy_mpm {
     double *d_pts_alt = nullptr;
     int *d_oidx = nullptr, *d_oidx_alt = nullptr, *d_keys = nullptr, *d_ranks = nullptr;
     int *d_counts = nullptr, *d_start = nullptr, *d_active = nullptr, *d_nactive = nullptr;
+    int *d_block_sums = nullptr;
+    int scan_blocks = 0;
     unsigned *d_flags = nullptr;
     unsigned long long *d_moved = nullptr;
     int ntx = 0, nty = 0, ntiles = 0;
