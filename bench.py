@@ -35,7 +35,11 @@ METRIC = "particle-steps/s"
 # algorithmic bytes per particle-step of the FP64 path, per kernel (FP64 HSSOA fields
 # each phase must touch): P2G reads utility, pos, vel, Fe, Bp = 13 doubles; G2P reads
 # utility, pos, Fe, Jp = 8 doubles and writes 14 doubles
-ALG_BYTES = {"k_p2g_simple": 13 * 8, "k_g2p_simple": (8 + 14) * 8}
+ALG_BYTES = {"k_p2g_simple": 13 * 8, "k_g2p_simple": (8 + 14) * 8,
+             # fused G2P(n)+P2G(n+1): the persistent point state (utility, pos, Fe, Jp)
+             # read once and written once; vel and Bp are not stored between steps
+             "k_tile_g2p2g": (8 + 8) * 8,
+             "k_tile_p2g": 14 * 8, "k_tile_g2p": (8 + 14) * 8}
 
 
 def make_workload(pinned):

@@ -103,7 +103,7 @@ int icy_mpm_update_constants(icy_mpm *h, const icy_sim_params *p)
     if (set_device(h)) return ICY_ERR_CUDA;
     h->prm = *p;
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
-    return ICY_OK;
+    return icy_instance_constants(h);
 }
 
 int icy_mpm_transfer_points_to_device(icy_mpm *h, const double *hssoa, unsigned capacity, unsigned size)

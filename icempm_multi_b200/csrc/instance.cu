@@ -79,6 +79,7 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(dalloc(&h->d_moved, 1));
     CK(dalloc(&h->d_acc, 2 * h->prm.n_indenter_subdivisions));
     CK(dalloc(&h->d_status, 1));
+    CK(dalloc(&h->d_grain, GRAIN_TAB));
     CK(cudaMallocHost(&h->h_status, sizeof(int)));
     CK(cudaMemsetAsync(h->d_pts, 0, sizeof(double) * 16 * h->pitch, h->stream));
     CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 5 * h->n_nodes, h->stream));
@@ -95,6 +96,7 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<true, true, false>, TILE_THREADS, TILE_DYN_SMEM));
     h->tile_grid = std::max(1, sms * std::max(per_sm, 1));
     h->update_grid = (int)std::max(1L, std::min((h->n_nodes + 255) / 256, (long)sms * 16));
+    if (int rc = icy_instance_constants(h)) return rc;
     CK(cudaStreamSynchronize(h->stream));
     return ICY_OK;
 }
@@ -106,7 +108,7 @@ void icy_instance_free(icy_mpm *h)
     if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->d_pts, h->d_pts_alt, h->d_grid, h->d_oidx, h->d_oidx_alt, h->d_keys, h->d_ranks,
                     h->d_counts, h->d_start, h->d_active, h->d_nactive, h->d_flags, h->d_moved, h->d_acc,
-                    h->d_status, h->d_block_sums};
+                    h->d_status, h->d_block_sums, h->d_grain};
     for (void *p : ptrs) cudaFree(p);
     cudaFreeHost(h->h_status);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
@@ -115,6 +117,7 @@ void icy_instance_free(icy_mpm *h)
     h->d_active = h->d_nactive = h->d_status = h->h_status = h->d_block_sums = nullptr;
     h->d_flags = nullptr;
     h->d_moved = nullptr;
+    h->d_grain = nullptr;
     h->own_stream = h->stream = nullptr;
 }
 
@@ -199,6 +202,7 @@ static TileArgs tile_args(icy_mpm *h, bool record)
     A.flags = h->d_flags;
     A.status = h->d_status;
     A.moved = h->d_moved;
+    A.grain_tab = h->d_grain;
     A.record_pq = record ? 1 : 0;
     return A;
 }
@@ -240,6 +244,14 @@ static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y)
     icy_prof_end(h);
     CK_LAUNCH("k_update_nodes");
     CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
+    return ICY_OK;
+}
+
+// per-instance tables that depend on the parameters
+int icy_instance_constants(icy_mpm *h)
+{
+    k_grain_table<<<(GRAIN_TAB + 255) / 256, 256, 0, h->stream>>>(icy_step_params(h->prm), h->d_grain);
+    CK_LAUNCH("k_grain_table");
     return ICY_OK;
 }
 

@@ -31,6 +31,7 @@ struct icy_mpm {
     int *d_oidx = nullptr, *d_oidx_alt = nullptr, *d_keys = nullptr, *d_ranks = nullptr;
     int *d_counts = nullptr, *d_start = nullptr, *d_active = nullptr, *d_nactive = nullptr;
     int *d_block_sums = nullptr;
+    icy_dev::GrainConst *d_grain = nullptr;   // failure-surface constants per grain slot
     int scan_blocks = 0;
     unsigned *d_flags = nullptr;
     unsigned long long *d_moved = nullptr;
@@ -84,3 +85,4 @@ int icy_phase_update(icy_mpm *h, double ind_x, double ind_y);
 int icy_phase_g2p(icy_mpm *h, bool recordPQ);
 int icy_instance_steps(icy_mpm *h, int step0, int nsteps, double *sim_time);
 int icy_instance_bin(icy_mpm *h);
+int icy_instance_constants(icy_mpm *h);

@@ -58,8 +58,15 @@ struct TileArgs {
     unsigned *flags;         // node tiles written by P2G since the last update
     int *status;
     unsigned long long *moved;  // points whose base is not their sorted cell (re-binning hint)
+    const GrainConst *grain_tab;  // failure-surface constants per grain slot
     int record_pq;
 };
+
+__global__ void k_grain_table(StepParams P, GrainConst *tab)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < GRAIN_TAB) tab[s] = grain_constants(P, s / GRAIN_N11 - 29, s % GRAIN_N11 - 10);
+}
 
 __device__ __forceinline__ bool node_in_grid(const StepParams &P, int gx, int gy)
 {
@@ -349,7 +356,11 @@ __device__ __forceinline__ void tile_point(const TileArgs &A, long i, int j, int
         } else {
             double Je;
             compute_pq(F, P.mu, P.kappa, Je, ptr, qtr);
-            if (!(util & kCrushed) && failure_surface_crushed(P, (short)util, ptr, qtr)) util |= kCrushed;
+            if (!(util & kCrushed)) {
+                const GrainConst *gc = A.grain_tab + grain_slot((short)util);
+                const GrainConst c{__ldg(&gc->pmin2), __ldg(&gc->k), __ldg(&gc->msq)};
+                if (failure_surface_crushed_tab(P, c, ptr, qtr)) util |= kCrushed;
+            }
             if (util & kCrushed) return_map(P, F, Jp, ptr, qtr, Je);
         }
         pts[i] = __longlong_as_double(util);
@@ -553,8 +564,10 @@ __global__ void __launch_bounds__(256) k_update_nodes(StepParams P, TileGeom G, 
     for (int k = threadIdx.x; k < 2 * P.nsub; k += blockDim.x) s_acc[k] = 0;
     __syncthreads();
     bool any = false;
-    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n_nodes; q += (long)gridDim.x * blockDim.x) {
-        const int gx = (int)(q / g.ny) - g.halo, gy = (int)(q % g.ny);
+    const int nn = (int)n_nodes;   // < 2^31 nodes per instance
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nn; q += gridDim.x * blockDim.x) {
+        const int col = q / g.ny;
+        const int gx = col - g.halo, gy = q - col * g.ny;
         if (!flags[(gy / TY) * G.ntx + (gx + g.halo) / TX]) continue;
         double vx = 0, vy = 0, fx, fy;
         int bin;

@@ -84,6 +84,48 @@ __device__ __forceinline__ void compute_pq(const M2<T> &F, T mu, T kappa, T &Je,
     q = ((T(kCoeff1) * mu) * (T(1) / Je)) * sqrt_t(sq);
 }
 
+// Grain-dependent constants of the failure surface.  GetParametersForGrain
+// (kernels.cuh:560-576) varies them with (grain+3) % 30 and (grain+4) % 11
+// only, so they take 59 x 21 distinct values (C++ remainders of a signed
+// 16-bit grain id lie in [-29, 29] and [-10, 10]); a per-instance table of
+// the exact same expressions replaces 3 divisions and a square root per point.
+constexpr int GRAIN_N30 = 59, GRAIN_N11 = 21, GRAIN_TAB = GRAIN_N30 * GRAIN_N11;
+struct GrainConst { double pmin2, k, msq; };
+
+__device__ __forceinline__ GrainConst grain_constants(const StepParams &P, int r30, int r11)
+{
+    double var2 = 1.0 + P.grain_var * 0.033 * (double)(-15 + r30);
+    double var3 = 1.0 + P.grain_var * 0.1 * (double)(-10 + r11);
+    double pmax = P.pmax, pmin = -P.pmin_t;
+    double qmax = P.qmax_s * var3;
+    double pmin2 = -P.t2 * var2;
+    double beta = P.beta;
+    GrainConst c;
+    c.msq = (4 * qmax * qmax * (1 + 2 * beta)) / ((pmax - pmin) * (pmax - pmin));
+    double q0 = 2 * sqrt(-pmax * pmin) * qmax / (pmax - pmin);
+    c.k = -q0 / pmin2;
+    c.pmin2 = pmin2;
+    return c;
+}
+
+__device__ __forceinline__ int grain_slot(int grain)
+{
+    return ((grain + 3) % 30 + 29) * GRAIN_N11 + ((grain + 4) % 11 + 10);
+}
+
+// CheckIfPointIsInsideFailureSurface with the grain constants looked up (kernels.cuh:598-619)
+__device__ __forceinline__ bool failure_surface_crushed_tab(const StepParams &P, const GrainConst &c, double p,
+                                                            double q)
+{
+    if (p < 0) {
+        if (p < c.pmin2) return true;
+        double q_limit = c.k * (p - c.pmin2);
+        return q > q_limit;
+    }
+    double y = (1. + 2. * P.beta) * q * q + c.msq * (p + P.beta * P.pmax) * (p - P.pmax);
+    return y > 0;
+}
+
 // GetParametersForGrain + CheckIfPointIsInsideFailureSurface (kernels.cuh:560-619)
 __device__ __forceinline__ bool failure_surface_crushed(const StepParams &P, int grain, double p, double q)
 {
