@@ -95,6 +95,8 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(cudaFuncSetAttribute(k_tile<false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TILE_DYN_SMEM));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile<true, true, false>, TILE_THREADS, TILE_DYN_SMEM));
     h->tile_grid = std::max(1, sms * std::max(per_sm, 1));
+    CK(cudaFuncSetAttribute(k_tile_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PIPE_SMEM));
+    h->pipe_grid = sms;
     h->update_grid = (int)std::max(1L, std::min((h->n_nodes + 255) / 256, (long)sms * 16));
     if (int rc = icy_instance_constants(h)) return rc;
     CK(cudaStreamSynchronize(h->stream));
@@ -219,7 +221,7 @@ static int launch_tile(icy_mpm *h, int which, bool record)
     switch (which) {
     case 0:
         icy_prof_begin(h, K_TILE_G2P2G);
-        k_tile<true, true, false><<<h->tile_grid, TILE_THREADS, TILE_DYN_SMEM, h->stream>>>(A);
+        k_tile_pipe<<<h->pipe_grid, PIPE_THREADS, PIPE_SMEM, h->stream>>>(A);
         break;
     case 1:
         icy_prof_begin(h, K_TILE_P2G);

@@ -21,6 +21,7 @@
 // memory beyond it; such points are counted so the host can re-bin.
 #pragma once
 #include "kernels_simple.cuh"
+#include "tma_pipe.cuh"
 
 namespace icy_dev {
 
@@ -29,10 +30,8 @@ constexpr int RM = 1;                          // drift margin (cells) of the st
 constexpr int RX = TX + 2 + 2 * RM, RY = TY + 2 + 2 * RM, RN = RX * RY;
 constexpr int TILE_THREADS = 256;
 constexpr int CAP = 640;                       // points staged per chunk
-constexpr int NMOM = 9;                        // P2G moments per point
 constexpr int BASE_NONE = 0x7fffffff;
-constexpr size_t TILE_DYN_SMEM = sizeof(double) * NMOM * CAP + sizeof(int) * CAP;
-static_assert(27 * TT <= NMOM * CAP, "cell partials alias the moment buffer");
+constexpr int ICY_TIMEOUT_CODE = 108;          // ICY_ERR_TIMEOUT
 
 // Tiles cover bases bx in [-halo, -halo + ntx*TX), by in [0, nty*TY);
 // tile id = ty*ntx + tx; cell key = tile*TT + lx*TY + ly; node tiles use the
@@ -281,133 +280,238 @@ __device__ __noinline__ void p2g_global(GridView g, unsigned *flags, int ntx, in
     flags[t1y * ntx + t1x] = 1u;
 }
 
-// ---------------------------------------------------------------- phase 1
-// G2P + return mapping of point i (if DO_G2P) and its P2G moments (if DO_P2G)
-// into slot j of the shared moment buffer.
-template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
-__device__ __forceinline__ void tile_point(const TileArgs &A, long i, int j, int RX0, int RY0,
-                                           const double (*s_v)[RN], double *s_mom, int *s_base)
+// ---------------------------------------------------------------- per point
+// State of one point during G2P (HSSOA fields) plus its p, q on record steps.
+struct PointState {
+    long long util;
+    double x, y, Jp, vx, vy, ptr, qtr;
+    M2<double> F, B;
+};
+
+// G2P + return mapping of one point (simulation/kernels.cuh:305-407).
+// vsrc(bx, by, a, b, nvx, nvy) supplies node velocities.  Returns false (and
+// records the reference's error code) if the stencil leaves the grid.
+template <typename VSrc>
+__device__ __forceinline__ bool g2p_update(const StepParams &P, const GrainConst *grain_tab, PointState &s,
+                                           int *status, VSrc &&vsrc)
 {
-    const StepParams &P = A.P;
-    double *__restrict__ pts = A.pts;
-    const long pitch = A.pitch;
-    long long util = __double_as_longlong(pts[i]);
-    if (util & kDisabled) {
-        if (DO_P2G) s_base[j] = BASE_NONE;
+    const int bx = (int)(s.x * P.hinv - 0.5), by = (int)(s.y * P.hinv - 0.5);
+    const double fx = s.x * P.hinv - (double)bx, fy = s.y * P.hinv - (double)by;
+    const int e = base_error(P, bx, by);
+    if (e) { *status = e; return false; }
+    double wx[3], wy[3];
+    bspline_weights(fx, wx);
+    bspline_weights(fy, wy);
+    double vx = 0, vy = 0;
+    M2<double> B{0, 0, 0, 0};
+    const double s4 = 4. * P.hinv;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const double d0 = (double)a - fx;
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const double d1 = (double)b - fy;
+            const double w = wx[a] * wy[b];
+            double nvx, nvy;
+            vsrc(bx, by, a, b, nvx, nvy);
+            vx = vx + w * nvx;
+            vy = vy + w * nvy;
+            const double sw = s4 * w;
+            const double snx = sw * nvx, sny = sw * nvy;
+            B.a00 = B.a00 + snx * d0; B.a01 = B.a01 + snx * d1;
+            B.a10 = B.a10 + sny * d0; B.a11 = B.a11 + sny * d1;
+        }
+    }
+    s.x = s.x + vx * P.dt;
+    s.y = s.y + vy * P.dt;
+    const M2<double> Am{1.0 + P.dt * B.a00, P.dt * B.a01, P.dt * B.a10, 1.0 + P.dt * B.a11};
+    const M2<double> F = s.F;
+    s.F = {Am.a00 * F.a00 + Am.a01 * F.a10, Am.a00 * F.a01 + Am.a01 * F.a11,
+           Am.a10 * F.a00 + Am.a11 * F.a10, Am.a10 * F.a01 + Am.a11 * F.a11};
+    s.ptr = 0;
+    s.qtr = 0;
+    if (s.util & kLiquid) {
+        s.Jp = s.Jp * (Am.a00 * Am.a11 - Am.a10 * Am.a01);
+    } else {
+        double Je;
+        compute_pq(s.F, P.mu, P.kappa, Je, s.ptr, s.qtr);
+        if (!(s.util & kCrushed)) {
+            const GrainConst *gc = grain_tab + grain_slot((short)s.util);
+            const GrainConst c{__ldg(&gc->pmin2), __ldg(&gc->k), __ldg(&gc->msq)};
+            if (failure_surface_crushed_tab(P, c, s.ptr, s.qtr)) s.util |= kCrushed;
+        }
+        if (s.util & kCrushed) return_map(P, s.F, s.Jp, s.ptr, s.qtr, Je);
+    }
+    s.vx = vx;
+    s.vy = vy;
+    s.B = B;
+    return true;
+}
+
+__device__ __forceinline__ void store_point(double *__restrict__ pts, long pitch, long i, const PointState &s,
+                                            bool write_vb, bool record_pq)
+{
+    pts[i] = __longlong_as_double(s.util);
+    pts[i + pitch * 3] = s.Jp;
+    pts[i + pitch * 4] = s.x;
+    pts[i + pitch * 5] = s.y;
+    pts[i + pitch * 8] = s.F.a00; pts[i + pitch * 9] = s.F.a01;
+    pts[i + pitch * 10] = s.F.a10; pts[i + pitch * 11] = s.F.a11;
+    if (write_vb) {
+        pts[i + pitch * 6] = s.vx; pts[i + pitch * 7] = s.vy;
+        pts[i + pitch * 12] = s.B.a00; pts[i + pitch * 13] = s.B.a01;
+        pts[i + pitch * 14] = s.B.a10; pts[i + pitch * 15] = s.B.a11;
+    }
+    if (record_pq) { pts[i + pitch * 1] = s.ptr; pts[i + pitch * 2] = s.qtr; }
+}
+
+// Shared buffer of P2G moments, one column per staged point, padded by one
+// slot every 16 points so that cell threads reading points ~4 apart hit
+// distinct banks.  After phase 2 the same buffer holds the cell partials.
+constexpr int NMOM = 10;                          // fx, fy, m, m*vx, m*vy, S00, S01, S10, S11, base
+constexpr int CAP_P = CAP + CAP / 16;
+constexpr size_t MOM_BYTES = sizeof(double) * NMOM * CAP_P;
+static_assert(27 * TT <= NMOM * CAP_P, "cell partials alias the moment buffer");
+__device__ __forceinline__ int mom_idx(int k, int j) { return k * CAP_P + j + (j >> 4); }
+constexpr size_t TILE_DYN_SMEM = MOM_BYTES;
+
+// P2G moments of a point (simulation/kernels.cuh:57-92) into column j.
+__device__ __forceinline__ void p2g_moments(const StepParams &P, const PointState &s, double *mom, int j,
+                                            int *status)
+{
+    const bool liquid = (s.util & kLiquid) != 0;
+    const double mass = liquid ? P.mass_water : P.mass_ice;
+    const int bx = (int)(s.x * P.hinv - 0.5), by = (int)(s.y * P.hinv - 0.5);
+    const int e = base_error(P, bx, by);
+    if (e) {
+        *status = e;
+        mom[mom_idx(9, j)] = __longlong_as_double((long long)BASE_NONE);
         return;
     }
-    const bool liquid = (util & kLiquid) != 0;
-    double x = pts[i + pitch * 4], y = pts[i + pitch * 5];
-    M2<double> F{pts[i + pitch * 8], pts[i + pitch * 9], pts[i + pitch * 10], pts[i + pitch * 11]};
-    double Jp = pts[i + pitch * 3];
-    double vx, vy;
-    M2<double> B;
-    if (DO_G2P) {
-        const int bx = (int)(x * P.hinv - 0.5), by = (int)(y * P.hinv - 0.5);
-        const double fx = x * P.hinv - (double)bx, fy = y * P.hinv - (double)by;
-        const int e = base_error(P, bx, by);
-        if (e) {
-            *A.status = e;
-            if (DO_P2G) s_base[j] = BASE_NONE;
-            return;
+    const M2<double> tau = liquid ? water_stress(s.Jp, P.kappa) : kirchhoff(s.F, P.mu, P.kappa);
+    mom[mom_idx(0, j)] = s.x * P.hinv - (double)bx;
+    mom[mom_idx(1, j)] = s.y * P.hinv - (double)by;
+    mom[mom_idx(2, j)] = mass;
+    mom[mom_idx(3, j)] = s.vx * mass;
+    mom[mom_idx(4, j)] = s.vy * mass;
+    mom[mom_idx(5, j)] = mass * s.B.a00 - P.dt_vol_Dpinv * tau.a00;
+    mom[mom_idx(6, j)] = mass * s.B.a01 - P.dt_vol_Dpinv * tau.a01;
+    mom[mom_idx(7, j)] = mass * s.B.a10 - P.dt_vol_Dpinv * tau.a10;
+    mom[mom_idx(8, j)] = mass * s.B.a11 - P.dt_vol_Dpinv * tau.a11;
+    mom[mom_idx(9, j)] = __longlong_as_double((long long)pack_base(bx, by));
+}
+
+__device__ __forceinline__ void mom_none(double *mom, int j)
+{
+    mom[mom_idx(9, j)] = __longlong_as_double((long long)BASE_NONE);
+}
+
+// Phases 2 and 3 for one chunk of points [cs, ce) of tile (tx, ty): cell
+// threads (tid < TT) sum their points' contributions in registers, then every
+// region node adds its 9 cell partials in a fixed order plus the off-cell
+// contributions and flushes to the global grid.  `sync` is a barrier over
+// the NT participating threads.
+template <int NT, typename Sync>
+__device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, int tx, int ty, int cs, int ce,
+                                                    const int *s_cs, double *mom, double (*s_odd)[RN],
+                                                    unsigned &touch, unsigned &moved, Sync &&sync)
+{
+    const StepParams &P = A.P;
+    const int X0 = tx * TX - P.halo, Y0 = ty * TY;
+    const int RX0 = X0 - RM, RY0 = Y0 - RM;
+    double acc[27];
+#pragma unroll
+    for (int q = 0; q < 27; q++) acc[q] = 0;
+    if (tid < TT) {
+        const int bxc = X0 + tid / TY, byc = Y0 + tid % TY;
+        const int r0 = max(s_cs[tid], cs) - cs, r1 = min(s_cs[tid + 1], ce) - cs;
+        for (int j = r0; j < r1; j++) {
+            const int pb = (int)__double_as_longlong(mom[mom_idx(9, j)]);
+            if (pb == BASE_NONE) continue;
+            int bx, by;
+            unpack_base(pb, bx, by);
+            const double fx = mom[mom_idx(0, j)], fy = mom[mom_idx(1, j)], mass = mom[mom_idx(2, j)];
+            const double mvx = mom[mom_idx(3, j)], mvy = mom[mom_idx(4, j)];
+            const double s00 = mom[mom_idx(5, j)], s01 = mom[mom_idx(6, j)];
+            const double s10 = mom[mom_idx(7, j)], s11 = mom[mom_idx(8, j)];
+            if (bx == bxc && by == byc) {
+                point_contributions(P.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
+                                    [&](int a, int b, double dm, double dpx, double dpy) {
+                                        const int q = (a * 3 + b) * 3;
+                                        acc[q] += dm;
+                                        acc[q + 1] += dpx;
+                                        acc[q + 2] += dpy;
+                                    });
+            } else {
+                moved++;
+                const int lx = bx - RX0, ly = by - RY0;
+                if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
+                    point_contributions(P.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
+                                        [&](int a, int b, double dm, double dpx, double dpy) {
+                                            const int k = (lx + a) * RY + (ly + b);
+                                            atomicAdd(&s_odd[0][k], dm);
+                                            atomicAdd(&s_odd[1][k], dpx);
+                                            atomicAdd(&s_odd[2][k], dpy);
+                                        });
+                } else {
+                    p2g_global(A.g, A.flags, A.G.ntx, P.halo, P.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01, s10,
+                               s11);
+                }
+            }
         }
-        double wx[3], wy[3];
-        bspline_weights(fx, wx);
-        bspline_weights(fy, wy);
-        vx = 0; vy = 0;
-        B = {0, 0, 0, 0};
-        const int lx = bx - RX0, ly = by - RY0;
-        const bool staged = lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY;
-        const double s4 = 4. * P.hinv;
+    }
+    sync();   // all moments read: the buffer becomes the cell partials
+    if (tid < TT) {
+#pragma unroll
+        for (int q = 0; q < 27; q++) mom[q * TT + tid] = acc[q];
+    }
+    sync();
+    for (int k = tid; k < RN; k += NT) {
+        const int i = k / RY, jj = k % RY;        // region coordinates
+        const int nx = i - RM, ny = jj - RM;       // node relative to the tile's first base
+        double m = 0, px = 0, py = 0;
 #pragma unroll
         for (int a = 0; a < 3; a++) {
-            const double d0 = (double)a - fx;
+            const int cx = nx - a;
+            if (cx < 0 || cx >= TX) continue;
 #pragma unroll
             for (int b = 0; b < 3; b++) {
-                const double d1 = (double)b - fy;
-                const double w = wx[a] * wy[b];
-                double nvx, nvy;
-                if (staged) {
-                    const int k = (lx + a) * RY + (ly + b);
-                    nvx = s_v[0][k];
-                    nvy = s_v[1][k];
-                } else {
-                    const long k = A.g.idx(bx + a, by + b);
-                    nvx = A.g.vx[k];
-                    nvy = A.g.vy[k];
-                }
-                vx = vx + w * nvx;
-                vy = vy + w * nvy;
-                const double s = s4 * w;
-                const double snx = s * nvx, sny = s * nvy;
-                B.a00 = B.a00 + snx * d0; B.a01 = B.a01 + snx * d1;
-                B.a10 = B.a10 + sny * d0; B.a11 = B.a11 + sny * d1;
+                const int cy = ny - b;
+                if (cy < 0 || cy >= TY) continue;
+                const int c = cx * TY + cy, q = (a * 3 + b) * 3;
+                m += mom[q * TT + c];
+                px += mom[(q + 1) * TT + c];
+                py += mom[(q + 2) * TT + c];
             }
         }
-        x = x + vx * P.dt;
-        y = y + vy * P.dt;
-        const M2<double> Am{1.0 + P.dt * B.a00, P.dt * B.a01, P.dt * B.a10, 1.0 + P.dt * B.a11};
-        const M2<double> Fn{Am.a00 * F.a00 + Am.a01 * F.a10, Am.a00 * F.a01 + Am.a01 * F.a11,
-                            Am.a10 * F.a00 + Am.a11 * F.a10, Am.a10 * F.a01 + Am.a11 * F.a11};
-        F = Fn;
-        double ptr = 0, qtr = 0;
-        if (liquid) {
-            Jp = Jp * (Am.a00 * Am.a11 - Am.a10 * Am.a01);
-        } else {
-            double Je;
-            compute_pq(F, P.mu, P.kappa, Je, ptr, qtr);
-            if (!(util & kCrushed)) {
-                const GrainConst *gc = A.grain_tab + grain_slot((short)util);
-                const GrainConst c{__ldg(&gc->pmin2), __ldg(&gc->k), __ldg(&gc->msq)};
-                if (failure_surface_crushed_tab(P, c, ptr, qtr)) util |= kCrushed;
-            }
-            if (util & kCrushed) return_map(P, F, Jp, ptr, qtr, Je);
+        m += s_odd[0][k]; px += s_odd[1][k]; py += s_odd[2][k];
+        s_odd[0][k] = 0; s_odd[1][k] = 0; s_odd[2][k] = 0;
+        if (m != 0.0 || px != 0.0 || py != 0.0) {
+            const int gx = RX0 + i, gy = RY0 + jj;   // inside the grid: only valid bases scatter
+            const long q = A.g.idx(gx, gy);
+            atomicAdd(A.g.m + q, m);
+            atomicAdd(A.g.px + q, px);
+            atomicAdd(A.g.py + q, py);
+            const int dx = (gx + P.halo) / TX - tx + 1, dy = gy / TY - ty + 1;
+            touch |= 1u << (dy * 3 + dx);
         }
-        pts[i] = __longlong_as_double(util);
-        pts[i + pitch * 3] = Jp;
-        pts[i + pitch * 4] = x;
-        pts[i + pitch * 5] = y;
-        pts[i + pitch * 8] = F.a00; pts[i + pitch * 9] = F.a01;
-        pts[i + pitch * 10] = F.a10; pts[i + pitch * 11] = F.a11;
-        if (WRITE_VB) {
-            pts[i + pitch * 6] = vx; pts[i + pitch * 7] = vy;
-            pts[i + pitch * 12] = B.a00; pts[i + pitch * 13] = B.a01;
-            pts[i + pitch * 14] = B.a10; pts[i + pitch * 15] = B.a11;
-        }
-        if (A.record_pq) { pts[i + pitch * 1] = ptr; pts[i + pitch * 2] = qtr; }
-    } else {
-        vx = pts[i + pitch * 6];
-        vy = pts[i + pitch * 7];
-        B = {pts[i + pitch * 12], pts[i + pitch * 13], pts[i + pitch * 14], pts[i + pitch * 15]};
     }
-    if (DO_P2G) {
-        // P2G moments of the (updated) point (simulation/kernels.cuh:57-92)
-        const double mass = liquid ? P.mass_water : P.mass_ice;
-        const M2<double> tau = liquid ? water_stress(Jp, P.kappa) : kirchhoff(F, P.mu, P.kappa);
-        const int bx = (int)(x * P.hinv - 0.5), by = (int)(y * P.hinv - 0.5);
-        const int e = base_error(P, bx, by);
-        if (e) {
-            *A.status = e;
-            s_base[j] = BASE_NONE;
-            return;
-        }
-        s_base[j] = pack_base(bx, by);
-        s_mom[0 * CAP + j] = x * P.hinv - (double)bx;
-        s_mom[1 * CAP + j] = y * P.hinv - (double)by;
-        s_mom[2 * CAP + j] = mass;
-        s_mom[3 * CAP + j] = vx * mass;
-        s_mom[4 * CAP + j] = vy * mass;
-        s_mom[5 * CAP + j] = mass * B.a00 - P.dt_vol_Dpinv * tau.a00;
-        s_mom[6 * CAP + j] = mass * B.a01 - P.dt_vol_Dpinv * tau.a01;
-        s_mom[7 * CAP + j] = mass * B.a10 - P.dt_vol_Dpinv * tau.a10;
-        s_mom[8 * CAP + j] = mass * B.a11 - P.dt_vol_Dpinv * tau.a11;
+    sync();   // partials consumed before the buffer is refilled
+}
+
+__device__ __forceinline__ void mark_node_tiles(const TileArgs &A, int tx, int ty, unsigned touch, int lane9)
+{
+    if (lane9 < 9 && ((touch >> lane9) & 1u)) {
+        const int ntx = tx + lane9 % 3 - 1, nty = ty + lane9 / 3 - 1;
+        A.flags[nty * A.G.ntx + ntx] = 1u;
     }
 }
 
-// One persistent CTA loop over the non-empty tiles.
-//   <true, true, false>  G2P(n) + P2G(n+1)          (steady state of a run)
-//   <false, true, false> P2G only                   (first step, per-phase p2g)
-//   <true, false, true>  G2P only, writes vel & Bp  (last step, per-phase g2p)
+// ---------------------------------------------------------------- plain tile kernel
+// One persistent CTA loop over the non-empty tiles, points read straight from
+// global memory.  Used for the first step of a run (<false, true, false>: P2G
+// only) and the last (<true, false, true>: G2P only, writes vel and Bp), and
+// by the per-phase calls.
 template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
 __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
 {
@@ -415,22 +519,20 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
     __shared__ double s_odd[3][RN];    // contributions of points off their sorted cell
     __shared__ int s_cs[TT + 1];       // cell ranges of the tile
     __shared__ unsigned s_touch;
-    extern __shared__ double s_dyn[];  // moments [NMOM][CAP] | cell partials [27][TT]; then bases [CAP]
-    double *s_mom = s_dyn;
-    int *s_base = reinterpret_cast<int *>(s_dyn + NMOM * CAP);
+    extern __shared__ double s_mom[];  // NMOM x CAP_P moments | 27 x TT cell partials
     const StepParams &P = A.P;
     const int na = *A.n_active;
     const int tid = threadIdx.x;
     unsigned moved = 0;
+    for (int k = tid; k < RN; k += blockDim.x) { s_odd[0][k] = 0; s_odd[1][k] = 0; s_odd[2][k] = 0; }
     for (int ti = blockIdx.x; ti < na; ti += gridDim.x) {
         const int t = A.active[ti];
         const int tx = t % A.G.ntx, ty = t / A.G.ntx;
-        const int X0 = tx * TX - P.halo, Y0 = ty * TY;
-        const int RX0 = X0 - RM, RY0 = Y0 - RM;
+        const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
         for (int c = tid; c <= TT; c += blockDim.x) s_cs[c] = A.cell_start[(long)t * TT + c];
         if (tid == 0) s_touch = 0;
-        for (int k = tid; k < RN; k += blockDim.x) {
-            if (DO_G2P) {
+        if (DO_G2P) {
+            for (int k = tid; k < RN; k += blockDim.x) {
                 const int gx = RX0 + k / RY, gy = RY0 + k % RY;
                 double vx = 0, vy = 0;
                 if (node_in_grid(P, gx, gy)) {
@@ -441,109 +543,61 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
                 s_v[0][k] = vx;
                 s_v[1][k] = vy;
             }
-            if (DO_P2G) { s_odd[0][k] = 0; s_odd[1][k] = 0; s_odd[2][k] = 0; }
         }
         __syncthreads();
         const int ps = s_cs[0], pe = s_cs[TT];
-        if (!DO_P2G) {
-            for (int i = ps + tid; i < pe; i += blockDim.x)
-                tile_point<DO_G2P, DO_P2G, WRITE_VB>(A, i, 0, RX0, RY0, s_v, s_mom, s_base);
-            __syncthreads();
-            continue;
-        }
+        auto vsrc = [&](int bx, int by, int a, int b, double &nvx, double &nvy) {
+            const int lx = bx - RX0, ly = by - RY0;
+            if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
+                const int k = (lx + a) * RY + (ly + b);
+                nvx = s_v[0][k];
+                nvy = s_v[1][k];
+            } else {
+                const long k = A.g.idx(bx + a, by + b);
+                nvx = A.g.vx[k];
+                nvy = A.g.vy[k];
+            }
+        };
+        unsigned touch = 0;
         for (int cs = ps; cs < pe; cs += CAP) {
             const int ce = min(cs + CAP, pe);
-            // phase 1: one thread per point
-            for (int j = tid; j < ce - cs; j += blockDim.x)
-                tile_point<DO_G2P, DO_P2G, WRITE_VB>(A, cs + j, j, RX0, RY0, s_v, s_mom, s_base);
-            __syncthreads();
-            // phase 2: one thread per cell, partials in registers
-            double acc[27];
-#pragma unroll
-            for (int q = 0; q < 27; q++) acc[q] = 0;
-            if (tid < TT) {
-                const int bxc = X0 + tid / TY, byc = Y0 + tid % TY;
-                const int r0 = max(s_cs[tid], cs) - cs, r1 = min(s_cs[tid + 1], ce) - cs;
-                for (int j = r0; j < r1; j++) {
-                    const int pb = s_base[j];
-                    if (pb == BASE_NONE) continue;
-                    int bx, by;
-                    unpack_base(pb, bx, by);
-                    const double fx = s_mom[j], fy = s_mom[CAP + j], mass = s_mom[2 * CAP + j];
-                    const double mvx = s_mom[3 * CAP + j], mvy = s_mom[4 * CAP + j];
-                    const double s00 = s_mom[5 * CAP + j], s01 = s_mom[6 * CAP + j];
-                    const double s10 = s_mom[7 * CAP + j], s11 = s_mom[8 * CAP + j];
-                    if (bx == bxc && by == byc) {
-                        point_contributions(P.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
-                                            [&](int a, int b, double dm, double dpx, double dpy) {
-                                                const int q = (a * 3 + b) * 3;
-                                                acc[q] += dm;
-                                                acc[q + 1] += dpx;
-                                                acc[q + 2] += dpy;
-                                            });
-                    } else {
-                        moved++;
-                        const int lx = bx - RX0, ly = by - RY0;
-                        if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
-                            point_contributions(P.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
-                                                [&](int a, int b, double dm, double dpx, double dpy) {
-                                                    const int k = (lx + a) * RY + (ly + b);
-                                                    atomicAdd(&s_odd[0][k], dm);
-                                                    atomicAdd(&s_odd[1][k], dpx);
-                                                    atomicAdd(&s_odd[2][k], dpy);
-                                                });
-                        } else {
-                            p2g_global(A.g, A.flags, A.G.ntx, P.halo, P.h, bx, by, fx, fy, mass, mvx, mvy, s00,
-                                       s01, s10, s11);
-                        }
-                    }
+            for (int j = tid; j < ce - cs; j += blockDim.x) {
+                const long i = cs + j;
+                PointState s;
+                s.util = __double_as_longlong(A.pts[i]);
+                if (s.util & kDisabled) {
+                    if (DO_P2G) mom_none(s_mom, j);
+                    continue;
                 }
-            }
-            __syncthreads();   // all moments read: the buffer becomes the cell partials
-            if (tid < TT) {
-#pragma unroll
-                for (int q = 0; q < 27; q++) s_mom[q * TT + tid] = acc[q];
+                const long pitch = A.pitch;
+                s.x = A.pts[i + pitch * 4];
+                s.y = A.pts[i + pitch * 5];
+                s.Jp = A.pts[i + pitch * 3];
+                s.F = {A.pts[i + pitch * 8], A.pts[i + pitch * 9], A.pts[i + pitch * 10], A.pts[i + pitch * 11]};
+                if (DO_G2P) {
+                    if (!g2p_update(P, A.grain_tab, s, A.status, vsrc)) {
+                        if (DO_P2G) mom_none(s_mom, j);
+                        continue;
+                    }
+                    store_point(A.pts, pitch, i, s, WRITE_VB, A.record_pq != 0);
+                } else {
+                    s.vx = A.pts[i + pitch * 6];
+                    s.vy = A.pts[i + pitch * 7];
+                    s.B = {A.pts[i + pitch * 12], A.pts[i + pitch * 13], A.pts[i + pitch * 14],
+                           A.pts[i + pitch * 15]};
+                }
+                if (DO_P2G) p2g_moments(P, s, s_mom, j, A.status);
             }
             __syncthreads();
-            // phase 3: one thread per region node, 9 partials in a fixed order, flush
-            unsigned touch = 0;
-            for (int k = tid; k < RN; k += blockDim.x) {
-                const int i = k / RY, jj = k % RY;        // region coordinates
-                const int nx = i - RM, ny = jj - RM;       // node relative to the tile's first base
-                double m = 0, px = 0, py = 0;
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    const int cx = nx - a;
-                    if (cx < 0 || cx >= TX) continue;
-#pragma unroll
-                    for (int b = 0; b < 3; b++) {
-                        const int cy = ny - b;
-                        if (cy < 0 || cy >= TY) continue;
-                        const int c = cx * TY + cy, q = (a * 3 + b) * 3;
-                        m += s_mom[q * TT + c];
-                        px += s_mom[(q + 1) * TT + c];
-                        py += s_mom[(q + 2) * TT + c];
-                    }
-                }
-                m += s_odd[0][k]; px += s_odd[1][k]; py += s_odd[2][k];
-                s_odd[0][k] = 0; s_odd[1][k] = 0; s_odd[2][k] = 0;
-                if (m != 0.0 || px != 0.0 || py != 0.0) {
-                    const int gx = RX0 + i, gy = RY0 + jj;   // inside the grid: only valid bases scatter
-                    const long q = A.g.idx(gx, gy);
-                    atomicAdd(A.g.m + q, m);
-                    atomicAdd(A.g.px + q, px);
-                    atomicAdd(A.g.py + q, py);
-                    const int dx = (gx + P.halo) / TX - tx + 1, dy = gy / TY - ty + 1;
-                    touch |= 1u << (dy * 3 + dx);
-                }
-            }
+            if (DO_P2G)
+                p2g_cells_and_flush<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_mom, s_odd, touch, moved,
+                                                  [] { __syncthreads(); });
+        }
+        if (DO_P2G) {
             touch = __reduce_or_sync(0xffffffffu, touch);
             if ((tid & 31) == 0 && touch) atomicOr(&s_touch, touch);
             __syncthreads();
-        }
-        if (tid < 9 && ((s_touch >> tid) & 1u)) {
-            const int ntx = tx + tid % 3 - 1, nty = ty + tid / 3 - 1;
-            A.flags[nty * A.G.ntx + ntx] = 1u;
+            mark_node_tiles(A, tx, ty, s_touch, tid);
         }
         __syncthreads();
     }
@@ -551,6 +605,176 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
         moved = __reduce_add_sync(0xffffffffu, moved);
         if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
     }
+}
+
+// ---------------------------------------------------------------- pipelined fused kernel
+// G2P(n) + P2G(n+1) with the point stream fed by bulk copies: warp PIPE_CONS/32
+// (the producer) walks the same chunk sequence as the consumers and, for each
+// chunk, loads the tile's node velocities and cell ranges with plain loads and
+// the chunk's 8 state lines with cp.async.bulk into one of NSTAGE ring slots;
+// the 8 consumer warps compute from shared memory and write the new state to
+// global memory.  One CTA per SM.
+constexpr int PIPE_CONS = 256, PIPE_THREADS = PIPE_CONS + 32, NSTAGE = 2;
+constexpr int NLINE = 8;                          // utility, Jp, x, y, Fe00..Fe11
+constexpr int LINE_CAP = CAP + 2;                 // slack for 16-byte alignment of the copy
+static_assert((LINE_CAP * sizeof(double)) % 16 == 0, "16-byte aligned staged lines");
+__device__ __constant__ const int kPipeLines[NLINE] = {0, 3, 4, 5, 8, 9, 10, 11};
+constexpr long PIPE_WAIT_LIMIT = 1L << 26;        // polls before a wait gives up
+
+struct PipeSmem {
+    double line[NSTAGE][NLINE][LINE_CAP];        // staged point lines
+    double v[NSTAGE][2][RN];                     // staged node velocities
+    int cs[NSTAGE][TT + 1];                      // staged cell ranges
+    int meta[NSTAGE][4];                         // tile, cs, ce, first aligned index
+    double mom[NMOM * CAP_P];                    // moments | cell partials
+    double odd[3][RN];
+    unsigned long long full[NSTAGE], empty[NSTAGE];
+    unsigned touch;
+    int abort;
+};
+constexpr size_t PIPE_SMEM = sizeof(PipeSmem) + 128;
+
+__global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(TileArgs A)
+{
+    extern __shared__ unsigned char s_raw[];
+    PipeSmem &S = *reinterpret_cast<PipeSmem *>((reinterpret_cast<uintptr_t>(s_raw) + 127) & ~uintptr_t(127));
+    const StepParams &P = A.P;
+    const int tid = threadIdx.x;
+    const int na = *A.n_active;
+    if (tid == 0) {
+        for (int s = 0; s < NSTAGE; s++) {
+            mbar_init(reinterpret_cast<uint64_t *>(&S.full[s]), 1);
+            mbar_init(reinterpret_cast<uint64_t *>(&S.empty[s]), 1);
+        }
+        mbar_init_fence();
+        S.touch = 0;
+        S.abort = 0;
+    }
+    for (int k = tid; k < RN; k += PIPE_THREADS) { S.odd[0][k] = 0; S.odd[1][k] = 0; S.odd[2][k] = 0; }
+    __syncthreads();
+
+    if (tid >= PIPE_CONS) {
+        // ------------------------------------------------ producer warp
+        const int lane = tid - PIPE_CONS;
+        int c = 0;
+        bool ok = true;
+        for (int ti = blockIdx.x; ti < na && ok; ti += gridDim.x) {
+            const int t = A.active[ti];
+            const int ps = A.cell_start[(long)t * TT], pe = A.cell_start[(long)(t + 1) * TT];
+            const int tx = t % A.G.ntx, ty = t / A.G.ntx;
+            const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
+            for (int cs = ps; cs < pe; cs += CAP, c++) {
+                const int st = c % NSTAGE, use = c / NSTAGE;
+                if (use > 0 && !mbar_wait(reinterpret_cast<uint64_t *>(&S.empty[st]), (use - 1) & 1,
+                                          PIPE_WAIT_LIMIT)) {
+                    *A.status = ICY_TIMEOUT_CODE;
+                    ok = false;
+                    break;
+                }
+                fence_proxy_async_smem();
+                const int ce = min(cs + CAP, pe);
+                const int a0 = cs & ~1, a1 = (ce + 1) & ~1;
+                for (int k = lane; k < RN; k += 32) {
+                    const int gx = RX0 + k / RY, gy = RY0 + k % RY;
+                    double vx = 0, vy = 0;
+                    if (node_in_grid(P, gx, gy)) {
+                        const long q = A.g.idx(gx, gy);
+                        vx = A.g.vx[q];
+                        vy = A.g.vy[q];
+                    }
+                    S.v[st][0][k] = vx;
+                    S.v[st][1][k] = vy;
+                }
+                for (int k = lane; k <= TT; k += 32) S.cs[st][k] = A.cell_start[(long)t * TT + k];
+                if (lane == 0) {
+                    S.meta[st][0] = t;
+                    S.meta[st][1] = cs;
+                    S.meta[st][2] = ce;
+                    S.meta[st][3] = a0;
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    const uint32_t bytes = (uint32_t)((a1 - a0) * sizeof(double));
+                    uint64_t *bar = reinterpret_cast<uint64_t *>(&S.full[st]);
+                    mbar_arrive_expect_tx(bar, bytes * NLINE);
+                    for (int l = 0; l < NLINE; l++)
+                        bulk_g2s(&S.line[st][l][0], A.pts + A.pitch * kPipeLines[l] + a0, bytes, bar);
+                }
+                __syncwarp();
+            }
+        }
+        // on a timeout, wait (bounded) for this warp's copies still in flight
+        if (!ok && lane == 0)
+            for (int k = max(0, c - NSTAGE); k < c; k++)
+                mbar_wait(reinterpret_cast<uint64_t *>(&S.full[k % NSTAGE]), (k / NSTAGE) & 1, PIPE_WAIT_LIMIT);
+        return;
+    }
+
+    // ---------------------------------------------------- consumer warps
+    unsigned moved = 0;
+    int c = 0;
+    unsigned touch = 0;
+    auto csync = [] { consumer_sync<PIPE_CONS>(); };
+    bool ok = true;
+    for (int ti = blockIdx.x; ti < na && ok; ti += gridDim.x) {
+        const int t = A.active[ti];
+        const int ps = A.cell_start[(long)t * TT], pe = A.cell_start[(long)(t + 1) * TT];
+        const int tx = t % A.G.ntx, ty = t / A.G.ntx;
+        const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
+        touch = 0;
+        for (int cs = ps; cs < pe; cs += CAP, c++) {
+            const int st = c % NSTAGE, use = c / NSTAGE;
+            // the decision to give up is made CTA-uniform through S.abort
+            if (!mbar_wait(reinterpret_cast<uint64_t *>(&S.full[st]), use & 1, PIPE_WAIT_LIMIT)) {
+                *A.status = ICY_TIMEOUT_CODE;
+                S.abort = 1;
+            }
+            csync();
+            if (S.abort) { ok = false; break; }
+            const int ce = S.meta[st][2], off = cs - S.meta[st][3];
+            const double(*sv)[RN] = S.v[st];
+            auto vsrc = [&](int bx, int by, int a, int b, double &nvx, double &nvy) {
+                const int lx = bx - RX0, ly = by - RY0;
+                if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
+                    const int k = (lx + a) * RY + (ly + b);
+                    nvx = sv[0][k];
+                    nvy = sv[1][k];
+                } else {
+                    const long k = A.g.idx(bx + a, by + b);
+                    nvx = A.g.vx[k];
+                    nvy = A.g.vy[k];
+                }
+            };
+            // phase 1: one thread per point, state from the staged lines
+            for (int j = tid; j < ce - cs; j += PIPE_CONS) {
+                const int q = off + j;
+                PointState s;
+                s.util = __double_as_longlong(S.line[st][0][q]);
+                if (s.util & kDisabled) { mom_none(S.mom, j); continue; }
+                s.Jp = S.line[st][1][q];
+                s.x = S.line[st][2][q];
+                s.y = S.line[st][3][q];
+                s.F = {S.line[st][4][q], S.line[st][5][q], S.line[st][6][q], S.line[st][7][q]};
+                if (!g2p_update(P, A.grain_tab, s, A.status, vsrc)) { mom_none(S.mom, j); continue; }
+                store_point(A.pts, A.pitch, cs + j, s, false, A.record_pq != 0);
+                p2g_moments(P, s, S.mom, j, A.status);
+            }
+            csync();
+            p2g_cells_and_flush<PIPE_CONS>(A, tid, tx, ty, cs, ce, S.cs[st], S.mom, S.odd, touch, moved, csync);
+            // the stage (lines, velocities, cell ranges) is no longer read: release it
+            if (tid == 0) mbar_arrive(reinterpret_cast<uint64_t *>(&S.empty[st]));
+        }
+        if (!ok) break;
+        touch = __reduce_or_sync(0xffffffffu, touch);
+        if ((tid & 31) == 0 && touch) atomicOr(&S.touch, touch);
+        csync();
+        const unsigned tt = S.touch;
+        csync();
+        if (tid == 0) S.touch = 0;
+        mark_node_tiles(A, tx, ty, tt, tid);
+    }
+    moved = __reduce_add_sync(0xffffffffu, moved);
+    if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
 }
 
 // Grid update of the nodes of marked tiles (simulation/kernels.cuh:164-301),
