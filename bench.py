@@ -208,6 +208,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--opt", action="append", default=[],
+                    help="instance option name=value (icy_mpm_set_option), repeatable")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -225,6 +227,9 @@ def main():
     stream = torch.cuda.Stream(device=local)
     g = GPUImplementation(p, soa, device=local)
     g.set_stream(stream.cuda_stream)
+    for o in args.opt:
+        k, v = o.split("=", 1)
+        g.set_option(k, float(v))
     g.update_constants()
     g.transfer_ponts_to_device()
     g.reset_indenter_force_accumulator()
@@ -305,7 +310,7 @@ def main():
         "config": {"workload": "single large FP64 instance: grid 4096x2048 h=0.05 m, 150x40 m block, 4 ppc, "
                                "dt=2e-5, E=1e9, phi=62, indenter r=1 m at 1 m/s",
                    "points": n, "precision": "fp64", "l2": "inputs larger than L2 (1.23 GB particle state)",
-                   "replicas": world},
+                   "replicas": world, "options": args.opt},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "frame_steps": frame, "downloads": downloads},
         "gpu_launches": int(launches),

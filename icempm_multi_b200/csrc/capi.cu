@@ -239,6 +239,8 @@ int icy_mpm_set_option(icy_mpm *h, const char *name, double value)
     if (k == "resort_every") {
         if (value < 0) return ICY_ERR_INVALID_ARGUMENT;
         h->resort_every = (int)value;
+    } else if (k == "pipe") {
+        h->pipe = value != 0;
     } else if (k == "tiled") {
         h->tiled = value != 0;
         h->primed = false;

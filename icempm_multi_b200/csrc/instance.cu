@@ -221,7 +221,8 @@ static int launch_tile(icy_mpm *h, int which, bool record)
     switch (which) {
     case 0:
         icy_prof_begin(h, K_TILE_G2P2G);
-        k_tile_pipe<<<h->pipe_grid, PIPE_THREADS, PIPE_SMEM, h->stream>>>(A);
+        if (h->pipe) k_tile_pipe<<<h->pipe_grid, PIPE_THREADS, PIPE_SMEM, h->stream>>>(A);
+        else k_tile<true, true, false><<<h->tile_grid, TILE_THREADS, TILE_DYN_SMEM, h->stream>>>(A);
         break;
     case 1:
         icy_prof_begin(h, K_TILE_P2G);

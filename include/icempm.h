@@ -225,6 +225,8 @@ int icy_mpm_status(icy_mpm *h);
  *   "resort_every"  re-bin the points by tile every N steps (0 = only after upload)
  *   "tiled"         1 = binned, tile-staged kernels (default); 0 = one thread per
  *                   point / node, unsorted (the reference's kernel structure)
+ *   "pipe"          1 = the fused step kernel is fed by a producer warp with
+ *                   bulk copies into a shared-memory ring (default 0)
  */
 int icy_mpm_set_option(icy_mpm *h, const char *name, double value);
 

@@ -168,7 +168,8 @@ def run_gpu_opts(p, soa, steps, **opts):
     return out
 
 
-@pytest.mark.parametrize("opts", [{"tiled": 0}, {"tiled": 1, "resort_every": 0}, {"tiled": 1, "resort_every": 3}])
+@pytest.mark.parametrize("opts", [{"tiled": 0}, {"tiled": 1, "resort_every": 0}, {"tiled": 1, "resort_every": 3},
+                                  {"tiled": 1, "pipe": 1}, {"tiled": 1, "pipe": 1, "resort_every": 5}])
 def test_kernel_paths_match_oracle(oracle, opts):
     p, soa = stress(seed=11)
     ref = soa.clone()
