@@ -286,8 +286,6 @@ struct PointState {
     long long util;
     double x, y, Jp, vx, vy, ptr, qtr;
     M2<double> F, B;
-    M2<double> tau;     // Kirchhoff stress of F when has_tau (reused by P2G)
-    bool has_tau;
 };
 
 // G2P + return mapping of one point (simulation/kernels.cuh:305-407).
@@ -332,31 +330,17 @@ __device__ __forceinline__ bool g2p_update(const StepParams &P, const GrainConst
            Am.a10 * F.a00 + Am.a11 * F.a10, Am.a10 * F.a01 + Am.a11 * F.a11};
     s.ptr = 0;
     s.qtr = 0;
-    s.has_tau = false;
     if (s.util & kLiquid) {
         s.Jp = s.Jp * (Am.a00 * Am.a11 - Am.a10 * Am.a01);
     } else {
-        // ComputePQ (kernels.cuh:547-557); det, 1/J and dev(FF^T) are the same
-        // terms KirchhoffStress_Wolper forms (kernels.cuh:30-32), so the
-        // stress of a point the return mapping leaves alone is kept for P2G
-        const double Je = det2(s.F);
-        const double inv = 1.0 / Je;
-        const M2<double> d = dev_ffT(s.F);
-        s.ptr = (-(P.kappa / 2.)) * (Je * Je - 1.);
-        const double sq = ((d.a00 * d.a00 + d.a10 * d.a10) + d.a01 * d.a01) + d.a11 * d.a11;
-        s.qtr = ((kCoeff1 * P.mu) * inv) * sqrt(sq);
+        double Je;
+        compute_pq(s.F, P.mu, P.kappa, Je, s.ptr, s.qtr);   // kernels.cuh:547-557
         if (!(s.util & kCrushed)) {
             const GrainConst *gc = grain_tab + grain_slot((short)s.util);
             const GrainConst c{__ldg(&gc->pmin2), __ldg(&gc->k), __ldg(&gc->msq)};
             if (failure_surface_crushed_tab(P, c, s.ptr, s.qtr)) s.util |= kCrushed;
         }
-        if (s.util & kCrushed) {
-            return_map(P, s.F, s.Jp, s.ptr, s.qtr, Je);
-        } else {
-            const double s1 = P.mu * inv, s2 = (P.kappa * 0.5) * (Je * Je - 1.);
-            s.tau = {s1 * d.a00 + s2, s1 * d.a01, s1 * d.a10, s1 * d.a11 + s2};
-            s.has_tau = true;
-        }
+        if (s.util & kCrushed) return_map(P, s.F, s.Jp, s.ptr, s.qtr, Je);
     }
     s.vx = vx;
     s.vy = vy;
@@ -404,7 +388,7 @@ __device__ __forceinline__ void p2g_moments(const StepParams &P, const PointStat
         mom[mom_idx(9, j)] = __longlong_as_double((long long)BASE_NONE);
         return;
     }
-    const M2<double> tau = liquid ? water_stress(s.Jp, P.kappa) : (s.has_tau ? s.tau : kirchhoff(s.F, P.mu, P.kappa));
+    const M2<double> tau = liquid ? water_stress(s.Jp, P.kappa) : kirchhoff(s.F, P.mu, P.kappa);
     mom[mom_idx(0, j)] = s.x * P.hinv - (double)bx;
     mom[mom_idx(1, j)] = s.y * P.hinv - (double)by;
     mom[mom_idx(2, j)] = mass;
@@ -435,15 +419,14 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
     const StepParams &P = A.P;
     const int X0 = tx * TX - P.halo, Y0 = ty * TY;
     const int RX0 = X0 - RM, RY0 = Y0 - RM;
-    static_assert(NT >= 2 * TT, "two threads per cell");
+    static_assert(NT >= TT, "one thread per cell");
     double acc[27];
 #pragma unroll
     for (int q = 0; q < 27; q++) acc[q] = 0;
-    const int cell = tid >> 1, half = tid & 1;   // threads 2c, 2c+1 share cell c (even / odd points)
-    if (cell < TT) {
-        const int bxc = X0 + cell / TY, byc = Y0 + cell % TY;
-        const int r0 = max(s_cs[cell], cs) - cs, r1 = min(s_cs[cell + 1], ce) - cs;
-        for (int j = r0 + half; j < r1; j += 2) {
+    if (tid < TT) {
+        const int bxc = X0 + tid / TY, byc = Y0 + tid % TY;
+        const int r0 = max(s_cs[tid], cs) - cs, r1 = min(s_cs[tid + 1], ce) - cs;
+        for (int j = r0; j < r1; j++) {
             const int pb = (int)__double_as_longlong(mom[mom_idx(9, j)]);
             if (pb == BASE_NONE) continue;
             int bx, by;
@@ -478,12 +461,10 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
             }
         }
     }
-#pragma unroll
-    for (int q = 0; q < 27; q++) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], 1);
     sync();   // all moments read: the buffer becomes the cell partials
-    if (cell < TT && half == 0) {
+    if (tid < TT) {
 #pragma unroll
-        for (int q = 0; q < 27; q++) mom[q * TT + cell] = acc[q];
+        for (int q = 0; q < 27; q++) mom[q * TT + tid] = acc[q];
     }
     sync();
     for (int k = tid; k < RN; k += NT) {
@@ -601,7 +582,6 @@ __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
                     }
                     store_point(A.pts, pitch, i, s, WRITE_VB, A.record_pq != 0);
                 } else {
-                    s.has_tau = false;
                     s.vx = A.pts[i + pitch * 6];
                     s.vy = A.pts[i + pitch * 7];
                     s.B = {A.pts[i + pitch * 12], A.pts[i + pitch * 13], A.pts[i + pitch * 14],
