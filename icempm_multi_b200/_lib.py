@@ -82,7 +82,7 @@ EXPORTED = [
     "icy_mpm_reset_indenter_force_accumulator", "icy_mpm_indenter_force", "icy_mpm_reset_grid", "icy_mpm_p2g",
     "icy_mpm_receive_halos", "icy_mpm_update_nodes", "icy_mpm_g2p", "icy_mpm_receive_points", "icy_mpm_step",
     "icy_mpm_synchronize", "icy_mpm_status", "icy_mpm_kernel_launches", "icy_version", "icy_last_error",
-    "icy_mpm_profile", "icy_mpm_profile_read", "icy_mpm_set_option",
+    "icy_mpm_profile", "icy_mpm_profile_read", "icy_mpm_set_option", "icy_step_noalloc",
 ]
 
 _lib = None
@@ -129,6 +129,7 @@ def lib():
         "icy_mpm_profile": (C.c_int, [vp, C.c_int]),
         "icy_mpm_set_option": (C.c_int, [vp, C.c_char_p, C.c_double]),
         "icy_mpm_profile_read": (C.c_int, [vp, C.c_int, C.c_char_p, vp, vp, C.POINTER(C.c_int)]),
+        "icy_step_noalloc": (C.c_int, [P, vp, C.c_uint, C.c_uint, C.c_int, C.c_int, dp, vp, vp]),
         "icy_version": (C.c_char_p, []),
         "icy_last_error": (C.c_char_p, []),
     }

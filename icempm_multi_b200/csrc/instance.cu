@@ -353,3 +353,47 @@ int icy_instance_steps(icy_mpm *h, int step0, int nsteps, double *sim_time)
     *sim_time = t;
     return ICY_OK;
 }
+
+// ---------------------------------------------------------------- launch helpers
+// The one-thread-per-item kernels on caller-supplied buffers, for entry points
+// defined in other translation units (icy_step_noalloc in noalloc.cu).  grid
+// holds five arrays of n_nodes doubles: m, px, py, vx, vy.
+static GridView raw_grid_view(double *grid, long n_nodes, int ny, int halo)
+{
+    GridView g;
+    g.m = grid;
+    g.px = grid + n_nodes;
+    g.py = grid + 2 * n_nodes;
+    g.vx = grid + 3 * n_nodes;
+    g.vy = grid + 4 * n_nodes;
+    g.ny = ny;
+    g.halo = halo;
+    return g;
+}
+
+cudaError_t icy_launch_p2g_simple(cudaStream_t s, const StepParams &P, const double *pts, long pitch, int n,
+                                  double *grid, long n_nodes, int *status)
+{
+    if (n > 0)
+        k_p2g_simple<<<(n + 255) / 256, 256, 0, s>>>(P, pts, pitch, n, raw_grid_view(grid, n_nodes, P.gridy, P.halo),
+                                                     status);
+    return cudaGetLastError();
+}
+
+cudaError_t icy_launch_update_simple(cudaStream_t s, const StepParams &P, double *grid, long n_nodes, double ind_x,
+                                     double ind_y, double *acc)
+{
+    const long nb = (n_nodes + 255) / 256;
+    k_update_simple<<<(unsigned)nb, 256, sizeof(double) * 2 * P.nsub, s>>>(
+        P, raw_grid_view(grid, n_nodes, P.gridy, P.halo), n_nodes, ind_x, ind_y, acc);
+    return cudaGetLastError();
+}
+
+cudaError_t icy_launch_g2p_simple(cudaStream_t s, const StepParams &P, double *pts, long pitch, int n, double *grid,
+                                  long n_nodes, int recordPQ, int *status)
+{
+    if (n > 0)
+        k_g2p_simple<<<(n + 127) / 128, 128, 0, s>>>(P, pts, pitch, n, raw_grid_view(grid, n_nodes, P.gridy, P.halo),
+                                                     recordPQ, status);
+    return cudaGetLastError();
+}

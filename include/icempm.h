@@ -247,6 +247,37 @@ int icy_mpm_profile(icy_mpm *h, int enable);
 int icy_mpm_profile_read(icy_mpm *h, int max, char *names, double *ms_total,
                          int64_t *launches, int *count);
 
+/* ------------------------------------------------------------------ */
+/* stepping without allocation                                          */
+/* ------------------------------------------------------------------ */
+/*
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- e.g. a plug-in inside a host framework that owns all device
+ * memory through its own pool and forbids cudaMalloc / cudaFree (which may
+ * synchronise the device), or code on a latency-critical path that must not
+ * allocate after start-up.  Runs nsteps sub-steps of icy::Model::Step
+ * (simulation/model.cpp:38-54) on a particle buffer the caller keeps in
+ * device memory: d_hssoa holds the 16 HSSOA lines with a line stride of
+ * `pitch` doubles and n points, and is updated in place in its own order.
+ * d_indenter_bins (2*n_indenter_subdivisions doubles in device memory, or
+ * NULL) accumulates the indenter force.  Work is queued on `stream` (NULL =
+ * the default stream); the call then synchronises that stream and returns
+ * the device error code (0, or the reference's 70..73).
+ *
+ * It allocates nothing: the grid (5 arrays of GridY*(GridX+2*halo) doubles)
+ * and the status word live in one file-scope device array of
+ * ICY_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * exit.  Grids that need more return ICY_ERR_CAPACITY (icy_last_error says
+ * how much was needed); the limit allows about 838,000 grid nodes.  The
+ * first call on each device resolves the array's device address, so make
+ * that first call before any stream capture.  All calls share the array and
+ * each clears what must start at zero; calls that overlap on the GPU race.
+ */
+#define ICY_NOALLOC_SCRATCH_BYTES (32u << 20)
+int icy_step_noalloc(const icy_sim_params *p, double *d_hssoa, unsigned pitch, unsigned n,
+                     int step0, int nsteps, double *sim_time, double *d_indenter_bins,
+                     void *stream);
+
 /* Library build description, e.g. "icempm_b200 sm_100a". */
 const char *icy_version(void);
 /* Text of the last error recorded on the calling thread ("" if none). */
