@@ -40,6 +40,9 @@ ALG_BYTES = {"k_p2g_simple": 13 * 8, "k_g2p_simple": (8 + 14) * 8,
              # read once and written once; vel and Bp are not stored between steps
              "k_tile_g2p2g": (8 + 8) * 8,
              "k_tile_p2g": 14 * 8, "k_tile_g2p": (8 + 14) * 8}
+# FP32 split state: 4-byte utility, packed cell, offset (2), Fe - I (4), Jp = 9 words
+# read and written by the fused step
+ALG_BYTES_F32 = {"k_tile_g2p2g": (9 + 9) * 4, "k_tile_p2g": 15 * 4, "k_tile_g2p": (9 + 15) * 4}
 
 
 def make_workload(pinned):
@@ -208,6 +211,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                    help="fp64: the plain drop-in path; fp32: split precision")
     ap.add_argument("--opt", action="append", default=[],
                     help="instance option name=value (icy_mpm_set_option), repeatable")
     args = ap.parse_args()
@@ -225,7 +230,9 @@ def main():
     p, soa = make_workload(pinned=True)
     n = soa.size
     stream = torch.cuda.Stream(device=local)
-    g = GPUImplementation(p, soa, device=local)
+    from icempm_multi_b200._lib import PRECISION_FP32_SPLIT, PRECISION_FP64
+    prec = PRECISION_FP32_SPLIT if args.precision == "fp32" else PRECISION_FP64
+    g = GPUImplementation(p, soa, device=local, precision=prec)
     g.set_stream(stream.cuda_stream)
     for o in args.opt:
         k, v = o.split("=", 1)
@@ -293,7 +300,7 @@ def main():
     dom = max(prof.items(), key=lambda kv: kv[1][0]) if prof else (None, (0, 0))
     name, (tot_ms, cnt) = dom
     per_launch_ms = tot_ms / max(cnt, 1)
-    alg = ALG_BYTES.get(name, 0) * n
+    alg = (ALG_BYTES_F32 if args.precision == "fp32" else ALG_BYTES).get(name, 0) * n
     achieved = alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
@@ -306,10 +313,11 @@ def main():
     out = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "single large FP64 instance: grid 4096x2048 h=0.05 m, 150x40 m block, 4 ppc, "
+        "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
+        "config": {"workload": "single large instance: grid 4096x2048 h=0.05 m, 150x40 m block, 4 ppc, "
                                "dt=2e-5, E=1e9, phi=62, indenter r=1 m at 1 m/s",
-                   "points": n, "precision": "fp64", "l2": "inputs larger than L2 (1.23 GB particle state)",
+                   "points": n, "precision": args.precision,
+                   "l2": "inputs larger than L2 (particle state 0.65-1.23 GB)",
                    "replicas": world, "options": args.opt},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "frame_steps": frame, "downloads": downloads},

@@ -5,7 +5,7 @@
 #include <algorithm>
 
 #include "instance.cuh"
-#include "kernels_tiled.cuh"
+#include "kernels_split.cuh"
 
 using namespace icy_dev;
 
@@ -44,7 +44,7 @@ static cudaError_t dalloc(T **p, size_t count)
 
 int icy_instance_allocate(icy_mpm *h, unsigned capacity)
 {
-    if (h->precision != ICY_PRECISION_FP64) return ICY_ERR_NOT_SUPPORTED;
+    const bool split = h->precision == ICY_PRECISION_FP32_SPLIT;
     CK(cudaSetDevice(h->device));
     CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     h->stream = h->own_stream;
@@ -55,14 +55,37 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     h->ntx = (nx + TX - 1) / TX;
     h->nty = (h->prm.GridY + TY - 1) / TY;
     h->ntiles = h->ntx * h->nty;
+    if (nx > 32767 || h->prm.GridY > 32767) return ICY_ERR_INVALID_ARGUMENT;   // packed 16-bit base/cell indices
     cudaError_t e;
-    if ((e = dalloc(&h->d_pts, 16 * h->pitch)) != cudaSuccess || (e = dalloc(&h->d_pts_alt, 16 * h->pitch)) != cudaSuccess) {
-        icy_set_error("cudaMalloc(particles)", e);
-        return ICY_ERR_OUT_OF_MEMORY;
-    }
-    if ((e = dalloc(&h->d_grid, 5 * h->n_nodes)) != cudaSuccess) {
-        icy_set_error("cudaMalloc(grid)", e);
-        return ICY_ERR_OUT_OF_MEMORY;
+    if (split) {
+        // FP32 state (two buffers for the binning permutation), FP32 grid,
+        // FP64 staging for the HSSOA conversion at upload/download
+        h->stage_n = std::min<long>(h->pitch, 1L << 20);
+        if ((e = dalloc(&h->d_st, S_NLINES * h->pitch)) != cudaSuccess ||
+            (e = dalloc(&h->d_st_alt, S_NLINES * h->pitch)) != cudaSuccess ||
+            (e = dalloc(&h->d_stage, 16 * h->stage_n)) != cudaSuccess) {
+            icy_set_error("cudaMalloc(particles)", e);
+            return ICY_ERR_OUT_OF_MEMORY;
+        }
+        if ((e = dalloc(&h->d_gridf, 5 * h->n_nodes)) != cudaSuccess) {
+            icy_set_error("cudaMalloc(grid)", e);
+            return ICY_ERR_OUT_OF_MEMORY;
+        }
+        CK(cudaMalloc(&h->d_grainf, sizeof(GrainConstF) * GRAIN_TAB));
+        CK(cudaMemsetAsync(h->d_st, 0, sizeof(unsigned) * S_NLINES * h->pitch, h->stream));
+        CK(cudaMemsetAsync(h->d_gridf, 0, sizeof(float) * 5 * h->n_nodes, h->stream));
+    } else {
+        if ((e = dalloc(&h->d_pts, 16 * h->pitch)) != cudaSuccess ||
+            (e = dalloc(&h->d_pts_alt, 16 * h->pitch)) != cudaSuccess) {
+            icy_set_error("cudaMalloc(particles)", e);
+            return ICY_ERR_OUT_OF_MEMORY;
+        }
+        if ((e = dalloc(&h->d_grid, 5 * h->n_nodes)) != cudaSuccess) {
+            icy_set_error("cudaMalloc(grid)", e);
+            return ICY_ERR_OUT_OF_MEMORY;
+        }
+        CK(cudaMemsetAsync(h->d_pts, 0, sizeof(double) * 16 * h->pitch, h->stream));
+        CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 5 * h->n_nodes, h->stream));
     }
     CK(dalloc(&h->d_oidx, h->pitch));
     CK(dalloc(&h->d_oidx_alt, h->pitch));
@@ -81,8 +104,6 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(dalloc(&h->d_status, 1));
     CK(dalloc(&h->d_grain, GRAIN_TAB));
     CK(cudaMallocHost(&h->h_status, sizeof(int)));
-    CK(cudaMemsetAsync(h->d_pts, 0, sizeof(double) * 16 * h->pitch, h->stream));
-    CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 5 * h->n_nodes, h->stream));
     CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
     CK(cudaMemsetAsync(h->d_nactive, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_moved, 0, sizeof(unsigned long long), h->stream));
@@ -97,6 +118,10 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     h->tile_grid = std::max(1, sms * std::max(per_sm, 1));
     CK(cudaFuncSetAttribute(k_tile_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PIPE_SMEM));
     h->pipe_grid = sms;
+    per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false>, TILE_THREADS,
+                                                     MOMF_BYTES));
+    h->tile_grid_f32 = std::max(1, sms * std::max(per_sm, 1));
     h->update_grid = (int)std::max(1L, std::min((h->n_nodes + 255) / 256, (long)sms * 16));
     if (int rc = icy_instance_constants(h)) return rc;
     CK(cudaStreamSynchronize(h->stream));
@@ -110,8 +135,13 @@ void icy_instance_free(icy_mpm *h)
     if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->d_pts, h->d_pts_alt, h->d_grid, h->d_oidx, h->d_oidx_alt, h->d_keys, h->d_ranks,
                     h->d_counts, h->d_start, h->d_active, h->d_nactive, h->d_flags, h->d_moved, h->d_acc,
-                    h->d_status, h->d_block_sums, h->d_grain};
+                    h->d_status, h->d_block_sums, h->d_grain, h->d_st, h->d_st_alt, h->d_stage, h->d_gridf,
+                    h->d_grainf};
     for (void *p : ptrs) cudaFree(p);
+    h->d_st = h->d_st_alt = nullptr;
+    h->d_stage = nullptr;
+    h->d_gridf = nullptr;
+    h->d_grainf = nullptr;
     cudaFreeHost(h->h_status);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     h->d_pts = h->d_pts_alt = h->d_grid = h->d_acc = nullptr;
@@ -123,12 +153,25 @@ void icy_instance_free(icy_mpm *h)
     h->own_stream = h->stream = nullptr;
 }
 
+static bool is_split(const icy_mpm *h) { return h->precision == ICY_PRECISION_FP32_SPLIT; }
+
 int icy_instance_upload(icy_mpm *h, const double *hssoa, unsigned cap, unsigned size)
 {
-    // one 2-D copy: 16 lines of `size` doubles, host line stride = cap
-    if (size)
+    if (is_split(h)) {
+        // FP64 HSSOA -> FP32 state, in chunks through the staging buffer
+        for (long a = 0; a < (long)size; a += h->stage_n) {
+            const long cnt = std::min<long>(h->stage_n, (long)size - a);
+            CK(cudaMemcpy2DAsync(h->d_stage, sizeof(double) * h->stage_n, hssoa + a, sizeof(double) * cap,
+                                 sizeof(double) * cnt, 16, cudaMemcpyHostToDevice, h->stream));
+            k_split_from_hssoa<<<(unsigned)((cnt + 255) / 256), 256, 0, h->stream>>>(
+                h->d_stage, h->stage_n, (int)cnt, h->d_st, h->pitch, (int)a, h->prm.cellsize_inv);
+            CK_LAUNCH("k_split_from_hssoa");
+        }
+    } else if (size) {
+        // one 2-D copy: 16 lines of `size` doubles, host line stride = cap
         CK(cudaMemcpy2DAsync(h->d_pts, sizeof(double) * h->pitch, hssoa, sizeof(double) * cap,
                              sizeof(double) * size, 16, cudaMemcpyHostToDevice, h->stream));
+    }
     h->n = size;
     h->binned = false;
     h->permuted = false;
@@ -143,6 +186,24 @@ int icy_instance_upload(icy_mpm *h, const double *hssoa, unsigned cap, unsigned 
 int icy_instance_download(icy_mpm *h, double *hssoa, unsigned cap)
 {
     if (!h->n) return ICY_OK;
+    if (is_split(h)) {
+        // FP32 state -> FP64 HSSOA in upload order, in chunks through the staging buffer
+        const int *inv = nullptr;
+        if (h->permuted) {
+            k_inverse_perm<<<(h->n + 255) / 256, 256, 0, h->stream>>>(h->d_oidx, (int)h->n, h->d_keys);
+            CK_LAUNCH("k_inverse_perm");
+            inv = h->d_keys;
+        }
+        for (long a = 0; a < (long)h->n; a += h->stage_n) {
+            const long cnt = std::min<long>(h->stage_n, (long)h->n - a);
+            k_split_to_hssoa<<<(unsigned)((cnt + 255) / 256), 256, 0, h->stream>>>(
+                h->d_st, h->pitch, inv, (int)a, (int)cnt, h->d_stage, h->stage_n, h->prm.cellsize);
+            CK_LAUNCH("k_split_to_hssoa");
+            CK(cudaMemcpy2DAsync(hssoa + a, sizeof(double) * cap, h->d_stage, sizeof(double) * h->stage_n,
+                                 sizeof(double) * cnt, 16, cudaMemcpyDeviceToHost, h->stream));
+        }
+        return ICY_OK;
+    }
     const double *src = h->d_pts;
     if (h->permuted) {
         icy_prof_begin(h, K_UNPERMUTE);
@@ -167,8 +228,12 @@ int icy_instance_bin(icy_mpm *h)
     const int nkeys = h->ntiles * TT + 1;
     icy_prof_begin(h, K_BIN);
     CK(cudaMemsetAsync(h->d_counts, 0, sizeof(int) * nkeys, h->stream));
-    k_bin_count<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_pts, h->pitch, (int)h->n, h->d_keys, h->d_ranks,
-                                           h->d_counts, h->d_status);
+    if (is_split(h))
+        k_bin_count_f32<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_st, h->pitch, (int)h->n, h->d_keys,
+                                                   h->d_ranks, h->d_counts, h->d_status);
+    else
+        k_bin_count<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_pts, h->pitch, (int)h->n, h->d_keys,
+                                               h->d_ranks, h->d_counts, h->d_status);
     CK_LAUNCH("k_bin_count");
     k_scan_reduce<<<h->scan_blocks, SCAN_NT, 0, h->stream>>>(h->d_counts, nkeys, h->d_block_sums);
     CK_LAUNCH("k_scan_reduce");
@@ -178,11 +243,17 @@ int icy_instance_bin(icy_mpm *h)
     CK_LAUNCH("k_scan_apply");
     k_tiles_active<<<1, 1024, 0, h->stream>>>(h->d_start, h->ntiles, h->d_active, h->d_nactive);
     CK_LAUNCH("k_tiles_active");
-    k_bin_scatter<<<nb, 256, 0, h->stream>>>(h->d_pts, h->d_pts_alt, h->pitch, (int)h->n, h->d_keys, h->d_ranks,
-                                             h->d_start, h->d_oidx, h->d_oidx_alt);
+    if (is_split(h)) {
+        k_bin_scatter_f32<<<nb, 256, 0, h->stream>>>(h->d_st, h->d_st_alt, h->pitch, (int)h->n, h->d_keys,
+                                                     h->d_ranks, h->d_start, h->d_oidx, h->d_oidx_alt);
+        std::swap(h->d_st, h->d_st_alt);
+    } else {
+        k_bin_scatter<<<nb, 256, 0, h->stream>>>(h->d_pts, h->d_pts_alt, h->pitch, (int)h->n, h->d_keys,
+                                                 h->d_ranks, h->d_start, h->d_oidx, h->d_oidx_alt);
+        std::swap(h->d_pts, h->d_pts_alt);
+    }
     CK_LAUNCH("k_bin_scatter");
     icy_prof_end(h);
-    std::swap(h->d_pts, h->d_pts_alt);
     std::swap(h->d_oidx, h->d_oidx_alt);
     h->binned = true;
     h->permuted = true;
@@ -209,6 +280,61 @@ static TileArgs tile_args(icy_mpm *h, bool record)
     return A;
 }
 
+static GridViewF grid_view_f32(icy_mpm *h)
+{
+    GridViewF g;
+    g.m = h->d_gridf;
+    g.px = h->d_gridf + h->n_nodes;
+    g.py = h->d_gridf + 2 * h->n_nodes;
+    g.vx = h->d_gridf + 3 * h->n_nodes;
+    g.vy = h->d_gridf + 4 * h->n_nodes;
+    g.ny = h->prm.GridY;
+    g.halo = h->prm.GridHaloSize;
+    return g;
+}
+
+static SplitArgs split_args(icy_mpm *h, bool record)
+{
+    SplitArgs A;
+    A.P = icy_step_params(h->prm);
+    A.Q = split_consts(A.P);
+    A.G = tile_geom(h);
+    A.g = grid_view_f32(h);
+    A.st = h->d_st;
+    A.pitch = h->pitch;
+    A.cell_start = h->d_start;
+    A.active = h->d_active;
+    A.n_active = h->d_nactive;
+    A.flags = h->d_flags;
+    A.status = h->d_status;
+    A.moved = h->d_moved;
+    A.grain_tab = static_cast<const GrainConstF *>(h->d_grainf);
+    A.record_pq = record ? 1 : 0;
+    return A;
+}
+
+static int launch_tile_split(icy_mpm *h, int which, bool record)
+{
+    SplitArgs A = split_args(h, record);
+    switch (which) {
+    case 0:
+        icy_prof_begin(h, K_TILE_G2P2G);
+        k_tile_f32<true, true, false><<<h->tile_grid_f32, TILE_THREADS, MOMF_BYTES, h->stream>>>(A);
+        break;
+    case 1:
+        icy_prof_begin(h, K_TILE_P2G);
+        k_tile_f32<false, true, false><<<h->tile_grid_f32, TILE_THREADS, MOMF_BYTES, h->stream>>>(A);
+        break;
+    default:
+        icy_prof_begin(h, K_TILE_G2P);
+        k_tile_f32<true, false, true><<<h->tile_grid_f32, TILE_THREADS, 0, h->stream>>>(A);
+        break;
+    }
+    icy_prof_end(h);
+    CK_LAUNCH("k_tile_f32");
+    return ICY_OK;
+}
+
 // which: 0 = G2P+P2G, 1 = P2G only, 2 = G2P only (writes vel and Bp)
 static int launch_tile(icy_mpm *h, int which, bool record)
 {
@@ -217,6 +343,7 @@ static int launch_tile(icy_mpm *h, int which, bool record)
         int rc = icy_instance_bin(h);
         if (rc) return rc;
     }
+    if (is_split(h)) return launch_tile_split(h, which, record);
     TileArgs A = tile_args(h, record);
     switch (which) {
     case 0:
@@ -242,8 +369,12 @@ static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y)
 {
     StepParams P = icy_step_params(h->prm);
     icy_prof_begin(h, K_UPDATE_TILES);
-    k_update_nodes<<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
-        P, tile_geom(h), grid_view(h), h->d_flags, h->n_nodes, ind_x, ind_y, h->d_acc);
+    if (is_split(h))
+        k_update_nodes_f32<<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
+            P, split_consts(P), tile_geom(h), grid_view_f32(h), h->d_flags, h->n_nodes, ind_x, ind_y, h->d_acc);
+    else
+        k_update_nodes<<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
+            P, tile_geom(h), grid_view(h), h->d_flags, h->n_nodes, ind_x, ind_y, h->d_acc);
     icy_prof_end(h);
     CK_LAUNCH("k_update_nodes");
     CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
@@ -255,15 +386,21 @@ int icy_instance_constants(icy_mpm *h)
 {
     k_grain_table<<<(GRAIN_TAB + 255) / 256, 256, 0, h->stream>>>(icy_step_params(h->prm), h->d_grain);
     CK_LAUNCH("k_grain_table");
+    if (is_split(h)) {
+        k_grain_table_f32<<<(GRAIN_TAB + 255) / 256, 256, 0, h->stream>>>(h->d_grain,
+                                                                        static_cast<GrainConstF *>(h->d_grainf));
+        CK_LAUNCH("k_grain_table_f32");
+    }
     return ICY_OK;
 }
 
 int icy_phase_reset_grid(icy_mpm *h)
 {
     icy_prof_begin(h, K_MEMSET_GRID);
-    CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 3 * h->n_nodes, h->stream));
+    if (is_split(h)) CK(cudaMemsetAsync(h->d_gridf, 0, sizeof(float) * 3 * h->n_nodes, h->stream));
+    else CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 3 * h->n_nodes, h->stream));
     icy_prof_end(h);
-    if (h->tiled) CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
+    if (h->tiled || is_split(h)) CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
     h->primed = false;
     return ICY_OK;
 }
@@ -271,7 +408,7 @@ int icy_phase_reset_grid(icy_mpm *h)
 int icy_phase_p2g(icy_mpm *h)
 {
     if (!h->n) return ICY_OK;
-    if (h->tiled) return launch_tile(h, 1, false);
+    if (h->tiled || is_split(h)) return launch_tile(h, 1, false);
     StepParams P = icy_step_params(h->prm);
     const int tpb = 256;
     icy_prof_begin(h, K_P2G_SIMPLE);
@@ -284,7 +421,7 @@ int icy_phase_p2g(icy_mpm *h)
 
 int icy_phase_update(icy_mpm *h, double ind_x, double ind_y)
 {
-    if (h->tiled) return launch_update_tiles(h, ind_x, ind_y);
+    if (h->tiled || is_split(h)) return launch_update_tiles(h, ind_x, ind_y);
     StepParams P = icy_step_params(h->prm);
     const int tpb = 256;
     const long nb = (h->n_nodes + tpb - 1) / tpb;
@@ -300,7 +437,7 @@ int icy_phase_g2p(icy_mpm *h, bool recordPQ)
 {
     if (!h->n) return ICY_OK;
     h->primed = false;
-    if (h->tiled) return launch_tile(h, 2, recordPQ);
+    if (h->tiled || is_split(h)) return launch_tile(h, 2, recordPQ);
     StepParams P = icy_step_params(h->prm);
     const int tpb = 128;
     icy_prof_begin(h, K_G2P_SIMPLE);
@@ -316,7 +453,7 @@ int icy_instance_steps(icy_mpm *h, int step0, int nsteps, double *sim_time)
     double t = *sim_time;
     const icy_sim_params &p = h->prm;
     int rc;
-    if (!h->tiled) {
+    if (!h->tiled && !is_split(h)) {
         for (int k = 0; k < nsteps; k++) {
             // icy::Model::Step sub-step (simulation/model.cpp:40-49)
             t += p.InitialTimeStep;

@@ -31,6 +31,16 @@ struct icy_mpm {
     int *d_oidx = nullptr, *d_oidx_alt = nullptr, *d_keys = nullptr, *d_ranks = nullptr;
     int *d_counts = nullptr, *d_start = nullptr, *d_active = nullptr, *d_nactive = nullptr;
     int *d_block_sums = nullptr;
+
+    // FP32 split-precision state (precision == ICY_PRECISION_FP32_SPLIT):
+    // 17 lines of 4-byte words per point, an FP32 grid, FP64 staging for the
+    // HSSOA conversion
+    unsigned *d_st = nullptr, *d_st_alt = nullptr;
+    double *d_stage = nullptr;
+    long stage_n = 0;
+    float *d_gridf = nullptr;
+    void *d_grainf = nullptr;
+    int tile_grid_f32 = 0;
     icy_dev::GrainConst *d_grain = nullptr;   // failure-surface constants per grain slot
     int scan_blocks = 0;
     unsigned *d_flags = nullptr;

@@ -1,0 +1,664 @@
+// kernels_split.cuh -- FP32 "split precision" variant of the tiled step.
+//
+// Device state per point (17 lines of 4 bytes, `pitch` entries each):
+//   utility (low 32 bits of the reference's 64-bit word), packed integer cell
+//   (cx + 32768) << 16 | cy, FP32 offset inside the cell (ox, oy in [0,1)),
+//   FP32 De = Fe - I, Jp, then vx, vy, Bp (4), P, Q.
+// Positions as integer cell + FP32 offset keep ~1e-8 cells of resolution on
+// any grid; holding Fe - I instead of Fe keeps full FP32 precision of the
+// small elastic strain, and det(Fe) - 1 and dev(Fe Fe^T) are formed from De
+// without cancellation.  Grid mass and momentum are FP32.  FP64 is kept for
+// the return mapping of crushed points (the projected Fe is formed in FP64
+// and stored back as Fe - I, so nearly equal singular values lose nothing)
+// and for the indenter force bins.  The tiling, sorting and the three phases
+// are those of the FP64 kernels in kernels_tiled.cuh.
+#pragma once
+#include "kernels_tiled.cuh"
+
+namespace icy_dev {
+
+enum SplitLine {
+    S_UTIL = 0, S_CELL, S_OX, S_OY, S_D00, S_D01, S_D10, S_D11, S_JP,
+    S_VX, S_VY, S_B00, S_B01, S_B10, S_B11, S_P, S_Q, S_NLINES
+};
+
+struct GrainConstF { float pmin2, k, msq; };
+
+// FP32 copies of the per-step constants
+struct SplitConsts {
+    float h, hinv, dt, dt_hinv, s4, dtvd, dtg, vmax, vmax_sq, mass_ice, mass_water, mu, kappa, beta, pmax;
+};
+
+__host__ __device__ inline SplitConsts split_consts(const StepParams &P)
+{
+    SplitConsts c;
+    c.h = (float)P.h; c.hinv = (float)P.hinv; c.dt = (float)P.dt; c.dt_hinv = (float)(P.dt * P.hinv);
+    c.s4 = (float)(4. * P.hinv); c.dtvd = (float)P.dt_vol_Dpinv; c.dtg = (float)P.dt_gravity;
+    c.vmax = (float)P.vmax; c.vmax_sq = (float)P.vmax_sq;
+    c.mass_ice = (float)P.mass_ice; c.mass_water = (float)P.mass_water;
+    c.mu = (float)P.mu; c.kappa = (float)P.kappa; c.beta = (float)P.beta; c.pmax = (float)P.pmax;
+    return c;
+}
+
+__global__ void k_grain_table_f32(const GrainConst *tab, GrainConstF *out)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < GRAIN_TAB) out[s] = GrainConstF{(float)tab[s].pmin2, (float)tab[s].k, (float)tab[s].msq};
+}
+
+__device__ __forceinline__ unsigned pack_cell(int cx, int cy) { return ((unsigned)(cx + 32768) << 16) | (unsigned)cy; }
+__device__ __forceinline__ void unpack_cell(unsigned k, int &cx, int &cy)
+{
+    cx = (int)(k >> 16) - 32768;
+    cy = (int)(k & 0xffffu);
+}
+
+// Stencil base with the reference's truncation, (int)(x/h - 0.5) (kernels.cuh:90),
+// from cell c and offset o (x/h = c + o), and the offset f = x/h - base.
+__device__ __forceinline__ void split_base(int c, float o, int &base, float &f)
+{
+    const bool nonneg = c >= 1 || (c == 0 && o >= 0.5f);   // c + o - 0.5 >= 0
+    base = nonneg ? (o >= 0.5f ? c : c - 1) : (o > 0.5f ? c + 1 : c);
+    f = (float)(c - base) + o;
+}
+
+__device__ __forceinline__ void split_renorm(int &c, float &o)
+{
+    if (o >= 1.0f) { c += 1; o -= 1.0f; }
+    else if (o < 0.0f) { c -= 1; o += 1.0f; }
+    if (o >= 1.0f) o = 0.99999994f;   // o = 1 - ulp after rounding
+}
+
+// dev(Fe Fe^T) and J = det Fe from De = Fe - I, without cancellation:
+// Fe Fe^T - I = De + De^T + De De^T, J - 1 = tr De + det De.
+__device__ __forceinline__ void split_dev(const M2<float> &D, float &jm1, float &d00, float &d01)
+{
+    jm1 = (D.a00 + D.a11) + (D.a00 * D.a11 - D.a10 * D.a01);
+    const float b00 = 2.f * D.a00 + D.a00 * D.a00 + D.a01 * D.a01;
+    const float b11 = 2.f * D.a11 + D.a10 * D.a10 + D.a11 * D.a11;
+    d00 = 0.5f * (b00 - b11);
+    d01 = D.a01 + D.a10 + D.a00 * D.a10 + D.a01 * D.a11;
+}
+
+struct PointF {
+    unsigned util;
+    int cx, cy;
+    float ox, oy, Jp, vx, vy, ptr, qtr;
+    M2<float> D, B;
+};
+
+template <typename VSrc>
+__device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitConsts &Q, const GrainConstF *tab,
+                                               PointF &s, int *status, VSrc &&vsrc)
+{
+    int bx, by;
+    float fx, fy;
+    split_base(s.cx, s.ox, bx, fx);
+    split_base(s.cy, s.oy, by, fy);
+    const int e = base_error(P, bx, by);
+    if (e) { *status = e; return false; }
+    float wx[3], wy[3];
+    bspline_weights(fx, wx);
+    bspline_weights(fy, wy);
+    float vx = 0.f, vy = 0.f;
+    M2<float> B{0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float d0 = (float)a - fx;
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const float d1 = (float)b - fy;
+            const float w = wx[a] * wy[b];
+            float nvx, nvy;
+            vsrc(bx, by, a, b, nvx, nvy);
+            vx += w * nvx;
+            vy += w * nvy;
+            const float sw = Q.s4 * w;
+            const float snx = sw * nvx, sny = sw * nvy;
+            B.a00 += snx * d0; B.a01 += snx * d1;
+            B.a10 += sny * d0; B.a11 += sny * d1;
+        }
+    }
+    // advection in cell units, x += v dt (kernels.cuh:375)
+    s.ox += vx * Q.dt_hinv;
+    s.oy += vy * Q.dt_hinv;
+    split_renorm(s.cx, s.ox);
+    split_renorm(s.cy, s.oy);
+    // Fe <- (I + dt Bp) Fe  as  De <- De + T + T De,  T = dt Bp (kernels.cuh:376)
+    const M2<float> T{Q.dt * B.a00, Q.dt * B.a01, Q.dt * B.a10, Q.dt * B.a11};
+    const M2<float> D = s.D;
+    s.D = {D.a00 + T.a00 + (T.a00 * D.a00 + T.a01 * D.a10), D.a01 + T.a01 + (T.a00 * D.a01 + T.a01 * D.a11),
+           D.a10 + T.a10 + (T.a10 * D.a00 + T.a11 * D.a10), D.a11 + T.a11 + (T.a10 * D.a01 + T.a11 * D.a11)};
+    s.ptr = 0.f;
+    s.qtr = 0.f;
+    if (s.util & (unsigned)kLiquid) {
+        s.Jp *= (1.f + T.a00) * (1.f + T.a11) - T.a10 * T.a01;   // kernels.cuh:380
+    } else {
+        // ComputePQ (kernels.cuh:547-557) from De
+        float jm1, d00, d01;
+        split_dev(s.D, jm1, d00, d01);
+        const float Je = 1.f + jm1;
+        s.ptr = -(Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
+        s.qtr = 2.f * Q.mu / Je * sqrtf(d00 * d00 + d01 * d01);   // sqrt(2) mu/J |dev|, |dev| = sqrt(2(d00^2+d01^2))
+        if (!(s.util & (unsigned)kCrushed)) {
+            const GrainConstF *gc = tab + grain_slot((short)s.util);
+            const float pmin2 = __ldg(&gc->pmin2), k = __ldg(&gc->k), msq = __ldg(&gc->msq);
+            bool crushed;
+            if (s.ptr < 0.f) crushed = s.ptr < pmin2 || s.qtr > k * (s.ptr - pmin2);
+            else crushed = (1.f + 2.f * Q.beta) * s.qtr * s.qtr + msq * (s.ptr + Q.beta * Q.pmax) * (s.ptr - Q.pmax) > 0.f;
+            if (crushed) s.util |= (unsigned)kCrushed;
+        }
+        if (s.util & (unsigned)kCrushed) {
+            // return mapping in FP64 (kernels.cuh:540-545, 623-674)
+            M2<double> F{1.0 + (double)s.D.a00, (double)s.D.a01, (double)s.D.a10, 1.0 + (double)s.D.a11};
+            double Jp = s.Jp;
+            double Je64 = det2(F), p64 = (-(P.kappa / 2.)) * (Je64 * Je64 - 1.);
+            M2<double> dv = dev_ffT(F);
+            double q64 = ((kCoeff1 * P.mu) * (1. / Je64)) *
+                         sqrt(((dv.a00 * dv.a00 + dv.a10 * dv.a10) + dv.a01 * dv.a01) + dv.a11 * dv.a11);
+            return_map(P, F, Jp, p64, q64, Je64);
+            s.D = {(float)(F.a00 - 1.0), (float)F.a01, (float)F.a10, (float)(F.a11 - 1.0)};
+            s.Jp = (float)Jp;
+        }
+    }
+    s.vx = vx;
+    s.vy = vy;
+    s.B = B;
+    return true;
+}
+
+__device__ __forceinline__ void store_point_f32(unsigned *__restrict__ st, long pitch, long i, const PointF &s,
+                                                bool write_vb, bool record_pq)
+{
+    float *f = reinterpret_cast<float *>(st);
+    st[i] = s.util;
+    st[i + pitch * S_CELL] = pack_cell(s.cx, s.cy);
+    f[i + pitch * S_OX] = s.ox;
+    f[i + pitch * S_OY] = s.oy;
+    f[i + pitch * S_D00] = s.D.a00; f[i + pitch * S_D01] = s.D.a01;
+    f[i + pitch * S_D10] = s.D.a10; f[i + pitch * S_D11] = s.D.a11;
+    f[i + pitch * S_JP] = s.Jp;
+    if (write_vb) {
+        f[i + pitch * S_VX] = s.vx; f[i + pitch * S_VY] = s.vy;
+        f[i + pitch * S_B00] = s.B.a00; f[i + pitch * S_B01] = s.B.a01;
+        f[i + pitch * S_B10] = s.B.a10; f[i + pitch * S_B11] = s.B.a11;
+    }
+    if (record_pq) { f[i + pitch * S_P] = s.ptr; f[i + pitch * S_Q] = s.qtr; }
+}
+
+__device__ __forceinline__ void load_point_f32(const unsigned *__restrict__ st, long pitch, long i, PointF &s)
+{
+    const float *f = reinterpret_cast<const float *>(st);
+    unpack_cell(st[i + pitch * S_CELL], s.cx, s.cy);
+    s.ox = f[i + pitch * S_OX];
+    s.oy = f[i + pitch * S_OY];
+    s.D = {f[i + pitch * S_D00], f[i + pitch * S_D01], f[i + pitch * S_D10], f[i + pitch * S_D11]};
+    s.Jp = f[i + pitch * S_JP];
+}
+
+// ---------------------------------------------------------------- P2G (FP32)
+constexpr int NMOMF = 10;   // fx, fy, m, m*vx, m*vy, S00, S01, S10, S11, base
+constexpr size_t MOMF_BYTES = sizeof(float) * NMOMF * CAP_P;
+
+__device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const SplitConsts &Q, const PointF &s,
+                                                float *mom, int j, int *status)
+{
+    const bool liquid = (s.util & (unsigned)kLiquid) != 0;
+    const float mass = liquid ? Q.mass_water : Q.mass_ice;
+    int bx, by;
+    float fx, fy;
+    split_base(s.cx, s.ox, bx, fx);
+    split_base(s.cy, s.oy, by, fy);
+    const int e = base_error(P, bx, by);
+    if (e) {
+        *status = e;
+        mom[mom_idx(9, j)] = __int_as_float(BASE_NONE);
+        return;
+    }
+    M2<float> tau;
+    if (liquid) {
+        const float sw = (float)(P.kappa * (1. - pow((double)s.Jp, -5.0)));   // Water (kernels.cuh:37-44)
+        tau = {sw, 0.f, 0.f, sw};
+    } else {
+        // KirchhoffStress_Wolper (kernels.cuh:24-34) from De
+        float jm1, d00, d01;
+        split_dev(s.D, jm1, d00, d01);
+        const float Je = 1.f + jm1;
+        const float s1 = Q.mu / Je, s2 = (Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
+        tau = {s1 * d00 + s2, s1 * d01, s1 * d01, -s1 * d00 + s2};
+    }
+    mom[mom_idx(0, j)] = fx;
+    mom[mom_idx(1, j)] = fy;
+    mom[mom_idx(2, j)] = mass;
+    mom[mom_idx(3, j)] = s.vx * mass;
+    mom[mom_idx(4, j)] = s.vy * mass;
+    mom[mom_idx(5, j)] = mass * s.B.a00 - Q.dtvd * tau.a00;
+    mom[mom_idx(6, j)] = mass * s.B.a01 - Q.dtvd * tau.a01;
+    mom[mom_idx(7, j)] = mass * s.B.a10 - Q.dtvd * tau.a10;
+    mom[mom_idx(8, j)] = mass * s.B.a11 - Q.dtvd * tau.a11;
+    mom[mom_idx(9, j)] = __int_as_float(pack_base(bx, by));
+}
+
+struct GridViewF {
+    float *m, *px, *py, *vx, *vy;
+    int ny, halo;
+    __device__ __forceinline__ long idx(int gx, int gy) const { return (long)(gx + halo) * ny + gy; }
+};
+
+struct SplitArgs {
+    StepParams P;
+    SplitConsts Q;
+    TileGeom G;
+    GridViewF g;
+    unsigned *st;
+    long pitch;
+    const int *cell_start, *active, *n_active;
+    unsigned *flags;
+    int *status;
+    unsigned long long *moved;
+    const GrainConstF *grain_tab;
+    int record_pq;
+};
+
+template <typename Sink>
+__device__ __forceinline__ void point_contributions_f32(float h, float fx, float fy, float mass, float mvx,
+                                                        float mvy, float s00, float s01, float s10, float s11,
+                                                        Sink &&sink)
+{
+    float wx[3], wy[3];
+    bspline_weights(fx, wx);
+    bspline_weights(fy, wy);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float d0 = ((float)a - fx) * h;
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            const float W = wx[a] * wy[b];
+            const float d1 = ((float)b - fy) * h;
+            sink(a, b, W * mass, W * (mvx + (s00 * d0 + s01 * d1)), W * (mvy + (s10 * d0 + s11 * d1)));
+        }
+    }
+}
+
+__device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags, int ntx, int halo, float h, int bx, int by,
+                                            float fx, float fy, float mass, float mvx, float mvy, float s00,
+                                            float s01, float s10, float s11)
+{
+    point_contributions_f32(h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
+                            [&](int a, int b, float dm, float dpx, float dpy) {
+                                const long k = g.idx(bx + a, by + b);
+                                atomicAdd(g.m + k, dm);
+                                atomicAdd(g.px + k, dpx);
+                                atomicAdd(g.py + k, dpy);
+                            });
+    const int t0x = (bx + halo) / TX, t1x = (bx + 2 + halo) / TX;
+    const int t0y = by / TY, t1y = (by + 2) / TY;
+    flags[t0y * ntx + t0x] = 1u;
+    flags[t0y * ntx + t1x] = 1u;
+    flags[t1y * ntx + t0x] = 1u;
+    flags[t1y * ntx + t1x] = 1u;
+}
+
+// phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32
+template <int NT, typename Sync>
+__device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int tid, int tx, int ty, int cs, int ce,
+                                                        const int *s_cs, float *mom, float (*s_odd)[RN],
+                                                        unsigned &touch, unsigned &moved, Sync &&sync)
+{
+    const StepParams &P = A.P;
+    const int X0 = tx * TX - P.halo, Y0 = ty * TY;
+    const int RX0 = X0 - RM, RY0 = Y0 - RM;
+    float acc[27];
+#pragma unroll
+    for (int q = 0; q < 27; q++) acc[q] = 0.f;
+    if (tid < TT) {
+        const int bxc = X0 + tid / TY, byc = Y0 + tid % TY;
+        const int r0 = max(s_cs[tid], cs) - cs, r1 = min(s_cs[tid + 1], ce) - cs;
+        for (int j = r0; j < r1; j++) {
+            const int pb = __float_as_int(mom[mom_idx(9, j)]);
+            if (pb == BASE_NONE) continue;
+            int bx, by;
+            unpack_base(pb, bx, by);
+            const float fx = mom[mom_idx(0, j)], fy = mom[mom_idx(1, j)], mass = mom[mom_idx(2, j)];
+            const float mvx = mom[mom_idx(3, j)], mvy = mom[mom_idx(4, j)];
+            const float s00 = mom[mom_idx(5, j)], s01 = mom[mom_idx(6, j)];
+            const float s10 = mom[mom_idx(7, j)], s11 = mom[mom_idx(8, j)];
+            if (bx == bxc && by == byc) {
+                point_contributions_f32(A.Q.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
+                                        [&](int a, int b, float dm, float dpx, float dpy) {
+                                            const int q = (a * 3 + b) * 3;
+                                            acc[q] += dm;
+                                            acc[q + 1] += dpx;
+                                            acc[q + 2] += dpy;
+                                        });
+            } else {
+                moved++;
+                const int lx = bx - RX0, ly = by - RY0;
+                if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
+                    point_contributions_f32(A.Q.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
+                                            [&](int a, int b, float dm, float dpx, float dpy) {
+                                                const int k = (lx + a) * RY + (ly + b);
+                                                atomicAdd(&s_odd[0][k], dm);
+                                                atomicAdd(&s_odd[1][k], dpx);
+                                                atomicAdd(&s_odd[2][k], dpy);
+                                            });
+                } else {
+                    p2g_global_f32(A.g, A.flags, A.G.ntx, P.halo, A.Q.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01,
+                                   s10, s11);
+                }
+            }
+        }
+    }
+    sync();
+    if (tid < TT) {
+#pragma unroll
+        for (int q = 0; q < 27; q++) mom[q * TT + tid] = acc[q];
+    }
+    sync();
+    for (int k = tid; k < RN; k += NT) {
+        const int i = k / RY, jj = k % RY;
+        const int nx = i - RM, ny = jj - RM;
+        float m = 0.f, px = 0.f, py = 0.f;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const int cx = nx - a;
+            if (cx < 0 || cx >= TX) continue;
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                const int cy = ny - b;
+                if (cy < 0 || cy >= TY) continue;
+                const int c = cx * TY + cy, q = (a * 3 + b) * 3;
+                m += mom[q * TT + c];
+                px += mom[(q + 1) * TT + c];
+                py += mom[(q + 2) * TT + c];
+            }
+        }
+        m += s_odd[0][k]; px += s_odd[1][k]; py += s_odd[2][k];
+        s_odd[0][k] = 0.f; s_odd[1][k] = 0.f; s_odd[2][k] = 0.f;
+        if (m != 0.f || px != 0.f || py != 0.f) {
+            const int gx = RX0 + i, gy = RY0 + jj;
+            const long q = A.g.idx(gx, gy);
+            atomicAdd(A.g.m + q, m);
+            atomicAdd(A.g.px + q, px);
+            atomicAdd(A.g.py + q, py);
+            const int dx = (gx + P.halo) / TX - tx + 1, dy = gy / TY - ty + 1;
+            touch |= 1u << (dy * 3 + dx);
+        }
+    }
+    sync();
+}
+
+// Tile kernel over the FP32 state: <G2P, P2G, write vel/Bp> as k_tile.
+template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
+__global__ void __launch_bounds__(TILE_THREADS, 3) k_tile_f32(SplitArgs A)
+{
+    __shared__ float s_v[2][RN];
+    __shared__ float s_odd[3][RN];
+    __shared__ int s_cs[TT + 1];
+    __shared__ unsigned s_touch;
+    extern __shared__ float s_momf[];
+    const StepParams &P = A.P;
+    const int na = *A.n_active;
+    const int tid = threadIdx.x;
+    unsigned moved = 0;
+    for (int k = tid; k < RN; k += blockDim.x) { s_odd[0][k] = 0.f; s_odd[1][k] = 0.f; s_odd[2][k] = 0.f; }
+    const float *fst = reinterpret_cast<const float *>(A.st);
+    for (int ti = blockIdx.x; ti < na; ti += gridDim.x) {
+        const int t = A.active[ti];
+        const int tx = t % A.G.ntx, ty = t / A.G.ntx;
+        const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
+        for (int c = tid; c <= TT; c += blockDim.x) s_cs[c] = A.cell_start[(long)t * TT + c];
+        if (tid == 0) s_touch = 0;
+        if (DO_G2P) {
+            for (int k = tid; k < RN; k += blockDim.x) {
+                const int gx = RX0 + k / RY, gy = RY0 + k % RY;
+                float vx = 0.f, vy = 0.f;
+                if (node_in_grid(P, gx, gy)) {
+                    const long q = A.g.idx(gx, gy);
+                    vx = A.g.vx[q];
+                    vy = A.g.vy[q];
+                }
+                s_v[0][k] = vx;
+                s_v[1][k] = vy;
+            }
+        }
+        __syncthreads();
+        const int ps = s_cs[0], pe = s_cs[TT];
+        auto vsrc = [&](int bx, int by, int a, int b, float &nvx, float &nvy) {
+            const int lx = bx - RX0, ly = by - RY0;
+            if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
+                const int k = (lx + a) * RY + (ly + b);
+                nvx = s_v[0][k];
+                nvy = s_v[1][k];
+            } else {
+                const long k = A.g.idx(bx + a, by + b);
+                nvx = A.g.vx[k];
+                nvy = A.g.vy[k];
+            }
+        };
+        unsigned touch = 0;
+        for (int cs = ps; cs < pe; cs += CAP) {
+            const int ce = min(cs + CAP, pe);
+            for (int j = tid; j < ce - cs; j += blockDim.x) {
+                const long i = cs + j;
+                PointF s;
+                s.util = A.st[i];
+                if (s.util & (unsigned)kDisabled) {
+                    if (DO_P2G) s_momf[mom_idx(9, j)] = __int_as_float(BASE_NONE);
+                    continue;
+                }
+                load_point_f32(A.st, A.pitch, i, s);
+                if (DO_G2P) {
+                    if (!g2p_update_f32(P, A.Q, A.grain_tab, s, A.status, vsrc)) {
+                        if (DO_P2G) s_momf[mom_idx(9, j)] = __int_as_float(BASE_NONE);
+                        continue;
+                    }
+                    store_point_f32(A.st, A.pitch, i, s, WRITE_VB, A.record_pq != 0);
+                } else {
+                    s.vx = fst[i + A.pitch * S_VX];
+                    s.vy = fst[i + A.pitch * S_VY];
+                    s.B = {fst[i + A.pitch * S_B00], fst[i + A.pitch * S_B01], fst[i + A.pitch * S_B10],
+                           fst[i + A.pitch * S_B11]};
+                }
+                if (DO_P2G) p2g_moments_f32(P, A.Q, s, s_momf, j, A.status);
+            }
+            __syncthreads();
+            if (DO_P2G)
+                p2g_cells_and_flush_f32<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
+                                                      [] { __syncthreads(); });
+        }
+        if (DO_P2G) {
+            touch = __reduce_or_sync(0xffffffffu, touch);
+            if ((tid & 31) == 0 && touch) atomicOr(&s_touch, touch);
+            __syncthreads();
+            if (tid < 9 && ((s_touch >> tid) & 1u)) {
+                const int ntx = tx + tid % 3 - 1, nty = ty + tid / 3 - 1;
+                A.flags[nty * A.G.ntx + ntx] = 1u;
+            }
+        }
+        __syncthreads();
+    }
+    if (DO_P2G) {
+        moved = __reduce_add_sync(0xffffffffu, moved);
+        if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
+    }
+}
+
+// Grid update in FP32 (simulation/kernels.cuh:175-300); the indenter geometry
+// and the force bins in FP64.
+__global__ void __launch_bounds__(256) k_update_nodes_f32(StepParams P, SplitConsts Q, TileGeom G, GridViewF g,
+                                                          const unsigned *__restrict__ flags, long n_nodes,
+                                                          double ind_x, double ind_y, double *acc)
+{
+    extern __shared__ double s_acc[];
+    for (int k = threadIdx.x; k < 2 * P.nsub; k += blockDim.x) s_acc[k] = 0;
+    __syncthreads();
+    bool any = false;
+    const int nn = (int)n_nodes;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nn; q += gridDim.x * blockDim.x) {
+        const int col = q / g.ny;
+        const int gx = col - g.halo, gy = q - col * g.ny;
+        if (!flags[(gy / TY) * G.ntx + (gx + g.halo) / TX]) continue;
+        const float mass = g.m[q];
+        float vx = 0.f, vy = 0.f;
+        if (mass != 0.f) {
+            vx = g.px[q] / mass;
+            vy = g.py[q] / mass;
+            vy -= Q.dtg;
+            const float v2 = vx * vx + vy * vy;
+            if (v2 > Q.vmax_sq) {
+                const float r = sqrtf(v2);
+                vx = vx / r * Q.vmax;
+                vy = vy / r * Q.vmax;
+            }
+            double nx = (double)gx * P.h - ind_x, ny = (double)gy * P.h - ind_y;
+            if (nx * nx + ny * ny < P.ind_rsq) {
+                const double r = sqrt(nx * nx + ny * ny);
+                if (r > 0) { nx /= r; ny /= r; }
+                const float fnx = (float)nx, fny = (float)ny;
+                const float vrx = vx - (float)P.ind_v, vry = vy;
+                const float vn = vrx * fnx + vry * fny;
+                if (vn < 0.f) {
+                    const float vtx = vrx - fnx * vn, vty = vry - fny * vn;
+                    const float pvx = vx, pvy = vy;
+                    vx = (float)P.ind_v + vtx;
+                    vy = vty;
+                    const double fxd = (double)(pvx - vx) * mass / P.dt, fyd = (double)(pvy - vy) * mass / P.dt;
+                    float angle = atan2f(fnx, fny);
+                    angle = (float)((double)angle + kPi);
+                    angle = (float)((double)angle * (P.nsub / (2 * kPi)));
+                    const int bin = min(max((int)angle, 0), P.nsub - 1);
+                    atomicAdd(&s_acc[2 * bin], fxd);
+                    atomicAdd(&s_acc[2 * bin + 1], fyd);
+                    any = true;
+                }
+            }
+            if (gy <= 2) { vx = 0.f; vy = 0.f; }
+            if (gy >= P.gridy - 3 && vy > 0.f) vy = 0.f;
+            if (gx <= 2 && vx < 0.f) vx = 0.f;
+            else if (gx >= P.gridx - 3 && vx > 0.f) vx = 0.f;
+        }
+        g.vx[q] = vx;
+        g.vy[q] = vy;
+        g.m[q] = 0.f;
+        g.px[q] = 0.f;
+        g.py[q] = 0.f;
+    }
+    if (!__syncthreads_or(any)) return;
+    for (int k = threadIdx.x; k < 2 * P.nsub; k += blockDim.x)
+        if (s_acc[k] != 0.0) atomicAdd(acc + k, s_acc[k]);
+}
+
+// ---------------------------------------------------------------- binning / conversion
+__global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__restrict__ st, long pitch, int n,
+                                int *keys, int *ranks, int *counts, int *status)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = i < n;
+    int key = G.ntiles * TT;
+    if (in) {
+        const unsigned u = st[i];
+        if (!(u & (unsigned)kDisabled)) {
+            int cx, cy, bx, by;
+            float fx, fy;
+            unpack_cell(st[i + pitch * S_CELL], cx, cy);
+            const float *f = reinterpret_cast<const float *>(st);
+            split_base(cx, f[i + pitch * S_OX], bx, fx);
+            split_base(cy, f[i + pitch * S_OY], by, fy);
+            const int e = base_error(P, bx, by);
+            if (e) *status = e;
+            else key = G.cell_key(bx, by, P.halo);
+        }
+    }
+    const unsigned act = __ballot_sync(0xffffffffu, in);
+    if (!in) return;
+    const unsigned peers = __match_any_sync(act, key);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&counts[key], __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    keys[i] = key;
+    ranks[i] = base + __popc(peers & ((1u << lane) - 1u));
+}
+
+__global__ void k_bin_scatter_f32(const unsigned *__restrict__ src, unsigned *__restrict__ dst, long pitch, int n,
+                                  const int *__restrict__ keys, const int *__restrict__ ranks,
+                                  const int *__restrict__ start, const int *__restrict__ oidx_src,
+                                  int *__restrict__ oidx_dst)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int d = start[keys[i]] + ranks[i];
+#pragma unroll
+    for (int l = 0; l < S_NLINES; l++) dst[d + pitch * l] = src[i + pitch * l];
+    oidx_dst[d] = oidx_src[i];
+}
+
+// FP64 HSSOA chunk (16 lines, stride cpitch) -> FP32 state slots [first, first+count)
+__global__ void k_split_from_hssoa(const double *__restrict__ chunk, long cpitch, int count, unsigned *st,
+                                   long pitch, int first, double hinv)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    const long i = first + j;
+    float *f = reinterpret_cast<float *>(st);
+    auto L = [&](int l) { return chunk[j + cpitch * l]; };
+    st[i] = (unsigned)(unsigned long long)__double_as_longlong(L(0));
+    int c[2];
+    float o[2];
+    for (int k = 0; k < 2; k++) {
+        const double xs = L(4 + k) * hinv;
+        const double fl = floor(xs);
+        c[k] = (int)fl;
+        o[k] = (float)(xs - fl);
+        if (o[k] >= 1.0f) { c[k] += 1; o[k] = 0.0f; }
+    }
+    st[i + pitch * S_CELL] = pack_cell(c[0], c[1]);
+    f[i + pitch * S_OX] = o[0];
+    f[i + pitch * S_OY] = o[1];
+    f[i + pitch * S_D00] = (float)(L(8) - 1.0);
+    f[i + pitch * S_D01] = (float)L(9);
+    f[i + pitch * S_D10] = (float)L(10);
+    f[i + pitch * S_D11] = (float)(L(11) - 1.0);
+    f[i + pitch * S_JP] = (float)L(3);
+    f[i + pitch * S_VX] = (float)L(6);
+    f[i + pitch * S_VY] = (float)L(7);
+    for (int k = 0; k < 4; k++) f[i + pitch * (S_B00 + k)] = (float)L(12 + k);
+    f[i + pitch * S_P] = (float)L(1);
+    f[i + pitch * S_Q] = (float)L(2);
+}
+
+// FP32 state -> FP64 HSSOA chunk of upload positions [first, first+count);
+// inv[o] is the slot holding the point uploaded at position o.
+__global__ void k_split_to_hssoa(const unsigned *__restrict__ st, long pitch, const int *__restrict__ inv, int first,
+                                 int count, double *__restrict__ chunk, long cpitch, double h)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= count) return;
+    const long i = inv ? inv[first + j] : first + j;
+    const float *f = reinterpret_cast<const float *>(st);
+    auto W = [&](int l, double v) { chunk[j + cpitch * l] = v; };
+    W(0, __longlong_as_double((long long)st[i]));
+    int cx, cy;
+    unpack_cell(st[i + pitch * S_CELL], cx, cy);
+    W(4, ((double)cx + (double)f[i + pitch * S_OX]) * h);
+    W(5, ((double)cy + (double)f[i + pitch * S_OY]) * h);
+    W(8, 1.0 + (double)f[i + pitch * S_D00]);
+    W(9, (double)f[i + pitch * S_D01]);
+    W(10, (double)f[i + pitch * S_D10]);
+    W(11, 1.0 + (double)f[i + pitch * S_D11]);
+    W(3, (double)f[i + pitch * S_JP]);
+    W(6, (double)f[i + pitch * S_VX]);
+    W(7, (double)f[i + pitch * S_VY]);
+    for (int k = 0; k < 4; k++) W(12 + k, (double)f[i + pitch * (S_B00 + k)]);
+    W(1, (double)f[i + pitch * S_P]);
+    W(2, (double)f[i + pitch * S_Q]);
+}
+
+__global__ void k_inverse_perm(const int *__restrict__ oidx, int n, int *__restrict__ inv)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) inv[oidx[i]] = i;
+}
+
+}  // namespace icy_dev

@@ -1,0 +1,102 @@
+"""GPU tests of the FP32 split-precision path (integer cell + FP32 offset
+positions, FP32 Fe - I, FP32 grid; FP64 return mapping and force bins).
+
+Accuracy gate: relative L2 position error ||X - X_ref|| / ||X_ref|| <= 1e-4
+against the FP64 CPU oracle after 1000 steps.  Other fields are reported and
+held to the looser FP32 bounds written below.
+"""
+import numpy as np
+import pytest
+
+from icempm_multi_b200 import GPUImplementation
+from icempm_multi_b200._lib import PRECISION_FP32_SPLIT
+from scenarios import standard, stress
+from test_gpu_parity import field_errors
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-4                       # the split-precision accuracy target
+TOL32 = {"vel": 5e-2, "Fe": 5e-2, "Jp": 5e-2}
+STATUS_MAX = 0.05
+
+
+@pytest.fixture(scope="module")
+def oracle(built):
+    from oracle.oracle import Oracle
+    return Oracle()
+
+
+def run_split(p, soa, steps, chunk=None, **opts):
+    out = soa.clone()
+    g = GPUImplementation(p, out, precision=PRECISION_FP32_SPLIT)
+    for k, v in opts.items():
+        g.set_option(k, v)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.reset_indenter_force_accumulator()
+    t, done = 0.0, 0
+    chunk = chunk or steps
+    while done < steps:
+        k = min(chunk, steps - done)
+        t = g.run_steps(done, k, t)
+        done += k
+    g.transfer_from_device()
+    bins = g.indenter_bins.copy()
+    g.close()
+    return out, t, bins
+
+
+def test_split_roundtrip(built):
+    p, soa = stress(seed=3)
+    out, _, _ = run_split(p, soa, 0)
+    m = ~soa.disabled()
+    assert np.array_equal(out.utility, soa.utility)
+    assert np.max(np.abs(out.pos - soa.pos)) <= 1e-7 * p.cellsize
+    dF = np.abs(out.Fe - soa.Fe)
+    assert np.max(dF) <= 1e-6 * max(np.max(np.abs(soa.Fe[[1, 2]])), 1e-3)
+    assert np.allclose(out.vel[:, m], soa.vel[:, m], rtol=1e-7, atol=1e-7)
+
+
+def test_split_1000_steps_within_target(oracle):
+    p, soa = standard(n_cells_x=48, n_cells_y=12, grid=(128, 48), seed=21)
+    ref = soa.clone()
+    assert oracle.run(p, ref, 0, 1000)[0] == 0
+    out, t, bins = run_split(p, soa, 1000, chunk=250)
+    errs = field_errors(out, ref)
+    print("split 1000 steps", soa.size, errs)
+    assert errs["pos"] <= POS_TOL
+    for k, v in TOL32.items():
+        assert errs[k] <= v, (k, errs)
+    assert errs["status"] <= STATUS_MAX
+
+
+def test_split_stress_branches(oracle):
+    """crushing / SVD return mapping / liquid / disabled points in FP32"""
+    p, soa = stress(seed=5)
+    ref = soa.clone()
+    assert oracle.run(p, ref, 0, 200)[0] == 0
+    out, _, _ = run_split(p, soa, 200, chunk=64, resort_every=16)
+    errs = field_errors(out, ref)
+    print("split stress", errs)
+    assert errs["pos"] <= POS_TOL
+    assert np.array_equal(out.disabled(), ref.disabled()) and np.array_equal(out.liquid(), ref.liquid())
+
+
+def test_split_phase_api(oracle):
+    p, soa = standard(seed=9)
+    a = soa.clone()
+    g = GPUImplementation(p, a, precision=PRECISION_FP32_SPLIT)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    t = 0.0
+    for k in range(60):
+        t += p.InitialTimeStep
+        g.reset_grid()
+        g.p2g()
+        g.update_nodes(t, p.indenter_x_initial + t * p.IndVelocity, p.indenter_y)
+        g.g2p(k % p.UpdateEveryNthStep == 0)
+    g.transfer_from_device()
+    g.close()
+    ref = soa.clone()
+    oracle.run(p, ref, 0, 60)
+    assert field_errors(a, ref)["pos"] <= POS_TOL
