@@ -83,6 +83,9 @@ EXPORTED = [
     "icy_mpm_receive_halos", "icy_mpm_update_nodes", "icy_mpm_g2p", "icy_mpm_receive_points", "icy_mpm_step",
     "icy_mpm_synchronize", "icy_mpm_status", "icy_mpm_kernel_launches", "icy_version", "icy_last_error",
     "icy_mpm_profile", "icy_mpm_profile_read", "icy_mpm_set_option", "icy_step_noalloc",
+    "icy_batch_create", "icy_batch_destroy", "icy_batch_add", "icy_batch_remove", "icy_batch_step",
+    "icy_batch_download", "icy_batch_synchronize", "icy_batch_set_option", "icy_batch_info",
+    "icy_batch_device_bytes", "icy_mpm_device_bytes",
 ]
 
 _lib = None
@@ -130,6 +133,18 @@ def lib():
         "icy_mpm_set_option": (C.c_int, [vp, C.c_char_p, C.c_double]),
         "icy_mpm_profile_read": (C.c_int, [vp, C.c_int, C.c_char_p, vp, vp, C.POINTER(C.c_int)]),
         "icy_step_noalloc": (C.c_int, [P, vp, C.c_uint, C.c_uint, C.c_int, C.c_int, dp, vp, vp]),
+        "icy_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(vp)]),
+        "icy_batch_destroy": (C.c_int, [vp]),
+        "icy_batch_add": (C.c_int, [vp, P, vp, C.c_uint, C.c_uint, C.POINTER(C.c_int)]),
+        "icy_batch_remove": (C.c_int, [vp, C.c_int]),
+        "icy_batch_step": (C.c_int, [vp, C.c_int]),
+        "icy_batch_download": (C.c_int, [vp, C.c_int, vp, C.c_uint, up, vp, dp, C.POINTER(C.c_int64)]),
+        "icy_batch_synchronize": (C.c_int, [vp]),
+        "icy_batch_set_option": (C.c_int, [vp, C.c_char_p, C.c_double]),
+        "icy_batch_info": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                                     C.POINTER(vp)]),
+        "icy_batch_device_bytes": (C.c_int64, [vp, C.c_int]),
+        "icy_mpm_device_bytes": (C.c_int64, [P, C.c_uint, C.c_int]),
         "icy_version": (C.c_char_p, []),
         "icy_last_error": (C.c_char_p, []),
     }

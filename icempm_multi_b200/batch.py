@@ -1,0 +1,79 @@
+"""Batches of independent floe scenarios advanced together (FP32 split precision).
+
+Python face of the icy_batch_* C-ABI (include/icempm.h): members are added
+with their own SimParams and HSSOA, every batch step advances all of them by
+the same number of sub-steps with a handful of kernel launches replayed as a
+CUDA graph, and each member keeps its own simulation time and step index.
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import PRECISION_FP32_SPLIT, check, lib
+
+
+class Batch:
+    def __init__(self, max_instances, device=0):
+        self._b = C.c_void_p()
+        check(lib().icy_batch_create(device, int(max_instances), C.byref(self._b)), "icy_batch_create")
+        self.params = {}
+
+    def close(self):
+        if self._b:
+            lib().icy_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, params, soa):
+        """Admit a scenario; returns its slot."""
+        slot = C.c_int(-1)
+        check(lib().icy_batch_add(self._b, C.byref(params), soa.ptr, soa.capacity, soa.size, C.byref(slot)),
+              "icy_batch_add")
+        self.params[slot.value] = params
+        return slot.value
+
+    def remove(self, slot):
+        check(lib().icy_batch_remove(self._b, int(slot)), "icy_batch_remove")
+        self.params.pop(slot, None)
+
+    def step(self, nsteps):
+        check(lib().icy_batch_step(self._b, int(nsteps)), "icy_batch_step")
+
+    def synchronize(self):
+        check(lib().icy_batch_synchronize(self._b), "icy_batch_synchronize")
+
+    def download(self, slot, soa):
+        """Member state into soa (upload order); returns (sim_time, next_step, bins)."""
+        p = self.params[slot]
+        bins = np.zeros(2 * p.n_indenter_subdivisions)
+        n = C.c_uint(0)
+        t = C.c_double(0)
+        st = C.c_int64(0)
+        rc = lib().icy_batch_download(self._b, int(slot), soa.ptr, soa.capacity, C.byref(n),
+                                      bins.ctypes.data_as(C.c_void_p), C.byref(t), C.byref(st))
+        soa.size = n.value
+        check(rc, "icy_batch_download")
+        return t.value, st.value, bins
+
+    def set_option(self, name, value):
+        check(lib().icy_batch_set_option(self._b, name.encode(), float(value)), "icy_batch_set_option")
+
+    def info(self):
+        live, pts, launches, stream = C.c_int(0), C.c_int64(0), C.c_int64(0), C.c_void_p()
+        check(lib().icy_batch_info(self._b, C.byref(live), C.byref(pts), C.byref(launches), C.byref(stream)),
+              "icy_batch_info")
+        return {"live": live.value, "points": pts.value, "kernel_launches": launches.value,
+                "stream": stream.value}
+
+    def device_bytes(self, slot):
+        return lib().icy_batch_device_bytes(self._b, int(slot))
+
+
+def device_bytes(params, capacity, precision=PRECISION_FP32_SPLIT):
+    """Device memory an instance of this size allocates."""
+    return lib().icy_mpm_device_bytes(C.byref(params), int(capacity), int(precision))

@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libicempm_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["capi.cu", "instance.cu", "noalloc.cu"]
+CUDA_SOURCES = ["capi.cu", "instance.cu", "noalloc.cu", "batch.cu"]
 CXX_SOURCES = ["params.cpp", "scene.cpp"]
 
 

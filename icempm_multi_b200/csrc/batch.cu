@@ -1,0 +1,383 @@
+// batch.cu -- many independent simulation instances advanced together.
+//
+// Every member is an FP32 split-precision instance with its own parameters,
+// grid and points.  One step of the whole batch is four launches, whatever the
+// number of members: advance the members' clocks, update all marked grid
+// nodes, clear the marks, and the tile kernel over the (instance, tile) work
+// list of all members.  A sequence of steps is captured once per length as a
+// CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <vector>
+
+#include "../../include/icempm.h"
+#include "instance.cuh"
+#include "kernels_split.cuh"
+
+using namespace icy_dev;
+
+#define CKB(call)                                                                 \
+    do {                                                                          \
+        cudaError_t e_ = (call);                                                  \
+        if (e_ != cudaSuccess) { icy_set_error(#call, e_); return ICY_ERR_CUDA; } \
+    } while (0)
+
+struct icy_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int nslots = 0;
+    std::vector<icy_mpm *> members;
+    SplitArgs *d_args = nullptr;
+    BatchClock *d_clk = nullptr;
+    int *d_rec = nullptr;
+    long *d_node_off = nullptr, *d_tile_off = nullptr;
+    BatchItem *d_work = nullptr;
+    long work_cap = 0;
+    int *d_woff = nullptr, *d_nwork = nullptr;
+    bool dirty = true;
+    int steps_since_bin = 0, resort_every = 256;
+    std::map<int, cudaGraphExec_t> graphs;
+    std::map<int, int> graph_launches;   // kernels per replay
+    int tile_grid = 0, update_grid = 0;
+    int64_t launches = 0;
+};
+
+static SplitArgs member_args(icy_mpm *h)
+{
+    SplitArgs A{};
+    A.P = icy_step_params(h->prm);
+    A.Q = split_consts(A.P);
+    A.G = TileGeom{h->ntx, h->nty, h->ntiles};
+    GridViewF g;
+    g.m = h->d_gridf;
+    g.px = h->d_gridf + h->n_nodes;
+    g.py = h->d_gridf + 2 * h->n_nodes;
+    g.vx = h->d_gridf + 3 * h->n_nodes;
+    g.vy = h->d_gridf + 4 * h->n_nodes;
+    g.ny = h->prm.GridY;
+    g.halo = h->prm.GridHaloSize;
+    A.g = g;
+    A.st = h->d_st;
+    A.pitch = h->pitch;
+    A.cell_start = h->d_start;
+    A.active = h->d_active;
+    A.n_active = h->d_nactive;
+    A.flags = h->d_flags;
+    A.status = h->d_status;
+    A.moved = h->d_moved;
+    A.grain_tab = static_cast<const GrainConstF *>(h->d_grainf);
+    A.record_pq = 0;
+    A.acc = h->d_acc;
+    A.n_nodes = h->n_nodes;
+    return A;
+}
+
+static void drop_graphs(icy_batch *b)
+{
+    for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+    b->graph_launches.clear();
+}
+
+// Upload the members' kernel arguments, node / tile offsets and work list.
+static int rebuild(icy_batch *b)
+{
+    std::vector<SplitArgs> args(b->nslots);
+    std::vector<long> node_off(b->nslots + 1, 0), tile_off(b->nslots + 1, 0);
+    long tiles = 0;
+    for (int s = 0; s < b->nslots; s++) {
+        icy_mpm *h = b->members[s];
+        if (h) args[s] = member_args(h);
+        node_off[s + 1] = node_off[s] + (h ? h->n_nodes : 0);
+        tile_off[s + 1] = tile_off[s] + (h ? h->ntiles : 0);
+        tiles += h ? h->ntiles : 0;
+    }
+    if (tiles > b->work_cap) {
+        cudaFree(b->d_work);
+        b->d_work = nullptr;
+        drop_graphs(b);   // the graphs hold the old work-list address
+        const long cap = std::max(tiles, 2 * b->work_cap);
+        cudaError_t e = cudaMalloc(&b->d_work, sizeof(BatchItem) * std::max(cap, 1L));
+        if (e != cudaSuccess) { icy_set_error("cudaMalloc(batch work list)", e); return ICY_ERR_OUT_OF_MEMORY; }
+        b->work_cap = cap;
+    }
+    CKB(cudaMemcpyAsync(b->d_args, args.data(), sizeof(SplitArgs) * b->nslots, cudaMemcpyHostToDevice, b->stream));
+    CKB(cudaMemcpyAsync(b->d_node_off, node_off.data(), sizeof(long) * (b->nslots + 1), cudaMemcpyHostToDevice,
+                        b->stream));
+    CKB(cudaMemcpyAsync(b->d_tile_off, tile_off.data(), sizeof(long) * (b->nslots + 1), cudaMemcpyHostToDevice,
+                        b->stream));
+    k_batch_work_offsets<<<1, 1024, 0, b->stream>>>(b->d_args, b->d_clk, b->nslots, b->d_woff, b->d_nwork);
+    k_batch_work_fill<<<dim3(8, b->nslots), 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_woff, b->d_work);
+    CKB(cudaGetLastError());
+    b->launches += 2;
+    CKB(cudaStreamSynchronize(b->stream));   // host vectors above go out of scope
+    b->dirty = false;
+    return ICY_OK;
+}
+
+static int rebin_members(icy_batch *b)
+{
+    for (icy_mpm *h : b->members)
+        if (h && h->n) {
+            const int64_t l0 = h->launches;
+            if (int rc = icy_instance_bin(h)) return rc;
+            b->launches += h->launches - l0;
+        }
+    b->steps_since_bin = 0;
+    b->dirty = true;
+    return ICY_OK;
+}
+
+// Capture [P2G] + nsteps x [advance, update, clear marks, G2P(+P2G)] as a graph.
+static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
+{
+    SplitArgs none{};
+    cudaGraph_t g = nullptr;
+    int n = 0;
+    CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    k_tile_f32<false, true, false, true><<<b->tile_grid, TILE_THREADS, MOMF_BYTES, b->stream>>>(
+        none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+    n++;
+    for (int k = 0; k < nsteps; k++) {
+        k_batch_advance<<<(b->nslots + 127) / 128, 128, 0, b->stream>>>(b->d_clk, b->d_rec, b->nslots);
+        k_update_batch_f32<<<b->update_grid, 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_node_off, b->nslots);
+        k_clear_flags_batch<<<b->update_grid / 4 + 1, 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_tile_off,
+                                                                         b->nslots);
+        if (k + 1 < nsteps)
+            k_tile_f32<true, true, false, true><<<b->tile_grid, TILE_THREADS, MOMF_BYTES, b->stream>>>(
+                none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+        else
+            k_tile_f32<true, false, true, true><<<b->tile_grid, TILE_THREADS, 0, b->stream>>>(
+                none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+        n += 4;
+    }
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (e != cudaSuccess) { icy_set_error("cudaStreamEndCapture", e); return ICY_ERR_CUDA; }
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { icy_set_error("cudaGraphInstantiate", e); return ICY_ERR_CUDA; }
+    *nlaunch = n;
+    return ICY_OK;
+}
+
+extern "C" int64_t icy_mpm_device_bytes(const icy_sim_params *p, unsigned capacity, int precision);
+
+static int64_t icy_instance_device_bytes(icy_mpm *h)
+{
+    return icy_mpm_device_bytes(&h->prm, h->capacity, h->precision);
+}
+
+extern "C" {
+
+// Device memory an instance of this size takes (as allocated by
+// icy_instance_allocate), for admission by memory budget.
+int64_t icy_mpm_device_bytes(const icy_sim_params *p, unsigned capacity, int precision)
+{
+    if (!p) return 0;
+    const long pitch = ((long)capacity + 31) / 32 * 32;
+    const long nx = p->GridXTotal + 2L * p->GridHaloSize;
+    const long n_nodes = (long)p->GridY * nx;
+    const long ntiles = ((nx + TX - 1) / TX) * ((p->GridY + TY - 1) / TY);
+    const long nkeys = ntiles * TT + 1;
+    int64_t b = 0;
+    if (precision == ICY_PRECISION_FP32_SPLIT)
+        b += 2 * (int64_t)S_NLINES * 4 * pitch + 16 * 8 * (int64_t)std::min(pitch, 1L << 20) + 5 * 4 * (int64_t)n_nodes;
+    else
+        b += 2 * 16 * 8 * (int64_t)pitch + 5 * 8 * (int64_t)n_nodes;
+    b += 4 * 4 * (int64_t)pitch + 4 * (2 * nkeys + 1) + 4 * 2 * ntiles + 2 * 8 * p->n_indenter_subdivisions + 65536;
+    return b;
+}
+
+int icy_batch_create(int device, int max_instances, icy_batch **out)
+{
+    if (!out || max_instances < 1 || max_instances > 65535) return ICY_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    icy_batch *b = new icy_batch();
+    b->device = device;
+    b->nslots = max_instances;
+    b->members.assign(max_instances, nullptr);
+    auto fail = [&](cudaError_t e, const char *w) {
+        icy_set_error(w, e);
+        icy_batch_destroy(b);
+        return ICY_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return fail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    if ((e = cudaMalloc(&b->d_args, sizeof(SplitArgs) * max_instances)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_clk, sizeof(BatchClock) * max_instances)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_rec, sizeof(int) * max_instances)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_node_off, sizeof(long) * (max_instances + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_tile_off, sizeof(long) * (max_instances + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_woff, sizeof(int) * max_instances)) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_nwork, sizeof(int))) != cudaSuccess)
+        return fail(e, "cudaMalloc(batch)");
+    cudaMemsetAsync(b->d_clk, 0, sizeof(BatchClock) * max_instances, b->stream);
+    cudaMemsetAsync(b->d_rec, 0, sizeof(int) * max_instances, b->stream);
+    cudaMemsetAsync(b->d_nwork, 0, sizeof(int), b->stream);
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false, true>, TILE_THREADS,
+                                                  MOMF_BYTES);
+    b->tile_grid = std::max(1, sms * std::max(per_sm, 1));
+    b->update_grid = std::max(1, sms * 16);
+    if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return fail(e, "batch init");
+    *out = b;
+    return ICY_OK;
+}
+
+int icy_batch_destroy(icy_batch *b)
+{
+    if (!b) return ICY_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop_graphs(b);
+    for (icy_mpm *h : b->members)
+        if (h) icy_mpm_destroy(h);
+    cudaFree(b->d_args);
+    cudaFree(b->d_clk);
+    cudaFree(b->d_rec);
+    cudaFree(b->d_node_off);
+    cudaFree(b->d_tile_off);
+    cudaFree(b->d_work);
+    cudaFree(b->d_woff);
+    cudaFree(b->d_nwork);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return ICY_OK;
+}
+
+int icy_batch_add(icy_batch *b, const icy_sim_params *p, const double *hssoa, unsigned capacity, unsigned size,
+                  int *slot)
+{
+    if (!b || !p || !hssoa || !slot || size > capacity || p->UpdateEveryNthStep <= 0) return ICY_ERR_INVALID_ARGUMENT;
+    int s = -1;
+    for (int k = 0; k < b->nslots; k++)
+        if (!b->members[k]) { s = k; break; }
+    if (s < 0) return ICY_ERR_NO_SPACE;
+    CKB(cudaSetDevice(b->device));
+    icy_mpm *h = nullptr;
+    int rc = icy_mpm_create(p, b->device, std::max(size, 1u), ICY_PRECISION_FP32_SPLIT, &h);
+    if (rc) return rc;
+    h->stream = b->stream;
+    if ((rc = icy_mpm_update_constants(h, p)) || (rc = icy_mpm_transfer_points_to_device(h, hssoa, capacity, size)) ||
+        (rc = icy_mpm_reset_indenter_force_accumulator(h)) || (rc = icy_instance_bin(h))) {
+        icy_mpm_destroy(h);
+        return rc;
+    }
+    BatchClock c{};
+    c.t = 0.0;
+    c.dt = p->InitialTimeStep;
+    c.x0 = p->indenter_x_initial;
+    c.y0 = p->indenter_y;
+    c.v = p->IndVelocity;
+    c.ind_x = p->indenter_x_initial;
+    c.step = 0;
+    c.every = p->UpdateEveryNthStep;
+    c.live = 1;
+    CKB(cudaMemcpyAsync(b->d_clk + s, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
+    CKB(cudaStreamSynchronize(b->stream));
+    b->members[s] = h;
+    b->dirty = true;
+    *slot = s;
+    return ICY_OK;
+}
+
+int icy_batch_remove(icy_batch *b, int slot)
+{
+    if (!b || slot < 0 || slot >= b->nslots || !b->members[slot]) return ICY_ERR_INVALID_ARGUMENT;
+    CKB(cudaSetDevice(b->device));
+    CKB(cudaStreamSynchronize(b->stream));
+    BatchClock c{};
+    CKB(cudaMemcpy(b->d_clk + slot, &c, sizeof(c), cudaMemcpyHostToDevice));
+    icy_mpm *h = b->members[slot];
+    h->stream = h->own_stream;
+    icy_mpm_destroy(h);
+    b->members[slot] = nullptr;
+    b->dirty = true;
+    return ICY_OK;
+}
+
+int icy_batch_step(icy_batch *b, int nsteps)
+{
+    if (!b || nsteps < 0) return ICY_ERR_INVALID_ARGUMENT;
+    if (nsteps == 0) return ICY_OK;
+    CKB(cudaSetDevice(b->device));
+    if (b->dirty)
+        if (int rc = rebuild(b)) return rc;
+    auto it = b->graphs.find(nsteps);
+    if (it == b->graphs.end()) {
+        cudaGraphExec_t ge;
+        int nl = 0;
+        if (int rc = capture(b, nsteps, &ge, &nl)) return rc;
+        it = b->graphs.emplace(nsteps, ge).first;
+        b->graph_launches[nsteps] = nl;
+    }
+    CKB(cudaGraphLaunch(it->second, b->stream));
+    b->launches += b->graph_launches[nsteps];
+    b->steps_since_bin += nsteps;
+    if (b->resort_every > 0 && b->steps_since_bin >= b->resort_every)
+        if (int rc = rebin_members(b)) return rc;
+    return ICY_OK;
+}
+
+int icy_batch_download(icy_batch *b, int slot, double *hssoa, unsigned capacity, unsigned *size, double *bins,
+                       double *sim_time, int64_t *step)
+{
+    if (!b || slot < 0 || slot >= b->nslots || !b->members[slot]) return ICY_ERR_INVALID_ARGUMENT;
+    CKB(cudaSetDevice(b->device));
+    BatchClock c;
+    CKB(cudaMemcpyAsync(&c, b->d_clk + slot, sizeof(c), cudaMemcpyDeviceToHost, b->stream));
+    int rc = icy_mpm_transfer_from_device(b->members[slot], hssoa, capacity, size, bins);
+    if (sim_time) *sim_time = c.t;
+    if (step) *step = c.step;
+    return rc;
+}
+
+int icy_batch_synchronize(icy_batch *b)
+{
+    if (!b) return ICY_ERR_INVALID_ARGUMENT;
+    CKB(cudaSetDevice(b->device));
+    CKB(cudaStreamSynchronize(b->stream));
+    return ICY_OK;
+}
+
+int icy_batch_set_option(icy_batch *b, const char *name, double value)
+{
+    if (!b || !name) return ICY_ERR_INVALID_ARGUMENT;
+    if (std::strcmp(name, "resort_every") == 0 && value >= 0) {
+        b->resort_every = (int)value;
+        return ICY_OK;
+    }
+    if (std::strcmp(name, "tile_ctas") == 0 && value >= 1) {   // persistent CTAs of the tile kernel
+        b->tile_grid = (int)value;
+        drop_graphs(b);
+        return ICY_OK;
+    }
+    return ICY_ERR_INVALID_ARGUMENT;
+}
+
+int icy_batch_info(icy_batch *b, int *live, int64_t *points, int64_t *kernel_launches, void **stream)
+{
+    if (!b) return ICY_ERR_INVALID_ARGUMENT;
+    int nl = 0;
+    int64_t np = 0;
+    for (icy_mpm *h : b->members)
+        if (h) { nl++; np += h->n; }
+    if (live) *live = nl;
+    if (points) *points = np;
+    if (kernel_launches) *kernel_launches = b->launches;
+    if (stream) *stream = b->stream;
+    return ICY_OK;
+}
+
+int64_t icy_batch_device_bytes(icy_batch *b, int slot)
+{
+    if (!b || slot < 0 || slot >= b->nslots || !b->members[slot]) return 0;
+    return icy_instance_device_bytes(b->members[slot]);
+}
+
+}  // extern "C"

@@ -25,7 +25,7 @@ __device__ __forceinline__ long long ld_util(const double *pts, long i)
 }
 
 // P2G, one thread per particle (kernels.cuh:46-122)
-__global__ void k_p2g_simple(StepParams P, const double *__restrict__ pts, long pitch, int n, GridView g,
+static __global__ void k_p2g_simple(StepParams P, const double *__restrict__ pts, long pitch, int n, GridView g,
                              int *status)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -66,7 +66,7 @@ __global__ void k_p2g_simple(StepParams P, const double *__restrict__ pts, long 
 
 // indenter force bins are accumulated per block in shared memory first
 // and added to the global accumulator once per block
-__global__ void k_update_simple(StepParams P, GridView g, long n_nodes, double ind_x, double ind_y,
+static __global__ void k_update_simple(StepParams P, GridView g, long n_nodes, double ind_x, double ind_y,
                                 double *acc)
 {
     extern __shared__ double s_acc[];   // 2*nsub
@@ -97,7 +97,7 @@ __global__ void k_update_simple(StepParams P, GridView g, long n_nodes, double i
 }
 
 // G2P + plasticity, one thread per particle (kernels.cuh:305-414)
-__global__ void k_g2p_simple(StepParams P, double *__restrict__ pts, long pitch, int n, GridView g, int recordPQ,
+static __global__ void k_g2p_simple(StepParams P, double *__restrict__ pts, long pitch, int n, GridView g, int recordPQ,
                              int *status)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -40,7 +40,7 @@ __host__ __device__ inline SplitConsts split_consts(const StepParams &P)
     return c;
 }
 
-__global__ void k_grain_table_f32(const GrainConst *tab, GrainConstF *out)
+static __global__ void k_grain_table_f32(const GrainConst *tab, GrainConstF *out)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < GRAIN_TAB) out[s] = GrainConstF{(float)tab[s].pmin2, (float)tab[s].k, (float)tab[s].msq};
@@ -258,6 +258,8 @@ struct SplitArgs {
     unsigned long long *moved;
     const GrainConstF *grain_tab;
     int record_pq;
+    double *acc;        // indenter force bins (batched update)
+    long n_nodes;       // nodes of the grid (batched update)
 };
 
 template <typename Sink>
@@ -280,7 +282,7 @@ __device__ __forceinline__ void point_contributions_f32(float h, float fx, float
     }
 }
 
-__device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags, int ntx, int halo, float h, int bx, int by,
+static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags, int ntx, int halo, float h, int bx, int by,
                                             float fx, float fy, float mass, float mvx, float mvy, float s00,
                                             float s01, float s10, float s11)
 {
@@ -388,23 +390,34 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
     sync();
 }
 
+// Work items of a batch: (instance, tile) pairs over all instances.
+struct BatchItem { int inst, tile; };
+
 // Tile kernel over the FP32 state: <G2P, P2G, write vel/Bp> as k_tile.
-template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
-__global__ void __launch_bounds__(TILE_THREADS, 3) k_tile_f32(SplitArgs A)
+// With BATCH, the CTAs walk the (instance, tile) list of many independent
+// instances, each with its own parameters, grid and points (Aarr[inst]), and
+// the record-PQ flag of each instance comes from rec[inst].
+template <bool DO_G2P, bool DO_P2G, bool WRITE_VB, bool BATCH = false>
+static __global__ void __launch_bounds__(TILE_THREADS, 3)
+    k_tile_f32(SplitArgs A1, const SplitArgs *__restrict__ Aarr = nullptr, const BatchItem *__restrict__ work = nullptr,
+               const int *__restrict__ nwork = nullptr, const int *__restrict__ rec = nullptr)
 {
     __shared__ float s_v[2][RN];
     __shared__ float s_odd[3][RN];
     __shared__ int s_cs[TT + 1];
     __shared__ unsigned s_touch;
     extern __shared__ float s_momf[];
-    const StepParams &P = A.P;
-    const int na = *A.n_active;
+    const int na = BATCH ? *nwork : *A1.n_active;
     const int tid = threadIdx.x;
-    unsigned moved = 0;
     for (int k = tid; k < RN; k += blockDim.x) { s_odd[0][k] = 0.f; s_odd[1][k] = 0.f; s_odd[2][k] = 0.f; }
-    const float *fst = reinterpret_cast<const float *>(A.st);
     for (int ti = blockIdx.x; ti < na; ti += gridDim.x) {
-        const int t = A.active[ti];
+        const BatchItem w = BATCH ? work[ti] : BatchItem{0, A1.active[ti]};
+        const SplitArgs &A = BATCH ? Aarr[w.inst] : A1;
+        const StepParams &P = A.P;
+        const bool record = BATCH ? rec[w.inst] != 0 : A.record_pq != 0;
+        const float *fst = reinterpret_cast<const float *>(A.st);
+        unsigned moved = 0;
+        const int t = w.tile;
         const int tx = t % A.G.ntx, ty = t / A.G.ntx;
         const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
         for (int c = tid; c <= TT; c += blockDim.x) s_cs[c] = A.cell_start[(long)t * TT + c];
@@ -453,7 +466,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) k_tile_f32(SplitArgs A)
                         if (DO_P2G) s_momf[mom_idx(9, j)] = __int_as_float(BASE_NONE);
                         continue;
                     }
-                    store_point_f32(A.st, A.pitch, i, s, WRITE_VB, A.record_pq != 0);
+                    store_point_f32(A.st, A.pitch, i, s, WRITE_VB, record);
                 } else {
                     s.vx = fst[i + A.pitch * S_VX];
                     s.vy = fst[i + A.pitch * S_VY];
@@ -475,18 +488,16 @@ __global__ void __launch_bounds__(TILE_THREADS, 3) k_tile_f32(SplitArgs A)
                 const int ntx = tx + tid % 3 - 1, nty = ty + tid / 3 - 1;
                 A.flags[nty * A.G.ntx + ntx] = 1u;
             }
+            moved = __reduce_add_sync(0xffffffffu, moved);
+            if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
         }
         __syncthreads();
-    }
-    if (DO_P2G) {
-        moved = __reduce_add_sync(0xffffffffu, moved);
-        if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
     }
 }
 
 // Grid update in FP32 (simulation/kernels.cuh:175-300); the indenter geometry
 // and the force bins in FP64.
-__global__ void __launch_bounds__(256) k_update_nodes_f32(StepParams P, SplitConsts Q, TileGeom G, GridViewF g,
+static __global__ void __launch_bounds__(256) k_update_nodes_f32(StepParams P, SplitConsts Q, TileGeom G, GridViewF g,
                                                           const unsigned *__restrict__ flags, long n_nodes,
                                                           double ind_x, double ind_y, double *acc)
 {
@@ -550,7 +561,7 @@ __global__ void __launch_bounds__(256) k_update_nodes_f32(StepParams P, SplitCon
 }
 
 // ---------------------------------------------------------------- binning / conversion
-__global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__restrict__ st, long pitch, int n,
+static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__restrict__ st, long pitch, int n,
                                 int *keys, int *ranks, int *counts, int *status)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -581,7 +592,7 @@ __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__rest
     ranks[i] = base + __popc(peers & ((1u << lane) - 1u));
 }
 
-__global__ void k_bin_scatter_f32(const unsigned *__restrict__ src, unsigned *__restrict__ dst, long pitch, int n,
+static __global__ void k_bin_scatter_f32(const unsigned *__restrict__ src, unsigned *__restrict__ dst, long pitch, int n,
                                   const int *__restrict__ keys, const int *__restrict__ ranks,
                                   const int *__restrict__ start, const int *__restrict__ oidx_src,
                                   int *__restrict__ oidx_dst)
@@ -595,7 +606,7 @@ __global__ void k_bin_scatter_f32(const unsigned *__restrict__ src, unsigned *__
 }
 
 // FP64 HSSOA chunk (16 lines, stride cpitch) -> FP32 state slots [first, first+count)
-__global__ void k_split_from_hssoa(const double *__restrict__ chunk, long cpitch, int count, unsigned *st,
+static __global__ void k_split_from_hssoa(const double *__restrict__ chunk, long cpitch, int count, unsigned *st,
                                    long pitch, int first, double hinv)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -630,7 +641,7 @@ __global__ void k_split_from_hssoa(const double *__restrict__ chunk, long cpitch
 
 // FP32 state -> FP64 HSSOA chunk of upload positions [first, first+count);
 // inv[o] is the slot holding the point uploaded at position o.
-__global__ void k_split_to_hssoa(const unsigned *__restrict__ st, long pitch, const int *__restrict__ inv, int first,
+static __global__ void k_split_to_hssoa(const unsigned *__restrict__ st, long pitch, const int *__restrict__ inv, int first,
                                  int count, double *__restrict__ chunk, long cpitch, double h)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -655,10 +666,152 @@ __global__ void k_split_to_hssoa(const unsigned *__restrict__ st, long pitch, co
     W(2, (double)f[i + pitch * S_Q]);
 }
 
-__global__ void k_inverse_perm(const int *__restrict__ oidx, int n, int *__restrict__ inv)
+static __global__ void k_inverse_perm(const int *__restrict__ oidx, int n, int *__restrict__ inv)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) inv[oidx[i]] = i;
+}
+
+}  // namespace icy_dev
+
+namespace icy_dev {
+
+// ---------------------------------------------------------------- batches
+// Time stepping of one batch member on the device, so that a sequence of
+// sub-steps can be replayed as a CUDA graph: the reference's
+// `t += dt; indenter_x = indenter_x_initial + t * IndVelocity`
+// (simulation/model.cpp:40-41), evaluated with explicit round-to-nearest
+// operations (no FMA contraction), as the host does it.
+struct BatchClock {
+    double t, dt, x0, y0, v, ind_x;
+    long long step;   // index of the next sub-step
+    int every;        // UpdateEveryNthStep
+    int live;         // 0 = free slot
+};
+
+static __global__ void k_batch_advance(BatchClock *clk, int *rec, int nslots)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nslots || !clk[i].live) return;
+    BatchClock c = clk[i];
+    c.t = __dadd_rn(c.t, c.dt);
+    c.ind_x = __dadd_rn(c.x0, __dmul_rn(c.t, c.v));
+    rec[i] = (c.step % c.every) == 0;
+    c.step += 1;
+    clk[i] = c;
+}
+
+__device__ __forceinline__ int find_slot(const long *off, int nslots, long q)
+{
+    int lo = 0, hi = nslots;   // off[lo] <= q < off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= q) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Grid update of all members' marked nodes (see k_update_nodes_f32); the force
+// of a contact node goes straight to its member's bins.
+static __global__ void __launch_bounds__(256) k_update_batch_f32(const SplitArgs *__restrict__ Aarr,
+                                                                 const BatchClock *__restrict__ clk,
+                                                                 const long *__restrict__ node_off, int nslots)
+{
+    const long total = node_off[nslots];
+    for (long gq = (long)blockIdx.x * blockDim.x + threadIdx.x; gq < total; gq += (long)gridDim.x * blockDim.x) {
+        const int s = find_slot(node_off, nslots, gq);
+        if (!clk[s].live) continue;
+        const SplitArgs &A = Aarr[s];
+        const StepParams &P = A.P;
+        const GridViewF &g = A.g;
+        const int q = (int)(gq - node_off[s]);
+        const int col = q / g.ny;
+        const int gx = col - g.halo, gy = q - col * g.ny;
+        if (!A.flags[(gy / TY) * A.G.ntx + (gx + g.halo) / TX]) continue;
+        const float mass = g.m[q];
+        float vx = 0.f, vy = 0.f;
+        if (mass != 0.f) {
+            vx = g.px[q] / mass;
+            vy = g.py[q] / mass;
+            vy -= A.Q.dtg;
+            const float v2 = vx * vx + vy * vy;
+            if (v2 > A.Q.vmax_sq) {
+                const float r = sqrtf(v2);
+                vx = vx / r * A.Q.vmax;
+                vy = vy / r * A.Q.vmax;
+            }
+            double nx = (double)gx * P.h - clk[s].ind_x, ny = (double)gy * P.h - clk[s].y0;
+            if (nx * nx + ny * ny < P.ind_rsq) {
+                const double r = sqrt(nx * nx + ny * ny);
+                if (r > 0) { nx /= r; ny /= r; }
+                const float fnx = (float)nx, fny = (float)ny;
+                const float vrx = vx - (float)P.ind_v, vry = vy;
+                const float vn = vrx * fnx + vry * fny;
+                if (vn < 0.f) {
+                    const float vtx = vrx - fnx * vn, vty = vry - fny * vn;
+                    const float pvx = vx, pvy = vy;
+                    vx = (float)P.ind_v + vtx;
+                    vy = vty;
+                    float angle = atan2f(fnx, fny);
+                    angle = (float)((double)angle + kPi);
+                    angle = (float)((double)angle * (P.nsub / (2 * kPi)));
+                    const int bin = min(max((int)angle, 0), P.nsub - 1);
+                    atomicAdd(A.acc + 2 * bin, (double)(pvx - vx) * mass / P.dt);
+                    atomicAdd(A.acc + 2 * bin + 1, (double)(pvy - vy) * mass / P.dt);
+                }
+            }
+            if (gy <= 2) { vx = 0.f; vy = 0.f; }
+            if (gy >= P.gridy - 3 && vy > 0.f) vy = 0.f;
+            if (gx <= 2 && vx < 0.f) vx = 0.f;
+            else if (gx >= P.gridx - 3 && vx > 0.f) vx = 0.f;
+        }
+        g.vx[q] = vx;
+        g.vy[q] = vy;
+        g.m[q] = 0.f;
+        g.px[q] = 0.f;
+        g.py[q] = 0.f;
+    }
+}
+
+static __global__ void k_clear_flags_batch(const SplitArgs *__restrict__ Aarr, const BatchClock *__restrict__ clk,
+                                           const long *__restrict__ tile_off, int nslots)
+{
+    const long total = tile_off[nslots];
+    for (long gt = (long)blockIdx.x * blockDim.x + threadIdx.x; gt < total; gt += (long)gridDim.x * blockDim.x) {
+        const int s = find_slot(tile_off, nslots, gt);
+        if (clk[s].live) Aarr[s].flags[gt - tile_off[s]] = 0u;
+    }
+}
+
+// (instance, tile) work list: offsets by an exclusive scan over the members'
+// non-empty-tile counts (one CTA), then a fill
+static __global__ void __launch_bounds__(1024) k_batch_work_offsets(const SplitArgs *__restrict__ Aarr,
+                                                                    const BatchClock *__restrict__ clk, int nslots,
+                                                                    int *off, int *nwork)
+{
+    __shared__ int s_warp[32];
+    const int per = (nslots + 1023) / 1024;
+    const int b = min((int)threadIdx.x * per, nslots), e = min(b + per, nslots);
+    int s = 0;
+    for (int i = b; i < e; i++) s += clk[i].live ? *Aarr[i].n_active : 0;
+    int total;
+    int run = block_exclusive_scan<1024>(s, s_warp, total);
+    for (int i = b; i < e; i++) {
+        off[i] = run;
+        run += clk[i].live ? *Aarr[i].n_active : 0;
+    }
+    if (threadIdx.x == 0) *nwork = total;
+}
+
+static __global__ void k_batch_work_fill(const SplitArgs *__restrict__ Aarr, const BatchClock *__restrict__ clk,
+                                         const int *__restrict__ off, BatchItem *work)
+{
+    const int s = blockIdx.y;
+    if (!clk[s].live) return;
+    const int n = *Aarr[s].n_active;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        work[off[s] + k] = BatchItem{s, Aarr[s].active[k]};
 }
 
 }  // namespace icy_dev

@@ -61,7 +61,7 @@ struct TileArgs {
     int record_pq;
 };
 
-__global__ void k_grain_table(StepParams P, GrainConst *tab)
+static __global__ void k_grain_table(StepParams P, GrainConst *tab)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s < GRAIN_TAB) tab[s] = grain_constants(P, s / GRAIN_N11 - 29, s % GRAIN_N11 - 10);
@@ -111,7 +111,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *s_warp, int &tot
 
 constexpr int SCAN_NT = 256, SCAN_PER = 16, SCAN_BLOCK = SCAN_NT * SCAN_PER;
 
-__global__ void __launch_bounds__(SCAN_NT) k_scan_reduce(const int *in, int n, int *block_sum)
+static __global__ void __launch_bounds__(SCAN_NT) k_scan_reduce(const int *in, int n, int *block_sum)
 {
     __shared__ int s_warp[SCAN_NT / 32];
     const long base = (long)blockIdx.x * SCAN_BLOCK;
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(SCAN_NT) k_scan_reduce(const int *in, int n, i
 }
 
 // one CTA: exclusive scan of the nb block sums, in place
-__global__ void __launch_bounds__(1024) k_scan_blocks(int *block_sum, int nb)
+static __global__ void __launch_bounds__(1024) k_scan_blocks(int *block_sum, int nb)
 {
     __shared__ int s_warp[32];
     const int per = (nb + 1023) / 1024;
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(1024) k_scan_blocks(int *block_sum, int nb)
 }
 
 // start[i] = exclusive prefix of in[] (n items); start[n] = total
-__global__ void __launch_bounds__(SCAN_NT) k_scan_apply(const int *in, int n, const int *block_off, int *start)
+static __global__ void __launch_bounds__(SCAN_NT) k_scan_apply(const int *in, int n, const int *block_off, int *start)
 {
     __shared__ int s_warp[SCAN_NT / 32];
     const long base = (long)blockIdx.x * SCAN_BLOCK + (long)threadIdx.x * SCAN_PER;
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(SCAN_NT) k_scan_apply(const int *in, int n, co
 }
 
 // one CTA: ordered list of tiles that hold points
-__global__ void __launch_bounds__(1024) k_tiles_active(const int *cell_start, int ntiles, int *active, int *n_active)
+static __global__ void __launch_bounds__(1024) k_tiles_active(const int *cell_start, int ntiles, int *active, int *n_active)
 {
     __shared__ int s_warp[32];
     const int per = (ntiles + 1023) / 1024;
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(1024) k_tiles_active(const int *cell_start, in
 }
 
 // ---------------------------------------------------------------- binning
-__global__ void k_bin_count(StepParams P, TileGeom G, const double *__restrict__ pts, long pitch, int n,
+static __global__ void k_bin_count(StepParams P, TileGeom G, const double *__restrict__ pts, long pitch, int n,
                             int *keys, int *ranks, int *counts, int *status)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -207,7 +207,7 @@ __global__ void k_bin_count(StepParams P, TileGeom G, const double *__restrict__
     ranks[i] = base + __popc(peers & ((1u << lane) - 1u));
 }
 
-__global__ void k_bin_scatter(const double *__restrict__ src, double *__restrict__ dst, long pitch, int n,
+static __global__ void k_bin_scatter(const double *__restrict__ src, double *__restrict__ dst, long pitch, int n,
                               const int *__restrict__ keys, const int *__restrict__ ranks,
                               const int *__restrict__ start, const int *__restrict__ oidx_src,
                               int *__restrict__ oidx_dst)
@@ -220,14 +220,14 @@ __global__ void k_bin_scatter(const double *__restrict__ src, double *__restrict
     oidx_dst[d] = oidx_src[i];
 }
 
-__global__ void k_iota(int *a, int n)
+static __global__ void k_iota(int *a, int n)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = i;
 }
 
 // HSSOA back in upload order: dst[l][oidx[i]] = src[l][i]
-__global__ void k_unpermute(const double *__restrict__ src, double *__restrict__ dst, long pitch, int n,
+static __global__ void k_unpermute(const double *__restrict__ src, double *__restrict__ dst, long pitch, int n,
                             const int *__restrict__ oidx)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -261,7 +261,7 @@ __device__ __forceinline__ void point_contributions(double h, double fx, double 
 }
 
 // P2G of one point straight into the global grid (its base left the staged region).
-__device__ __noinline__ void p2g_global(GridView g, unsigned *flags, int ntx, int halo, double h, int bx, int by,
+static __device__ __noinline__ void p2g_global(GridView g, unsigned *flags, int ntx, int halo, double h, int bx, int by,
                                         double fx, double fy, double mass, double mvx, double mvy, double s00,
                                         double s01, double s10, double s11)
 {
@@ -514,7 +514,7 @@ __device__ __forceinline__ void mark_node_tiles(const TileArgs &A, int tx, int t
 // only) and the last (<true, false, true>: G2P only, writes vel and Bp), and
 // by the per-phase calls.
 template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
-__global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
+static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
 {
     __shared__ double s_v[2][RN];      // staged node velocities (G2P)
     __shared__ double s_odd[3][RN];    // contributions of points off their sorted cell
@@ -619,7 +619,7 @@ constexpr int PIPE_CONS = 256, PIPE_THREADS = PIPE_CONS + 32, NSTAGE = 2;
 constexpr int NLINE = 8;                          // utility, Jp, x, y, Fe00..Fe11
 constexpr int LINE_CAP = CAP + 2;                 // slack for 16-byte alignment of the copy
 static_assert((LINE_CAP * sizeof(double)) % 16 == 0, "16-byte aligned staged lines");
-__device__ __constant__ const int kPipeLines[NLINE] = {0, 3, 4, 5, 8, 9, 10, 11};
+static __device__ __constant__ const int kPipeLines[NLINE] = {0, 3, 4, 5, 8, 9, 10, 11};
 constexpr long PIPE_WAIT_LIMIT = 1L << 26;        // polls before a wait gives up
 
 struct PipeSmem {
@@ -635,7 +635,7 @@ struct PipeSmem {
 };
 constexpr size_t PIPE_SMEM = sizeof(PipeSmem) + 128;
 
-__global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(TileArgs A)
+static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(TileArgs A)
 {
     extern __shared__ unsigned char s_raw[];
     PipeSmem &S = *reinterpret_cast<PipeSmem *>((reinterpret_cast<uintptr_t>(s_raw) + 127) & ~uintptr_t(127));
@@ -781,7 +781,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(TileArgs A)
 // Grid update of the nodes of marked tiles (simulation/kernels.cuh:164-301),
 // one thread per node; zeroes the accumulators for the next step.  The marks
 // are cleared by the caller afterwards.
-__global__ void __launch_bounds__(256) k_update_nodes(StepParams P, TileGeom G, GridView g,
+static __global__ void __launch_bounds__(256) k_update_nodes(StepParams P, TileGeom G, GridView g,
                                                       const unsigned *__restrict__ flags, long n_nodes,
                                                       double ind_x, double ind_y, double *acc)
 {

@@ -248,6 +248,46 @@ int icy_mpm_profile_read(icy_mpm *h, int max, char *names, double *ms_total,
                          int64_t *launches, int *count);
 
 /* ------------------------------------------------------------------ */
+/* batches of independent instances                                     */
+/* ------------------------------------------------------------------ */
+/*
+ * No counterpart in the reference (which runs one scenario per process).
+ * A batch advances many independent floe scenarios together on one GPU:
+ * every member is an FP32 split-precision instance with its own parameters,
+ * grid and points, and one batch step is four kernel launches whatever the
+ * number of members (clocks, grid update, mark clearing, tile kernel over
+ * the (member, tile) work list), replayed as a CUDA graph per step count.
+ * Each member keeps its own simulation time and step index on the device,
+ * so members admitted at different times progress independently.
+ */
+typedef struct icy_batch icy_batch;
+int icy_batch_create(int device, int max_instances, icy_batch **out);
+int icy_batch_destroy(icy_batch *b);
+/* Admit a scenario (SimParams + HSSOA, line stride = capacity, `size` points);
+   *slot receives its member index.  ICY_ERR_NO_SPACE if all slots are taken. */
+int icy_batch_add(icy_batch *b, const icy_sim_params *p, const double *hssoa,
+                  unsigned capacity, unsigned size, int *slot);
+/* Free a member's slot and device memory. */
+int icy_batch_remove(icy_batch *b, int slot);
+/* Advance every member by nsteps sub-steps of icy::Model::Step (asynchronous). */
+int icy_batch_step(icy_batch *b, int nsteps);
+/* Download one member: HSSOA in its upload order, indenter bins (may be
+   NULL), its simulation time and next step index (may be NULL); synchronises. */
+int icy_batch_download(icy_batch *b, int slot, double *hssoa, unsigned capacity,
+                       unsigned *size, double *bins, double *sim_time, int64_t *step);
+int icy_batch_synchronize(icy_batch *b);
+/* "resort_every" (steps between re-binning, 0 = never), "tile_ctas"
+   (persistent CTAs of the tile kernel). */
+int icy_batch_set_option(icy_batch *b, const char *name, double value);
+/* Live members, their total points, kernels launched so far, the batch stream. */
+int icy_batch_info(icy_batch *b, int *live, int64_t *points, int64_t *kernel_launches,
+                   void **stream);
+/* Device bytes of one member. */
+int64_t icy_batch_device_bytes(icy_batch *b, int slot);
+/* Device bytes an instance of this size and precision allocates. */
+int64_t icy_mpm_device_bytes(const icy_sim_params *p, unsigned capacity, int precision);
+
+/* ------------------------------------------------------------------ */
 /* stepping without allocation                                          */
 /* ------------------------------------------------------------------ */
 /*

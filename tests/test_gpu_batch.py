@@ -1,0 +1,95 @@
+"""GPU tests of batches of independent scenarios (icy_batch_*): every member
+matches its own single-instance FP32 run and the FP64 oracle, members added
+at different times keep their own clocks, slots are reused after removal."""
+import numpy as np
+import pytest
+
+from icempm_multi_b200 import GPUImplementation
+from icempm_multi_b200._lib import PRECISION_FP32_SPLIT
+from icempm_multi_b200.batch import Batch
+from scenarios import standard, stress
+from test_gpu_parity import field_errors
+from test_gpu_split import POS_TOL
+
+pytestmark = pytest.mark.gpu
+
+
+def single_f32(p, soa, steps, chunk):
+    out = soa.clone()
+    g = GPUImplementation(p, out, precision=PRECISION_FP32_SPLIT)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.reset_indenter_force_accumulator()
+    t, done = 0.0, 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        t = g.run_steps(done, k, t)
+        done += k
+    g.transfer_from_device()
+    g.close()
+    return out, t
+
+
+def scenarios():
+    return [standard(seed=31), standard(n_cells_x=20, n_cells_y=6, grid=(64, 32), seed=32, IndVelocity=2.0),
+            stress(seed=33), standard(n_cells_x=40, n_cells_y=10, grid=(128, 48), seed=34, DP_phi=45),
+            standard(n_cells_x=12, n_cells_y=12, grid=(64, 64), seed=35, YoungsModulus=5e8)]
+
+
+@pytest.fixture(scope="module")
+def oracle(built):
+    from oracle.oracle import Oracle
+    return Oracle()
+
+
+def test_batch_members_match_single_and_oracle(oracle):
+    sc = scenarios()
+    b = Batch(8)
+    slots = [b.add(p, soa) for p, soa in sc]
+    b.step(40)
+    b.step(40)
+    for (p, soa), s in zip(sc, slots):
+        out = soa.clone()
+        t, step, bins = b.download(s, out)
+        assert step == 80
+        tt = 0.0
+        for _ in range(80):
+            tt += p.InitialTimeStep
+        assert t == tt                       # the host recurrence of Model::Step, exactly
+        one, t1 = single_f32(p, soa, 80, 40)
+        assert t1 == t
+        e1 = field_errors(out, one)
+        assert e1["pos"] <= 1e-6, e1
+        ref = soa.clone()
+        assert oracle.run(p, ref, 0, 80)[0] == 0
+        assert field_errors(out, ref)["pos"] <= POS_TOL
+    info = b.info()
+    assert info["live"] == 5 and info["kernel_launches"] > 0
+    b.close()
+
+
+def test_batch_members_keep_their_own_clock(oracle):
+    (pa, sa), (pb, sb) = standard(seed=41), standard(n_cells_x=16, n_cells_y=6, grid=(64, 32), seed=42)
+    b = Batch(4)
+    a = b.add(pa, sa)
+    b.step(30)
+    c = b.add(pb, sb)
+    b.step(30)
+    oa, ob = sa.clone(), sb.clone()
+    _, step_a, _ = b.download(a, oa)
+    _, step_c, _ = b.download(c, ob)
+    assert (step_a, step_c) == (60, 30)
+    ra, rb = sa.clone(), sb.clone()
+    oracle.run(pa, ra, 0, 60)
+    oracle.run(pb, rb, 0, 30)
+    assert field_errors(oa, ra)["pos"] <= POS_TOL
+    assert field_errors(ob, rb)["pos"] <= POS_TOL
+    # free a slot and reuse it
+    b.remove(a)
+    d = b.add(pa, sa)
+    assert d == a
+    b.step(10)
+    od = sa.clone()
+    _, step_d, _ = b.download(d, od)
+    assert step_d == 10
+    b.close()
