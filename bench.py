@@ -1,14 +1,18 @@
 #!/usr/bin/env python
 """Benchmark of the MLS-MPM hot path (particle-steps/s) on one or more B200s.
 
-Workload: the single large instance -- grid 4096 x 2048 cells at h = 0.05 m,
-an ice block of 150 m x 40 m at 4 points per cell (9.6 M points, 1.23 GB of
-FP64 particle state), dt = 2e-5 s, E = 1 GPa, nu = 0.3, rho = 980, friction
-angle 62 deg, cohesion 0, gravity 9.81, indenter radius 1 m at 1 m/s.  The
-points are seeded synthetic (no point-cloud files are available).  One bench
-step = one MPM sub-step (grid reset, P2G, grid update, G2P + return mapping)
-over the whole instance.  The particle state (1.23 GB) is larger than L2, so
-no extra flush is done between steps.
+Headline workload: the single large instance -- grid 4096 x 2048 cells at
+h = 0.05 m, an ice block of 150 m x 40 m at 4 points per cell (9.6 M points),
+dt = 2e-5 s, E = 1 GPa, nu = 0.3, rho = 980, friction angle 62 deg, cohesion 0,
+gravity 9.81, indenter radius 1 m at 1 m/s; seeded synthetic points (no
+point-cloud files are available).  One bench step = one MPM sub-step (P2G,
+grid update, G2P + return mapping) over the whole instance.  `value` is the
+FP32 split-precision path (its accuracy, <= 1e-4 relative position error
+against the FP64 oracle after 1000 steps, is a GPU test); the plain FP64
+drop-in path is measured on the same instance and reported under "fp64".
+The particle state (0.65 GB FP32, 1.23 GB FP64) is larger than L2, so no extra
+flush is done between steps.  Also reported: a batch of independent
+scenarios ("batched") and a served Poisson request stream ("served").
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -203,6 +207,134 @@ def run_reference_arm(args):
     return 0
 
 
+
+
+def measure_instance(p, soa, precision, steps, warmup, local, pg, opts=(), profile=True, clocks=True):
+    """Device-timed steps of one instance (inputs resident in HBM)."""
+    import torch
+    from icempm_multi_b200 import GPUImplementation
+    from icempm_multi_b200._lib import PRECISION_FP32_SPLIT, PRECISION_FP64
+    prec = PRECISION_FP32_SPLIT if precision == "fp32" else PRECISION_FP64
+    stream = torch.cuda.Stream(device=local)
+    g = GPUImplementation(p, soa, device=local, precision=prec)
+    g.set_stream(stream.cuda_stream)
+    for o in opts:
+        k, v = o.split("=", 1)
+        g.set_option(k, float(v))
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.reset_indenter_force_accumulator()
+    t_sim = g.run_steps(0, warmup, 0.0)
+    torch.cuda.synchronize()
+    barrier(pg, local)
+    torch.cuda.synchronize()
+    l0 = g.kernel_launches()
+    if profile:
+        g.profile(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local) if clocks else None
+    if sampler:
+        sampler.__enter__()
+    ev0.record(stream)
+    t_sim = g.run_steps(warmup, steps, t_sim)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__exit__(None, None, None)
+    barrier(pg, local)
+    ms = ev0.elapsed_time(ev1)
+    launches = g.kernel_launches() - l0
+    prof = g.profile_read() if profile else {}
+    g.profile(False)
+    return g, stream, {"ms": ms, "launches": launches, "prof": prof,
+                       "clocks": sampler.summary() if sampler else None}
+
+
+def measure_e2e(g, stream, soa, steps, frame, local, pg):
+    """End to end through the C-ABI with host buffers: upload the HSSOA from
+    pinned host memory, run the steps with the reference's frame structure (a
+    full HSSOA download every UpdateEveryNthStep sub-steps and at the end)."""
+    import torch
+    barrier(pg, local)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    downloads = 0
+    w0 = time.perf_counter()
+    e0.record(stream)
+    g.transfer_ponts_to_device()
+    done, t2 = 0, 0.0
+    while done < steps:
+        k = min(frame, steps - done)
+        t2 = g.run_steps(done, k, t2)
+        done += k
+        g.transfer_from_device()   # synchronous download, as Model::Step does
+        downloads += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - w0
+    return max(e0.elapsed_time(e1), wall * 1e3), downloads
+
+
+def measure_batch(n_instances=256, steps=100, seed=7):
+    """The batched workload: n_instances floe scenarios (points log-uniform
+    10k-500k, E 5e8-2e9 Pa, friction angle 45-70 deg, indenter 0.5-3 m/s,
+    CFL time steps) advanced together, one graph replay per call."""
+    import torch
+    from icempm_multi_b200.batch import Batch
+    from icempm_multi_b200.workloads import batch_scenarios, make_workload as mk
+    ws = batch_scenarios(n_instances, seed=seed)
+    b = Batch(n_instances)
+    npts = 0
+    for w in ws:
+        p, soa = mk(w)
+        b.add(p, soa)
+        npts += soa.size
+    b.step(steps)            # captures the graph for this step count, warms up
+    b.synchronize()
+    stream = torch.cuda.ExternalStream(b.info()["stream"])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.info()["kernel_launches"]
+    e0.record(stream)
+    b.step(steps)
+    e1.record(stream)
+    b.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = b.info()["kernel_launches"] - l0
+    b.close()
+    return {"value": npts * steps / (ms / 1e3), "unit": METRIC, "instances": n_instances, "points": npts,
+            "steps": steps, "ms_per_step": ms / steps, "gpu_launches": int(launches),
+            "workload": "floe scenarios: points log-uniform 10k-500k, grids 128x128..1024x512 (h=0.1 m), "
+                        "E U(5e8,2e9), phi U(45,70), indenter U(0.5,3) m/s, CFL dt, FP32 split, CUDA graph"}
+
+
+def measure_serve(rate_load=0.7, duration=12.0, batch_rate=None, seed=11):
+    """Served Poisson request stream: scenarios of 5k-2M points (log-uniform),
+    200-5000 steps, admitted by a 150 GB device-memory budget, continuous
+    batching in rounds of 50 steps; p50/p99 completion latency."""
+    import numpy as np
+    from icempm_multi_b200.serve import Server, poisson_requests
+    from icempm_multi_b200.workloads import floe_scenario, make_workload as mk
+    rng = np.random.default_rng(seed)
+    scenes = []
+    for k in range(16):
+        n = int(round(np.exp(rng.uniform(np.log(5e3), np.log(2e6)))))
+        w = floe_scenario(n, E=float(rng.uniform(5e8, 2e9)), phi=float(rng.uniform(45, 70)),
+                          v_ind=float(rng.uniform(0.5, 3.0)), seed=seed * 100 + k)
+        scenes.append(mk(w))
+    mean_pts = float(np.mean([s.size for _, s in scenes]))
+    mean_steps = 2600.0
+    rate = rate_load * (batch_rate or 2e10) / (mean_pts * mean_steps)
+    n_req = max(8, int(rate * duration))
+    reqs = poisson_requests(scenes, rate, n_req, round_steps=50, seed=seed)
+    srv = Server(budget_bytes=150e9, round_steps=50, keep_results=False)
+    st = srv.run(reqs)
+    srv.close()
+    st.update({"arrival_rate_per_s": rate, "budget_bytes": 150e9, "round_steps": 50, "unit": METRIC,
+               "workload": "Poisson arrivals, points log-uniform 5k-2M, steps U(200,5000), FP32 split, "
+                           "150 GB budget, continuous batching"})
+    return st
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -211,8 +343,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ref-gpu", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
-                    help="fp64: the plain drop-in path; fp32: split precision")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
+                    help="path of the headline value: fp32 split precision (default) or fp64")
     ap.add_argument("--opt", action="append", default=[],
                     help="instance option name=value (icy_mpm_set_option), repeatable")
     args = ap.parse_args()
@@ -220,85 +353,29 @@ def main():
     if args.impl == "reference":
         return run_reference_arm(args)
 
-    import numpy as np
     import torch
-    from icempm_multi_b200 import GPUImplementation
-    from icempm_multi_b200._lib import lib
 
     rank, world, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     p, soa = make_workload(pinned=True)
     n = soa.size
-    stream = torch.cuda.Stream(device=local)
-    from icempm_multi_b200._lib import PRECISION_FP32_SPLIT, PRECISION_FP64
-    prec = PRECISION_FP32_SPLIT if args.precision == "fp32" else PRECISION_FP64
-    g = GPUImplementation(p, soa, device=local, precision=prec)
-    g.set_stream(stream.cuda_stream)
-    for o in args.opt:
-        k, v = o.split("=", 1)
-        g.set_option(k, float(v))
-    g.update_constants()
-    g.transfer_ponts_to_device()
-    g.reset_indenter_force_accumulator()
-    t_sim = 0.0
-    with torch.cuda.stream(stream):
-        t_sim = g.run_steps(0, args.warmup, t_sim)
-    torch.cuda.synchronize()
 
-    # ---- device-resident timed region --------------------------------------------------
-    barrier(pg, local)
-    torch.cuda.synchronize()
-    l0 = g.kernel_launches()
-    g.profile(True)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-            t_sim = g.run_steps(args.warmup, args.steps, t_sim)
-            ev1.record(stream)
-        torch.cuda.synchronize()
-    barrier(pg, local)
-    ms_local = ev0.elapsed_time(ev1)
-    launches = g.kernel_launches() - l0
-    prof = g.profile_read()
-    g.profile(False)
-    ms = max_over_ranks(pg, ms_local, local)
+    # ---- headline path, device-resident timed region ----------------------------------
+    g, stream, r = measure_instance(p, soa, args.precision, args.steps, args.warmup, local, pg, args.opt)
+    ms = max_over_ranks(pg, r["ms"], local)
     value = n * args.steps * world / (ms / 1e3)
 
     # ---- end to end through the C-ABI with host buffers ----------------------------------
-    # upload the HSSOA from pinned host memory, run the steps with the reference's
-    # frame structure (a full HSSOA download every UpdateEveryNthStep sub-steps and
-    # at the end), all inside the timed region
     frame = p.UpdateEveryNthStep
-    host = soa
-    barrier(pg, local)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    downloads = 0
-    w0 = time.perf_counter()
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-        g.transfer_ponts_to_device()
-        done = 0
-        t2 = 0.0
-        while done < args.steps:
-            k = min(frame, args.steps - done)
-            t2 = g.run_steps(done, k, t2)
-            done += k
-            g.transfer_from_device()     # synchronous download, as Model::Step does
-            downloads += 1
-        e1.record(stream)
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - w0
-    ms_e2e = max_over_ranks(pg, max(e0.elapsed_time(e1), wall * 1e3), local)
+    ms_e2e, downloads = measure_e2e(g, stream, soa, args.steps, frame, local, pg)
+    ms_e2e = max_over_ranks(pg, ms_e2e, local)
     e2e_value = n * args.steps * world / (ms_e2e / 1e3)
-    h2d = 16 * 8 * n / args.steps
-    d2h = 16 * 8 * n * downloads / args.steps
+    g.close()
 
     # ---- roofline of the dominant kernel ------------------------------------------------
     peak, peak_kind = peaks()
-    dom = max(prof.items(), key=lambda kv: kv[1][0]) if prof else (None, (0, 0))
-    name, (tot_ms, cnt) = dom
+    prof = r["prof"]
+    name, (tot_ms, cnt) = max(prof.items(), key=lambda kv: kv[1][0]) if prof else (None, (0, 0))
     per_launch_ms = tot_ms / max(cnt, 1)
     alg = (ALG_BYTES_F32 if args.precision == "fp32" else ALG_BYTES).get(name, 0) * n
     achieved = alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
@@ -306,7 +383,7 @@ def main():
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(name)
+            traffic = json.load(open(tf)).get(f"{name}:{args.precision}")
         except Exception:
             traffic = None
 
@@ -316,43 +393,59 @@ def main():
         "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
         "config": {"workload": "single large instance: grid 4096x2048 h=0.05 m, 150x40 m block, 4 ppc, "
                                "dt=2e-5, E=1e9, phi=62, indenter r=1 m at 1 m/s",
-                   "points": n, "precision": args.precision,
-                   "l2": "inputs larger than L2 (particle state 0.65-1.23 GB)",
-                   "replicas": world, "options": args.opt},
-        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "frame_steps": frame, "downloads": downloads},
-        "gpu_launches": int(launches),
+                   "points": n, "precision": args.precision + (" split" if args.precision == "fp32" else ""),
+                   "l2": "inputs larger than L2 (particle state 0.65-1.23 GB)", "replicas": world,
+                   "options": args.opt},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 16 * 8 * n / args.steps,
+                "d2h_bytes_per_step": 16 * 8 * n * downloads / args.steps, "frame_steps": frame,
+                "downloads": downloads},
+        "gpu_launches": int(r["launches"]),
         "kernels": {k: {"ms_total": v[0], "launches": v[1], "ms_per_launch": v[0] / max(v[1], 1)}
                     for k, v in prof.items()},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if peak else None, "traffic": traffic,
-                     "peak_kind": peak_kind, "alg_bytes_per_launch": alg},
-        "clocks": clk.summary(),
+                     "frac": achieved / peak if peak else None, "traffic": traffic, "peak_kind": peak_kind,
+                     "alg_bytes_per_launch": alg},
+        "clocks": r["clocks"],
     }
-    g.close()
 
-    # ---- reference kernels built for sm_100a on the same GPU (a few steps) -----------------
-    if rank == 0 and world == 1 and not args.no_ref_gpu:
-        try:
-            from oracle.oracle import RefCuda
-            work = soa.clone(pinned=False)
-            k = min(args.steps, 50)
-            err, _, _, rms = RefCuda().run(p, work, 0, k, 0.0)
-            out["reference_sm100a"] = {"value": n * k / (rms / 1e3), "unit": METRIC, "steps": k,
-                                       "error_code": err,
-                                       "what": "reference kernels.cuh built for sm_100a, one partition"}
-        except Exception as e:  # informational only
-            out["reference_sm100a"] = {"unavailable": str(e)[:200]}
+    # ---- the other precision on the same instance -----------------------------------------
+    other = "fp64" if args.precision == "fp32" else "fp32"
+    g2, _, r2 = measure_instance(p, soa, other, min(args.steps, 100), args.warmup, local, pg, profile=True,
+                                 clocks=False)
+    g2.close()
+    ms2 = max_over_ranks(pg, r2["ms"], local)
+    out[other] = {"value": n * min(args.steps, 100) * world / (ms2 / 1e3), "unit": METRIC,
+                  "ms_per_step": ms2 / min(args.steps, 100),
+                  "kernels": {k: v[0] / max(v[1], 1) for k, v in r2["prof"].items()}}
 
-    # ---- CPU baseline (rank 0, N = 1) ---------------------------------------------------------
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            v, steps, threads, secs, err = cpu_reference_rate(p, soa)
-            out["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
-                                   "sample": f"{steps} sub-steps of the full {n}-point instance "
-                                             f"({secs:.1f} s), reference kernels built for the host, OpenMP"}
-        except Exception as e:
-            out["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    if rank == 0 and world == 1:
+        # ---- reference kernels built for sm_100a on the same GPU (a few steps) -----------
+        if not args.no_ref_gpu:
+            try:
+                from oracle.oracle import RefCuda
+                work = soa.clone(pinned=False)
+                k = min(args.steps, 50)
+                err, _, _, rms = RefCuda().run(p, work, 0, k, 0.0)
+                out["reference_sm100a"] = {"value": n * k / (rms / 1e3), "unit": METRIC, "steps": k,
+                                           "error_code": err, "precision": "fp64",
+                                           "what": "reference kernels.cuh built for sm_100a, one partition"}
+            except Exception as e:  # informational only
+                out["reference_sm100a"] = {"unavailable": str(e)[:200]}
+        if not args.no_extra:
+            try:
+                out["batched"] = measure_batch()
+                out["served"] = measure_serve(batch_rate=out["batched"]["value"])
+            except Exception as e:
+                out["batched_or_served_error"] = str(e)[:300]
+        # ---- CPU baseline ------------------------------------------------------------------
+        if not args.no_cpu_baseline:
+            try:
+                v, steps, threads, secs, err = cpu_reference_rate(p, soa)
+                out["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
+                                       "sample": f"{steps} sub-steps of the full {n}-point instance "
+                                                 f"({secs:.1f} s), reference kernels built for the host, OpenMP"}
+            except Exception as e:
+                out["cpu_baseline"] = {"unavailable": str(e)[:200]}
     if rank == 0:
         print(json.dumps(out), flush=True)
     if pg is not None:

@@ -1,0 +1,149 @@
+"""Serving floe-indentation scenarios with continuous batching on one GPU.
+
+Requests arrive over time (e.g. a Poisson process); each asks for a scenario
+(SimParams + initial HSSOA) to be advanced by a number of sub-steps.  The
+server keeps every admitted scenario's state resident on the device as a
+member of one Batch, advances all members together in rounds of
+`round_steps` sub-steps, and between rounds:
+  * downloads and releases the members that have done their steps,
+  * admits waiting requests, first come first served, while their device
+    memory fits the budget and a slot is free.
+So requests that arrive while others run join the running batch as memory
+frees up, and their work overlaps on the device.  Completion latency is
+measured from arrival to the end of the result download.
+
+This is host-side scheduling over the icy_batch_* C-ABI; the reference has
+no counterpart (it runs one scenario per process).
+"""
+import collections
+import dataclasses
+import time
+
+import numpy as np
+
+from .batch import Batch, device_bytes
+from .hssoa import HostSideSOA
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    arrival: float              # seconds after the start of the run
+    params: object              # SimParams
+    soa: HostSideSOA            # initial state (kept only until admission)
+    steps: int                  # sub-steps to run (a multiple of the round length)
+    slot: int = -1
+    admitted: float = None
+    done: float = None
+    steps_done: int = 0
+    bytes: int = 0
+    result: HostSideSOA = None
+    sim_time: float = None
+    bins: np.ndarray = None
+
+    @property
+    def points(self):
+        return self.soa.size if self.soa is not None else (self.result.size if self.result is not None else 0)
+
+
+class Server:
+    def __init__(self, budget_bytes=150e9, max_instances=1024, round_steps=50, device=0, keep_results=True):
+        self.batch = Batch(max_instances, device=device)
+        self.budget = float(budget_bytes)
+        self.round_steps = int(round_steps)
+        self.max_instances = int(max_instances)
+        self.keep_results = keep_results
+        self.used = 0.0
+        self.running = {}
+        self.queue = collections.deque()
+        self.completed = []
+        self.rounds = 0
+        self.peak_live = 0
+        self.peak_bytes = 0.0
+
+    def close(self):
+        self.batch.close()
+
+    def _admit(self, now):
+        while self.queue and len(self.running) < self.max_instances:
+            r = self.queue[0]
+            need = device_bytes(r.params, r.soa.capacity)
+            if self.used + need > self.budget:
+                if not self.running:   # larger than the whole budget: refuse instead of waiting forever
+                    raise RuntimeError(f"request {r.rid} needs {need} bytes, budget {self.budget}")
+                break
+            self.queue.popleft()
+            r.slot = self.batch.add(r.params, r.soa)
+            r.bytes = need
+            r.admitted = now
+            self.used += need
+            self.running[r.slot] = r
+        self.peak_live = max(self.peak_live, len(self.running))
+        self.peak_bytes = max(self.peak_bytes, self.used)
+
+    def _complete(self, t0):
+        for slot, r in list(self.running.items()):
+            if r.steps_done >= r.steps:
+                out = HostSideSOA(r.soa.capacity)
+                r.sim_time, _, r.bins = self.batch.download(slot, out)
+                self.batch.remove(slot)
+                r.done = time.perf_counter() - t0
+                if self.keep_results:
+                    r.result = out
+                self.used -= r.bytes
+                del self.running[slot]
+                self.completed.append(r)
+
+    def run(self, requests):
+        """Serve `requests` (arrival times relative to now); returns stats."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        pi = 0
+        work = 0.0
+        t0 = time.perf_counter()
+        while pi < len(pending) or self.queue or self.running:
+            now = time.perf_counter() - t0
+            while pi < len(pending) and pending[pi].arrival <= now:
+                self.queue.append(pending[pi])
+                pi += 1
+            self._admit(now)
+            if not self.running:
+                if pi < len(pending):
+                    time.sleep(max(0.0, min(0.01, pending[pi].arrival - now)))
+                continue
+            self.batch.step(self.round_steps)
+            self.batch.synchronize()
+            self.rounds += 1
+            for r in self.running.values():
+                r.steps_done += self.round_steps
+                work += r.points * self.round_steps
+            self._complete(t0)
+        makespan = time.perf_counter() - t0
+        lat = np.array([r.done - r.arrival for r in self.completed]) if self.completed else np.zeros(1)
+        return {
+            "requests": len(self.completed),
+            "makespan_s": makespan,
+            "particle_steps": work,
+            "particle_steps_per_s": work / makespan if makespan > 0 else 0.0,
+            "latency_p50_s": float(np.percentile(lat, 50)),
+            "latency_p99_s": float(np.percentile(lat, 99)),
+            "latency_mean_s": float(lat.mean()),
+            "rounds": self.rounds,
+            "peak_live": self.peak_live,
+            "peak_device_bytes": self.peak_bytes,
+        }
+
+
+def poisson_requests(scenes, rate, n, steps_range=(200, 5000), round_steps=50, seed=11):
+    """n requests at Poisson arrival `rate` (per second); each takes a scene
+    (params, soa) from `scenes` in turn and a step count uniform in
+    steps_range, rounded to a multiple of round_steps."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    lo, hi = steps_range
+    for k in range(n):
+        t += rng.exponential(1.0 / rate)
+        p, soa = scenes[k % len(scenes)]
+        steps = int(rng.integers(lo // round_steps, hi // round_steps + 1)) * round_steps
+        out.append(Request(rid=k, arrival=t, params=p.copy(), soa=soa, steps=max(steps, round_steps)))
+    return out

@@ -41,3 +41,56 @@ def make_workload(w, pinned=False):
     soa = make_block(p, w["block_w"], w["block_h"], ppc=w["ppc"], seed=w["seed"], n_grains=w["n_grains"],
                      pinned=pinned)
     return p, soa
+
+
+# ---------------------------------------------------------------- many scenarios
+# grids available to batched / served scenarios (cells), smallest that fits first
+GRIDS = [(128, 128), (256, 128), (256, 256), (512, 256), (512, 512), (1024, 512), (2048, 512), (2048, 1024)]
+
+
+def wave_speed(E, nu, rho):
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    return ((lam + 2 * mu) / rho) ** 0.5
+
+
+def cfl_dt(E, nu, rho, h, courant=0.4):
+    """Explicit time step with c dt / h = courant (c: P-wave speed), rounded
+    down to 2 significant digits."""
+    import math
+    dt = courant * h / wave_speed(E, nu, rho)
+    e = math.floor(math.log10(dt))
+    return math.floor(dt / 10 ** (e - 1)) * 10 ** (e - 1)
+
+
+def floe_scenario(n_points, E, phi, v_ind, seed, h=0.1, aspect=4.0, ppc=4, nu=0.3, rho=980.0):
+    """A floe-indentation scenario of about n_points points: a block of
+    aspect:1 cells at ppc points per cell on the smallest grid of GRIDS that
+    leaves room around it, dt from the CFL condition."""
+    import math
+    cells = max(n_points // ppc, 16)
+    ch = max(4, int(round(math.sqrt(cells / aspect))))
+    cw = max(4, cells // ch)
+    for gx, gy in GRIDS:
+        if cw + 24 <= gx and ch + 16 <= gy:
+            break
+    else:
+        gx, gy = GRIDS[-1]
+    w = dict(grid_x=gx, grid_y=gy, h=h, block_w=cw * h, block_h=ch * h, ppc=ppc,
+             dt=cfl_dt(E, nu, rho, h), E=E, nu=nu, rho=rho, phi=phi, cohesion=0.0,
+             ind_radius=1.0, ind_velocity=v_ind, ind_depth=0.5, seed=seed, n_grains=16)
+    return w
+
+
+def batch_scenarios(n_instances=256, seed=7, n_min=10_000, n_max=500_000):
+    """The batched workload: particle counts log-uniform in [n_min, n_max],
+    E uniform 5e8-2e9 Pa, friction angle uniform 45-70 deg, indenter speed
+    uniform 0.5-3 m/s (seeded)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_instances):
+        n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+        out.append(floe_scenario(n, E=float(rng.uniform(5e8, 2e9)), phi=float(rng.uniform(45, 70)),
+                                 v_ind=float(rng.uniform(0.5, 3.0)), seed=seed * 1000 + k))
+    return out

@@ -1,0 +1,74 @@
+"""GPU tests of the serving loop (continuous batching by device-memory budget):
+requests that arrive while others run are admitted and run alongside them,
+the budget bounds how many are resident, and every result is the same alone
+and in the mix (relative L2 position difference <= 1e-6; FP32 grid sums are
+accumulated in a different order in a different mix) and within the FP32
+target of the FP64 oracle."""
+import pytest
+
+from icempm_multi_b200.batch import device_bytes
+from icempm_multi_b200.serve import Request, Server
+from scenarios import standard, stress
+from test_gpu_parity import field_errors
+from test_gpu_split import POS_TOL
+
+pytestmark = pytest.mark.gpu
+
+MIX_TOL = 1e-6
+
+
+def scenes():
+    return [standard(seed=51), standard(n_cells_x=20, n_cells_y=6, grid=(64, 32), seed=52), stress(seed=53),
+            standard(n_cells_x=36, n_cells_y=9, grid=(128, 48), seed=54, IndVelocity=2.5)]
+
+
+def requests(sc, arrivals, steps):
+    return [Request(rid=k, arrival=a, params=sc[k % len(sc)][0].copy(), soa=sc[k % len(sc)][1], steps=s)
+            for k, (a, s) in enumerate(zip(arrivals, steps))]
+
+
+@pytest.fixture(scope="module")
+def oracle(built):
+    from oracle.oracle import Oracle
+    return Oracle()
+
+
+def test_serving_mix_matches_alone(oracle):
+    sc = scenes()
+    arrivals = [0.0, 0.0, 0.05, 0.1, 0.15, 0.2]
+    steps = [120, 60, 80, 100, 40, 60]
+    srv = Server(budget_bytes=8e9, round_steps=20)
+    stats = srv.run(requests(sc, arrivals, steps))
+    srv.close()
+    assert stats["requests"] == 6
+    assert stats["peak_live"] > 1                     # work overlapped on the device
+    done = {r.rid: r for r in srv.completed}
+    # a request that arrived while others were running joined them
+    assert any(r.admitted < max(o.done for o in done.values() if o.rid != r.rid) and r.arrival > 0
+               for r in done.values())
+    for rid in (0, 2, 3):
+        alone = Server(budget_bytes=8e9, round_steps=20)
+        alone.run(requests(sc, [0.0], [steps[rid]]) if rid == 0 else
+                  [Request(rid=0, arrival=0.0, params=sc[rid % len(sc)][0].copy(), soa=sc[rid % len(sc)][1],
+                           steps=steps[rid])])
+        a = alone.completed[0]
+        alone.close()
+        m = done[rid]
+        assert m.steps_done == a.steps_done == steps[rid]
+        assert m.sim_time == a.sim_time
+        e = field_errors(m.result, a.result)
+        assert e["pos"] <= MIX_TOL, (rid, e)
+        ref = sc[rid % len(sc)][1].clone()
+        assert oracle.run(sc[rid % len(sc)][0], ref, 0, steps[rid])[0] == 0
+        assert field_errors(m.result, ref)["pos"] <= POS_TOL
+
+
+def test_serving_budget_bounds_residency():
+    sc = scenes()
+    one = max(device_bytes(p, s.capacity) for p, s in sc)
+    srv = Server(budget_bytes=2.2 * one, round_steps=20)
+    stats = srv.run(requests(sc, [0.0] * 5, [40] * 5))
+    srv.close()
+    assert stats["requests"] == 5
+    assert stats["peak_live"] <= 2
+    assert stats["peak_device_bytes"] <= 2.2 * one
