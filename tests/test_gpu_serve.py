@@ -64,8 +64,8 @@ def test_serving_mix_matches_alone(oracle):
 
 
 def test_serving_budget_bounds_residency():
-    sc = scenes()
-    one = max(device_bytes(p, s.capacity) for p, s in sc)
+    sc = [scenes()[0]]                       # five requests of the same size
+    one = device_bytes(sc[0][0], sc[0][1].capacity)
     srv = Server(budget_bytes=2.2 * one, round_steps=20)
     stats = srv.run(requests(sc, [0.0] * 5, [40] * 5))
     srv.close()
