@@ -32,7 +32,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from icempm_multi_b200.workloads import LARGE as WORKLOAD  # noqa: E402
+from icempm_multi_b200.workloads import LARGE, MEDIUM  # noqa: E402
 from icempm_multi_b200.workloads import make_workload as _make, workload_params  # noqa: E402
 
 METRIC = "particle-steps/s"
@@ -47,6 +47,16 @@ ALG_BYTES = {"k_p2g_simple": 13 * 8, "k_g2p_simple": (8 + 14) * 8,
 # FP32 split state: 4-byte utility, packed cell, offset (2), Fe - I (4), Jp = 9 words
 # read and written by the fused step
 ALG_BYTES_F32 = {"k_tile_g2p2g": (9 + 9) * 4, "k_tile_p2g": 15 * 4, "k_tile_g2p": (9 + 15) * 4}
+
+
+WORKLOAD = LARGE
+
+
+def workload_desc():
+    w = WORKLOAD
+    return (f"single instance: grid {w['grid_x']}x{w['grid_y']} h={w['h']} m, {w['block_w']:g}x{w['block_h']:g} m "
+            f"block, {w['ppc']} ppc, dt={w['dt']:g}, E={w['E']:g}, phi={w['phi']:g}, "
+            f"indenter r={w['ind_radius']:g} m at {w['ind_velocity']:g} m/s")
 
 
 def make_workload(pinned):
@@ -197,7 +207,7 @@ def run_reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "error_code": err,
-        "config": {"workload": "single large FP64 instance, grid 4096x2048 h=0.05, 150x40 m block, 4 ppc",
+        "config": {"workload": workload_desc() + ", FP64",
                    "points": soa.size, "dt": WORKLOAD["dt"]},
         "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
                          "sample": desc + ", reference kernels (simulation/kernels.cuh) built for the host, OpenMP"},
@@ -342,14 +352,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-ref-gpu", action="store_true")
-    ap.add_argument("--no-extra", action="store_true", help="skip the batched and served measurements")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="time only the headline path (no other precision, batched or served legs)")
+    ap.add_argument("--workload", default="large", choices=["large", "medium"],
+                    help="large: the 9.6 M-point headline instance; medium: the 4.8 M-point profiling case")
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
                     help="path of the headline value: fp32 split precision (default) or fp64")
     ap.add_argument("--opt", action="append", default=[],
                     help="instance option name=value (icy_mpm_set_option), repeatable")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global WORKLOAD
+    WORKLOAD = LARGE if args.workload == "large" else MEDIUM
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -391,10 +405,10 @@ def main():
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic",
-        "config": {"workload": "single large instance: grid 4096x2048 h=0.05 m, 150x40 m block, 4 ppc, "
-                               "dt=2e-5, E=1e9, phi=62, indenter r=1 m at 1 m/s",
+        "config": {"workload": workload_desc(),
                    "points": n, "precision": args.precision + (" split" if args.precision == "fp32" else ""),
-                   "l2": "inputs larger than L2 (particle state 0.65-1.23 GB)", "replicas": world,
+                   "l2": f"inputs larger than L2 (particle state {n * (36 if args.precision == 'fp32' else 128) / 1e9:.2f} GB "
+                         "read and written per step; no extra flush)", "replicas": world,
                    "options": args.opt},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 16 * 8 * n / args.steps,
                 "d2h_bytes_per_step": 16 * 8 * n * downloads / args.steps, "frame_steps": frame,
@@ -409,28 +423,16 @@ def main():
     }
 
     # ---- the other precision on the same instance -----------------------------------------
-    other = "fp64" if args.precision == "fp32" else "fp32"
-    g2, _, r2 = measure_instance(p, soa, other, min(args.steps, 100), args.warmup, local, pg, profile=True,
-                                 clocks=False)
-    g2.close()
-    ms2 = max_over_ranks(pg, r2["ms"], local)
-    out[other] = {"value": n * min(args.steps, 100) * world / (ms2 / 1e3), "unit": METRIC,
-                  "ms_per_step": ms2 / min(args.steps, 100),
-                  "kernels": {k: v[0] / max(v[1], 1) for k, v in r2["prof"].items()}}
+    if not args.no_extra:
+        other = "fp64" if args.precision == "fp32" else "fp32"
+        k2 = min(args.steps, 100)
+        g2, _, r2 = measure_instance(p, soa, other, k2, args.warmup, local, pg, profile=True, clocks=False)
+        g2.close()
+        ms2 = max_over_ranks(pg, r2["ms"], local)
+        out[other] = {"value": n * k2 * world / (ms2 / 1e3), "unit": METRIC, "ms_per_step": ms2 / k2,
+                      "kernels": {k: v[0] / max(v[1], 1) for k, v in r2["prof"].items()}}
 
     if rank == 0 and world == 1:
-        # ---- reference kernels built for sm_100a on the same GPU (a few steps) -----------
-        if not args.no_ref_gpu:
-            try:
-                from oracle.oracle import RefCuda
-                work = soa.clone(pinned=False)
-                k = min(args.steps, 50)
-                err, _, _, rms = RefCuda().run(p, work, 0, k, 0.0)
-                out["reference_sm100a"] = {"value": n * k / (rms / 1e3), "unit": METRIC, "steps": k,
-                                           "error_code": err, "precision": "fp64",
-                                           "what": "reference kernels.cuh built for sm_100a, one partition"}
-            except Exception as e:  # informational only
-                out["reference_sm100a"] = {"unavailable": str(e)[:200]}
         if not args.no_extra:
             try:
                 out["batched"] = measure_batch()

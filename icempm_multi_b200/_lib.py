@@ -85,7 +85,7 @@ EXPORTED = [
     "icy_mpm_profile", "icy_mpm_profile_read", "icy_mpm_set_option", "icy_step_noalloc",
     "icy_batch_create", "icy_batch_destroy", "icy_batch_add", "icy_batch_remove", "icy_batch_step",
     "icy_batch_download", "icy_batch_synchronize", "icy_batch_set_option", "icy_batch_info",
-    "icy_batch_device_bytes", "icy_mpm_device_bytes",
+    "icy_batch_device_bytes", "icy_mpm_device_bytes", "icy_scene_place", "icy_host_alloc", "icy_host_free",
 ]
 
 _lib = None
@@ -110,6 +110,9 @@ def lib():
         "icy_params_parse_file": (C.c_int, [P, C.c_char_p, C.c_char_p, C.c_size_t]),
         "icy_scene_block": (C.c_int, [P, C.c_double, C.c_double, C.c_int, C.c_uint64, C.c_int, vp, C.c_uint, up]),
         "icy_scene_block_count": (C.c_uint, [P, C.c_double, C.c_double, C.c_int]),
+        "icy_scene_place": (C.c_int, [P, vp, C.c_uint, up, C.c_double]),
+        "icy_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(vp)]),
+        "icy_host_free": (C.c_int, [vp]),
         "icy_mpm_create": (C.c_int, [P, C.c_int, C.c_uint, C.c_int, C.POINTER(vp)]),
         "icy_mpm_destroy": (C.c_int, [vp]),
         "icy_mpm_set_stream": (C.c_int, [vp, vp]),

@@ -53,6 +53,27 @@ static int set_device(icy_mpm *h)
 extern "C" {
 
 const char *icy_version(void) { return "icempm_b200 sm_100a"; }
+
+int icy_host_alloc(size_t bytes, void **ptr)
+{
+    if (!ptr || bytes == 0) return ICY_ERR_INVALID_ARGUMENT;
+    *ptr = nullptr;
+    cudaError_t e = cudaMallocHost(ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        icy_set_error("cudaMallocHost", e);
+        *ptr = nullptr;
+        return ICY_ERR_OUT_OF_MEMORY;
+    }
+    std::memset(*ptr, 0, bytes);
+    return ICY_OK;
+}
+
+int icy_host_free(void *ptr)
+{
+    if (ptr) CK(cudaFreeHost(ptr));
+    return ICY_OK;
+}
 const char *icy_last_error(void) { return g_last_error.c_str(); }
 
 int icy_mpm_create(const icy_sim_params *p, int device, unsigned capacity, int precision, icy_mpm **out)

@@ -44,6 +44,78 @@ void block_cells(const icy_sim_params *p, double bw, double bh, long *ncx, long 
 
 extern "C" {
 
+/* LoadRawPoints' placement of a point cloud already in the HSSOA
+   (simulation/snapshotmanager.cpp:62-109); see include/icempm.h. */
+int icy_scene_place(icy_sim_params *p, double *hssoa, unsigned capacity, unsigned *n_points, double volume)
+{
+    if (!p || !hssoa || !n_points || *n_points == 0 || *n_points > capacity || !(volume > 0))
+        return ICY_ERR_INVALID_ARGUMENT;
+    icy_params_compute_helpers(p);
+    const double h = p->cellsize;
+    const size_t N0 = *n_points;
+    size_t N = N0;
+    p->nPtsTotal = (int)N;
+    p->Volume = volume;
+    double *X = hssoa + (size_t)ICY_POSX * capacity, *Y = hssoa + (size_t)(ICY_POSX + 1) * capacity;
+    double xmin = *std::min_element(X, X + N), xmax = *std::max_element(X, X + N);
+    double ymin = *std::min_element(Y, Y + N), ymax = *std::max_element(Y, Y + N);
+    p->xmin = xmin; p->xmax = xmax; p->ymin = ymin; p->ymax = ymax;
+    const double box_x = p->GridXTotal * h;
+    const double length = xmax - xmin;
+    const double x_offset = (box_x - length) / 2;
+    const double y_offset = 2 * h;
+    for (size_t i = 0; i < N; i++) { X[i] += x_offset; Y[i] += y_offset; }
+
+    // RemoveDisabledAndSort (host_side_soa.cpp:50-61): drop points with the disabled bit
+    // (keeping the order of the rest), then sort by the cell index of ProxyPoint::getCellIndex (proxypoint2d.cpp:114-119),
+    // stable so the order is the same on every platform
+    std::vector<uint32_t> perm;
+    perm.reserve(N);
+    for (size_t i = 0; i < N; i++) {
+        long long u;
+        std::memcpy(&u, hssoa + i, 8);
+        if (!(u & ICY_STATUS_DISABLED)) perm.push_back((uint32_t)i);
+    }
+    std::vector<long> key(N);
+    const double hinv = p->cellsize_inv;
+    for (size_t i = 0; i < N; i++)
+        key[i] = (long)(int)(X[i] * hinv + 0.5) * p->GridY + (int)(Y[i] * hinv + 0.5);
+    std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
+    std::vector<double> tmp(perm.size());
+    for (int l : {0, (int)ICY_POSX, (int)ICY_POSX + 1}) {
+        double *L = hssoa + (size_t)l * capacity;
+        for (size_t i = 0; i < perm.size(); i++) tmp[i] = L[perm[i]];
+        std::memcpy(L, tmp.data(), sizeof(double) * perm.size());
+    }
+    N = perm.size();
+    // the other lines start at zero (HostSideSOA::Allocate clears the buffer,
+    // host_side_soa.cpp:64-79), then InitializeBlock (host_side_soa.cpp:94-105)
+    for (int l = 1; l < ICY_N_PTS_ARRAYS; l++)
+        if (l != ICY_POSX && l != ICY_POSX + 1) std::memset(hssoa + (size_t)l * capacity, 0, sizeof(double) * N0);
+    for (size_t i = 0; i < N; i++) {
+        hssoa[(size_t)ICY_IDX_JP_INV * capacity + i] = 1.0;
+        hssoa[(size_t)ICY_FE00 * capacity + i] = 1.0;
+        hssoa[(size_t)(ICY_FE00 + 3) * capacity + i] = 1.0;
+    }
+    // indenter start (snapshotmanager.cpp:84-105)
+    const double block_left = x_offset;
+    const double block_top = p->ymax + y_offset;
+    const double r = p->IndDiameter / 2;
+    const double ht = r - p->IndDepth;
+    const double x_ind_offset = std::sqrt(r * r - ht * ht);
+    p->indenter_x = std::floor((block_left - x_ind_offset) / h) * h;
+    if (p->SetupType == 0) p->indenter_y = block_top + ht;
+    else if (p->SetupType == 1) p->indenter_y = std::ceil(block_top / h) * h;
+    else p->indenter_x = p->indenter_y = -1;
+    p->indenter_x_initial = p->indenter_x;
+    p->indenter_y_initial = p->indenter_y;
+    // particle volume and mass (snapshotmanager.cpp:108-109)
+    p->ParticleVolume = p->Volume / N0;
+    icy_params_compute_helpers(p);
+    *n_points = (unsigned)N;
+    return ICY_OK;
+}
+
 unsigned icy_scene_block_count(const icy_sim_params *p, double block_w, double block_h, int ppc)
 {
     long ncx, ncy;
@@ -107,55 +179,10 @@ int icy_scene_block(icy_sim_params *p, double block_w, double block_h, int ppc, 
             }
         }
 
-    // LoadRawPoints placement (simulation/snapshotmanager.cpp:62-109)
-    p->nPtsTotal = (int)N;
-    p->Volume = area;
-    double xmin = *std::min_element(X, X + N), xmax = *std::max_element(X, X + N);
-    double ymin = *std::min_element(Y, Y + N), ymax = *std::max_element(Y, Y + N);
-    p->xmin = xmin; p->xmax = xmax; p->ymin = ymin; p->ymax = ymax;
-    const double box_x = p->GridXTotal * h;
-    const double length = xmax - xmin;
-    const double x_offset = (box_x - length) / 2;
-    const double y_offset = 2 * h;
-    for (size_t i = 0; i < N; i++) { X[i] += x_offset; Y[i] += y_offset; }
-
-    // sort by the cell index of ProxyPoint::getCellIndex (proxypoint2d.cpp:114-119),
-    // stable so the order is the same on every platform
-    std::vector<uint32_t> perm(N);
-    std::iota(perm.begin(), perm.end(), 0u);
-    std::vector<long> key(N);
-    const double hinv = p->cellsize_inv;
-    for (size_t i = 0; i < N; i++)
-        key[i] = (long)(int)(X[i] * hinv + 0.5) * p->GridY + (int)(Y[i] * hinv + 0.5);
-    std::stable_sort(perm.begin(), perm.end(), [&](uint32_t a, uint32_t b) { return key[a] < key[b]; });
-    std::vector<double> tmp(N);
-    for (int l : {0, (int)ICY_POSX, (int)ICY_POSX + 1}) {
-        double *L = hssoa + (size_t)l * capacity;
-        for (size_t i = 0; i < N; i++) tmp[i] = L[perm[i]];
-        std::memcpy(L, tmp.data(), sizeof(double) * N);
-    }
-    // InitializeBlock (host_side_soa.cpp:94-105)
-    for (size_t i = 0; i < N; i++) {
-        hssoa[(size_t)ICY_IDX_JP_INV * capacity + i] = 1.0;
-        hssoa[(size_t)ICY_FE00 * capacity + i] = 1.0;
-        hssoa[(size_t)(ICY_FE00 + 3) * capacity + i] = 1.0;
-    }
-    // indenter start (snapshotmanager.cpp:84-105)
-    const double block_left = x_offset;
-    const double block_top = p->ymax + y_offset;
-    const double r = p->IndDiameter / 2;
-    const double ht = r - p->IndDepth;
-    const double x_ind_offset = std::sqrt(r * r - ht * ht);
-    p->indenter_x = std::floor((block_left - x_ind_offset) / h) * h;
-    if (p->SetupType == 0) p->indenter_y = block_top + ht;
-    else if (p->SetupType == 1) p->indenter_y = std::ceil(block_top / h) * h;
-    else p->indenter_x = p->indenter_y = -1;
-    p->indenter_x_initial = p->indenter_x;
-    p->indenter_y_initial = p->indenter_y;
-    // particle volume and mass (snapshotmanager.cpp:108-109)
-    p->ParticleVolume = p->Volume / N;
-    icy_params_compute_helpers(p);
-    if (n_points) *n_points = (unsigned)N;
+    unsigned n = (unsigned)N;
+    int rc = icy_scene_place(p, hssoa, capacity, &n, area);
+    if (rc != ICY_OK) return rc;
+    if (n_points) *n_points = n;
     return ICY_OK;
 }
 

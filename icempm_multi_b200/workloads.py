@@ -16,6 +16,10 @@ LARGE = dict(grid_x=4096, grid_y=2048, h=0.05, block_w=150.0, block_h=40.0, ppc=
              E=1e9, nu=0.3, rho=980.0, phi=62.0, cohesion=0.0, ind_radius=1.0, ind_velocity=1.0,
              ind_depth=0.5, seed=1, n_grains=64)
 
+# a profiling-size instance on the same grid: 100 m x 30 m block (4.8 M points); its
+# FP32 state (173 MB) is still larger than L2
+MEDIUM = dict(LARGE, block_w=100.0, block_h=30.0)
+
 # the CPU-runnable small instance: grid 512 x 256 at h = 0.25 m, 64 m x 16 m block
 # (65,536 points), dt = 1e-4 s, 1000 steps
 SMALL = dict(grid_x=512, grid_y=256, h=0.25, block_w=64.0, block_h=16.0, ppc=4, dt=1e-4,

@@ -151,6 +151,28 @@ int icy_scene_block(icy_sim_params *p, double block_w, double block_h, int ppc,
                     unsigned *n_points);
 /* Number of points icy_scene_block would create (for sizing the HSSOA). */
 unsigned icy_scene_block_count(const icy_sim_params *p, double block_w, double block_h, int ppc);
+/*
+ * The placement half of SnapshotManager::LoadRawPoints
+ * (simulation/snapshotmanager.cpp:62-109) for a point cloud whose x, y and
+ * utility lines are already in the HSSOA (*n_points points, e.g. read from
+ * the reference's HDF5 files): block extent into xmin..ymax, block centred
+ * in x and lifted by 2h, RemoveDisabledAndSort (points with the disabled bit
+ * dropped, the rest stable-sorted by ProxyPoint::getCellIndex), the other
+ * lines cleared and InitializeBlock (Fe = I, Jp_inv = 1), indenter start,
+ * nPtsTotal, Volume = volume, ParticleVolume = volume / (points loaded) and
+ * ComputeHelperVariables.  On return *n_points holds the points kept.
+ */
+int icy_scene_place(icy_sim_params *p, double *hssoa, unsigned capacity, unsigned *n_points,
+                    double volume);
+
+/*
+ * Page-locked host memory for an HSSOA buffer, as HostSideSOA::Allocate
+ * takes it with cudaMallocHost (simulation/hssoa/host_side_soa.cpp:64-79);
+ * the memory is cleared.  Lets a host that links only this library keep its
+ * transfers asynchronous.  icy_host_free(NULL) is a no-op.
+ */
+int icy_host_alloc(size_t bytes, void **ptr);
+int icy_host_free(void *ptr);
 
 /* ------------------------------------------------------------------ */
 /* one simulation instance on one device                                */
