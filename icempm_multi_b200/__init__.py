@@ -5,7 +5,8 @@ C-ABI of ``include/icempm.h``; this package is the Python mirror of the
 reference's host interface (SimParams, HostSideSOA, GPU_Implementation5,
 Model) over that C-ABI.
 """
-from ._lib import (PRECISION_FP32_SPLIT, PRECISION_FP64, IcyError, SimParams, lib)  # noqa: F401
-from .hssoa import HostSideSOA, make_block  # noqa: F401
+from ._lib import (PRECISION_FP32_SPLIT, PRECISION_FP64, IcyError, SimParams, format_double, host_lib,  # noqa: F401
+                   lib)
+from .hssoa import HostSideSOA, load_h5, make_block  # noqa: F401
 from .model import GPUImplementation, Model  # noqa: F401
 from .params import block_params, default_params, parse_file, parse_json  # noqa: F401

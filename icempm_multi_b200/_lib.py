@@ -11,6 +11,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libicempm_b200.so")
+HOST_LIB_PATH = os.path.join(HERE, "libicempm_host.so")
+CLI_PATH = os.path.join(HERE, "icy_cli")
 
 # --- status codes (include/icempm.h) ---
 ICY_OK = 0
@@ -157,6 +159,43 @@ def lib():
         f.argtypes = args
     _lib = L
     return L
+
+
+# the symbols include/icempm_host.h declares
+HOST_EXPORTED = ["icy_h5_count", "icy_h5_load", "icy_format_double", "icy_host_last_error"]
+
+_host = None
+
+
+def host_lib():
+    """Load libicempm_host.so, the C++ host layer (raises if it was not built)."""
+    global _host
+    if _host is not None:
+        return _host
+    lib()
+    if not os.path.exists(HOST_LIB_PATH):
+        raise RuntimeError(f"{HOST_LIB_PATH} is missing: build it with `python -m icempm_multi_b200.build`")
+    L = C.CDLL(HOST_LIB_PATH)
+    P = C.POINTER(SimParams)
+    sig = {
+        "icy_h5_count": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint)]),
+        "icy_h5_load": (C.c_int, [P, C.c_char_p, C.c_void_p, C.c_uint, C.POINTER(C.c_uint)]),
+        "icy_format_double": (C.c_int, [C.c_double, C.c_char_p, C.c_size_t]),
+        "icy_host_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _host = L
+    return L
+
+
+def format_double(v):
+    """The indenter_force.csv number format (fmt's "{}" for a double)."""
+    buf = C.create_string_buffer(64)
+    check(host_lib().icy_format_double(float(v), buf, 64), "icy_format_double")
+    return buf.value.decode()
 
 
 class IcyError(RuntimeError):

@@ -104,3 +104,25 @@ def make_block(params, block_w, block_h, ppc=4, seed=1, n_grains=0, extra_space=
     check(rc, "icy_scene_block")
     soa.size = out_n.value
     return soa
+
+
+def load_h5(params, path, extra_space=None, pinned=False):
+    """A point cloud of the reference's HDF5 format ("x", "y", "llGrainIDs" with
+    its "volume" attribute), read and placed as SnapshotManager::LoadRawPoints
+    does (simulation/snapshotmanager.cpp:29-109).  Capacity = points x (1 +
+    ExtraSpaceForIncomingPoints) unless extra_space is given.  Updates
+    ``params`` in place."""
+    from ._lib import host_lib
+    H = host_lib()
+    n = C.c_uint(0)
+    rc = H.icy_h5_count(str(path).encode(), C.byref(n))
+    if rc != 0:
+        raise RuntimeError(f"icy_h5_count({path}) failed with status {rc}: {H.icy_host_last_error().decode()}")
+    es = params.ExtraSpaceForIncomingPoints if extra_space is None else extra_space
+    soa = HostSideSOA(max(int(n.value * (1 + es)), 1), pinned=pinned)
+    got = C.c_uint(0)
+    rc = H.icy_h5_load(C.byref(params), str(path).encode(), soa.ptr, soa.capacity, C.byref(got))
+    if rc != 0:
+        raise RuntimeError(f"icy_h5_load({path}) failed with status {rc}: {H.icy_host_last_error().decode()}")
+    soa.size = got.value
+    return soa
