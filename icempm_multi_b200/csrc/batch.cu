@@ -33,7 +33,8 @@ struct icy_batch {
     SplitArgs *d_args = nullptr;
     BatchClock *d_clk = nullptr;
     int *d_rec = nullptr;
-    long *d_node_off = nullptr, *d_tile_off = nullptr;
+    int2 *d_tlist = nullptr;         // node tiles written since the last update, all members
+    unsigned *d_tlist_n = nullptr;   // [0] entries, [1] CTAs of the update done
     BatchItem *d_work = nullptr;
     long work_cap = 0;
     int *d_woff = nullptr, *d_nwork = nullptr;
@@ -45,7 +46,7 @@ struct icy_batch {
     int64_t launches = 0;
 };
 
-static SplitArgs member_args(icy_mpm *h)
+static SplitArgs member_args(icy_batch *b, icy_mpm *h, int slot)
 {
     SplitArgs A{};
     A.P = icy_step_params(h->prm);
@@ -66,6 +67,9 @@ static SplitArgs member_args(icy_mpm *h)
     A.active = h->d_active;
     A.n_active = h->d_nactive;
     A.flags = h->d_flags;
+    A.tlist = b->d_tlist;
+    A.tlist_n = b->d_tlist_n;
+    A.inst = slot;
     A.status = h->d_status;
     A.moved = h->d_moved;
     A.grain_tab = static_cast<const GrainConstF *>(h->d_grainf);
@@ -82,33 +86,29 @@ static void drop_graphs(icy_batch *b)
     b->graph_launches.clear();
 }
 
-// Upload the members' kernel arguments, node / tile offsets and work list.
+// Upload the members' kernel arguments and work list (and grow the work and
+// node-tile lists to the members' total tile count).
 static int rebuild(icy_batch *b)
 {
     std::vector<SplitArgs> args(b->nslots);
-    std::vector<long> node_off(b->nslots + 1, 0), tile_off(b->nslots + 1, 0);
     long tiles = 0;
-    for (int s = 0; s < b->nslots; s++) {
-        icy_mpm *h = b->members[s];
-        if (h) args[s] = member_args(h);
-        node_off[s + 1] = node_off[s] + (h ? h->n_nodes : 0);
-        tile_off[s + 1] = tile_off[s] + (h ? h->ntiles : 0);
-        tiles += h ? h->ntiles : 0;
-    }
+    for (int s = 0; s < b->nslots; s++)
+        tiles += b->members[s] ? b->members[s]->ntiles : 0;
     if (tiles > b->work_cap) {
         cudaFree(b->d_work);
         b->d_work = nullptr;
         drop_graphs(b);   // the graphs hold the old work-list address
+        cudaFree(b->d_tlist);
+        b->d_tlist = nullptr;
         const long cap = std::max(tiles, 2 * b->work_cap);
         cudaError_t e = cudaMalloc(&b->d_work, sizeof(BatchItem) * std::max(cap, 1L));
+        if (e == cudaSuccess) e = cudaMalloc(&b->d_tlist, sizeof(int2) * std::max(cap, 1L));
         if (e != cudaSuccess) { icy_set_error("cudaMalloc(batch work list)", e); return ICY_ERR_OUT_OF_MEMORY; }
         b->work_cap = cap;
     }
+    for (int s = 0; s < b->nslots; s++)
+        if (b->members[s]) args[s] = member_args(b, b->members[s], s);
     CKB(cudaMemcpyAsync(b->d_args, args.data(), sizeof(SplitArgs) * b->nslots, cudaMemcpyHostToDevice, b->stream));
-    CKB(cudaMemcpyAsync(b->d_node_off, node_off.data(), sizeof(long) * (b->nslots + 1), cudaMemcpyHostToDevice,
-                        b->stream));
-    CKB(cudaMemcpyAsync(b->d_tile_off, tile_off.data(), sizeof(long) * (b->nslots + 1), cudaMemcpyHostToDevice,
-                        b->stream));
     k_batch_work_offsets<<<1, 1024, 0, b->stream>>>(b->d_args, b->d_clk, b->nslots, b->d_woff, b->d_nwork);
     k_batch_work_fill<<<dim3(8, b->nslots), 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_woff, b->d_work);
     CKB(cudaGetLastError());
@@ -131,7 +131,7 @@ static int rebin_members(icy_batch *b)
     return ICY_OK;
 }
 
-// Capture [P2G] + nsteps x [advance, update, clear marks, G2P(+P2G)] as a graph.
+// Capture [P2G] + nsteps x [advance, update, G2P(+P2G)] as a graph.
 static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
 {
     SplitArgs none{};
@@ -143,16 +143,15 @@ static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
     n++;
     for (int k = 0; k < nsteps; k++) {
         k_batch_advance<<<(b->nslots + 127) / 128, 128, 0, b->stream>>>(b->d_clk, b->d_rec, b->nslots);
-        k_update_batch_f32<<<b->update_grid, 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_node_off, b->nslots);
-        k_clear_flags_batch<<<b->update_grid / 4 + 1, 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_tile_off,
-                                                                         b->nslots);
+        k_update_list_f32<true><<<b->update_grid, 256, 0, b->stream>>>(SplitArgs{}, b->d_args, b->d_clk, b->d_tlist,
+                                                                          b->d_tlist_n, 0.0, 0.0);
         if (k + 1 < nsteps)
             k_tile_f32<true, true, false, true><<<b->tile_grid, TILE_THREADS, MOMF_BYTES, b->stream>>>(
                 none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
         else
             k_tile_f32<true, false, true, true><<<b->tile_grid, TILE_THREADS, 0, b->stream>>>(
                 none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
-        n += 4;
+        n += 3;
     }
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (e != cudaSuccess) { icy_set_error("cudaStreamEndCapture", e); return ICY_ERR_CUDA; }
@@ -210,20 +209,20 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
     if ((e = cudaMalloc(&b->d_args, sizeof(SplitArgs) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_clk, sizeof(BatchClock) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_rec, sizeof(int) * max_instances)) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_node_off, sizeof(long) * (max_instances + 1))) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_tile_off, sizeof(long) * (max_instances + 1))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_tlist_n, sizeof(unsigned) * 2)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_woff, sizeof(int) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_nwork, sizeof(int))) != cudaSuccess)
         return fail(e, "cudaMalloc(batch)");
     cudaMemsetAsync(b->d_clk, 0, sizeof(BatchClock) * max_instances, b->stream);
     cudaMemsetAsync(b->d_rec, 0, sizeof(int) * max_instances, b->stream);
     cudaMemsetAsync(b->d_nwork, 0, sizeof(int), b->stream);
+    cudaMemsetAsync(b->d_tlist_n, 0, sizeof(unsigned) * 2, b->stream);
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false, true>, TILE_THREADS,
                                                   MOMF_BYTES);
     b->tile_grid = std::max(1, sms * std::max(per_sm, 1));
-    b->update_grid = std::max(1, sms * 16);
+    b->update_grid = std::max(1, sms * 8);
     if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return fail(e, "batch init");
     *out = b;
     return ICY_OK;
@@ -240,8 +239,8 @@ int icy_batch_destroy(icy_batch *b)
     cudaFree(b->d_args);
     cudaFree(b->d_clk);
     cudaFree(b->d_rec);
-    cudaFree(b->d_node_off);
-    cudaFree(b->d_tile_off);
+    cudaFree(b->d_tlist);
+    cudaFree(b->d_tlist_n);
     cudaFree(b->d_work);
     cudaFree(b->d_woff);
     cudaFree(b->d_nwork);

@@ -99,12 +99,15 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(dalloc(&h->d_active, h->ntiles));
     CK(dalloc(&h->d_nactive, 1));
     CK(dalloc(&h->d_flags, h->ntiles));
+    CK(cudaMalloc(&h->d_tlist, sizeof(int2) * h->ntiles));
+    CK(dalloc(&h->d_tlist_n, 2));
     CK(dalloc(&h->d_moved, 1));
     CK(dalloc(&h->d_acc, 2 * h->prm.n_indenter_subdivisions));
     CK(dalloc(&h->d_status, 1));
     CK(dalloc(&h->d_grain, GRAIN_TAB));
     CK(cudaMallocHost(&h->h_status, sizeof(int)));
     CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
+    CK(cudaMemsetAsync(h->d_tlist_n, 0, sizeof(unsigned) * 2, h->stream));
     CK(cudaMemsetAsync(h->d_nactive, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_moved, 0, sizeof(unsigned long long), h->stream));
     CK(cudaMemsetAsync(h->d_acc, 0, sizeof(double) * 2 * h->prm.n_indenter_subdivisions, h->stream));
@@ -122,7 +125,7 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false>, TILE_THREADS,
                                                      MOMF_BYTES));
     h->tile_grid_f32 = std::max(1, sms * std::max(per_sm, 1));
-    h->update_grid = (int)std::max(1L, std::min((h->n_nodes + 255) / 256, (long)sms * 16));
+    h->update_grid = (int)std::max(1L, std::min((long)(h->ntiles + 1) / 2, (long)sms * 8));
     if (int rc = icy_instance_constants(h)) return rc;
     CK(cudaStreamSynchronize(h->stream));
     return ICY_OK;
@@ -136,7 +139,7 @@ void icy_instance_free(icy_mpm *h)
     void *ptrs[] = {h->d_pts, h->d_pts_alt, h->d_grid, h->d_oidx, h->d_oidx_alt, h->d_keys, h->d_ranks,
                     h->d_counts, h->d_start, h->d_active, h->d_nactive, h->d_flags, h->d_moved, h->d_acc,
                     h->d_status, h->d_block_sums, h->d_grain, h->d_st, h->d_st_alt, h->d_stage, h->d_gridf,
-                    h->d_grainf};
+                    h->d_grainf, h->d_tlist, h->d_tlist_n};
     for (void *p : ptrs) cudaFree(p);
     h->d_st = h->d_st_alt = nullptr;
     h->d_stage = nullptr;
@@ -148,6 +151,8 @@ void icy_instance_free(icy_mpm *h)
     h->d_oidx = h->d_oidx_alt = h->d_keys = h->d_ranks = h->d_counts = h->d_start = nullptr;
     h->d_active = h->d_nactive = h->d_status = h->h_status = h->d_block_sums = nullptr;
     h->d_flags = nullptr;
+    h->d_tlist = nullptr;
+    h->d_tlist_n = nullptr;
     h->d_moved = nullptr;
     h->d_grain = nullptr;
     h->own_stream = h->stream = nullptr;
@@ -273,6 +278,8 @@ static TileArgs tile_args(icy_mpm *h, bool record)
     A.active = h->d_active;
     A.n_active = h->d_nactive;
     A.flags = h->d_flags;
+    A.tlist = h->d_tlist;
+    A.tlist_n = h->d_tlist_n;
     A.status = h->d_status;
     A.moved = h->d_moved;
     A.grain_tab = h->d_grain;
@@ -306,10 +313,15 @@ static SplitArgs split_args(icy_mpm *h, bool record)
     A.active = h->d_active;
     A.n_active = h->d_nactive;
     A.flags = h->d_flags;
+    A.tlist = h->d_tlist;
+    A.tlist_n = h->d_tlist_n;
+    A.inst = 0;
     A.status = h->d_status;
     A.moved = h->d_moved;
     A.grain_tab = static_cast<const GrainConstF *>(h->d_grainf);
     A.record_pq = record ? 1 : 0;
+    A.acc = h->d_acc;
+    A.n_nodes = h->n_nodes;
     return A;
 }
 
@@ -370,14 +382,13 @@ static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y)
     StepParams P = icy_step_params(h->prm);
     icy_prof_begin(h, K_UPDATE_TILES);
     if (is_split(h))
-        k_update_nodes_f32<<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
-            P, split_consts(P), tile_geom(h), grid_view_f32(h), h->d_flags, h->n_nodes, ind_x, ind_y, h->d_acc);
+        k_update_list_f32<false><<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
+            split_args(h, false), nullptr, nullptr, h->d_tlist, h->d_tlist_n, ind_x, ind_y);
     else
-        k_update_nodes<<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
-            P, tile_geom(h), grid_view(h), h->d_flags, h->n_nodes, ind_x, ind_y, h->d_acc);
+        k_update_list<<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
+            P, tile_geom(h), grid_view(h), h->d_flags, h->d_tlist, h->d_tlist_n, ind_x, ind_y, h->d_acc);
     icy_prof_end(h);
     CK_LAUNCH("k_update_nodes");
-    CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
     return ICY_OK;
 }
 
@@ -400,7 +411,10 @@ int icy_phase_reset_grid(icy_mpm *h)
     if (is_split(h)) CK(cudaMemsetAsync(h->d_gridf, 0, sizeof(float) * 3 * h->n_nodes, h->stream));
     else CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 3 * h->n_nodes, h->stream));
     icy_prof_end(h);
-    if (h->tiled || is_split(h)) CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
+    if (h->tiled || is_split(h)) {
+        CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
+        CK(cudaMemsetAsync(h->d_tlist_n, 0, sizeof(unsigned) * 2, h->stream));
+    }
     h->primed = false;
     return ICY_OK;
 }

@@ -44,6 +44,8 @@ struct icy_mpm {
     icy_dev::GrainConst *d_grain = nullptr;   // failure-surface constants per grain slot
     int scan_blocks = 0;
     unsigned *d_flags = nullptr;
+    int2 *d_tlist = nullptr;        // node tiles written since the last grid update (once each)
+    unsigned *d_tlist_n = nullptr;  // [0] entries, [1] CTAs of the update done
     unsigned long long *d_moved = nullptr;
     int ntx = 0, nty = 0, ntiles = 0;
     int tile_grid = 0, update_grid = 0, pipe_grid = 0;

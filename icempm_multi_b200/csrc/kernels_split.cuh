@@ -254,12 +254,15 @@ struct SplitArgs {
     long pitch;
     const int *cell_start, *active, *n_active;
     unsigned *flags;
+    int2 *tlist;        // node tiles written since the last update, each once: (inst, tile)
+    unsigned *tlist_n;  // [0] entries, [1] CTAs of the update done
+    int inst;           // this instance's slot in a batch (0 alone)
     int *status;
     unsigned long long *moved;
     const GrainConstF *grain_tab;
     int record_pq;
-    double *acc;        // indenter force bins (batched update)
-    long n_nodes;       // nodes of the grid (batched update)
+    double *acc;        // indenter force bins
+    long n_nodes;       // nodes of the grid
 };
 
 template <typename Sink>
@@ -282,9 +285,10 @@ __device__ __forceinline__ void point_contributions_f32(float h, float fx, float
     }
 }
 
-static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags, int ntx, int halo, float h, int bx, int by,
-                                            float fx, float fy, float mass, float mvx, float mvy, float s00,
-                                            float s01, float s10, float s11)
+static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags, int2 *tlist, unsigned *tlist_n,
+                                                   int inst, int ntx, int halo, float h, int bx, int by, float fx,
+                                                   float fy, float mass, float mvx, float mvy, float s00, float s01,
+                                                   float s10, float s11)
 {
     point_contributions_f32(h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
                             [&](int a, int b, float dm, float dpx, float dpy) {
@@ -295,10 +299,12 @@ static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags,
                             });
     const int t0x = (bx + halo) / TX, t1x = (bx + 2 + halo) / TX;
     const int t0y = by / TY, t1y = (by + 2) / TY;
-    flags[t0y * ntx + t0x] = 1u;
-    flags[t0y * ntx + t1x] = 1u;
-    flags[t1y * ntx + t0x] = 1u;
-    flags[t1y * ntx + t1x] = 1u;
+    mark_tile(flags, tlist, tlist_n, inst, t0y * ntx + t0x);
+    if (t1x != t0x) mark_tile(flags, tlist, tlist_n, inst, t0y * ntx + t1x);
+    if (t1y != t0y) {
+        mark_tile(flags, tlist, tlist_n, inst, t1y * ntx + t0x);
+        if (t1x != t0x) mark_tile(flags, tlist, tlist_n, inst, t1y * ntx + t1x);
+    }
 }
 
 // phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32
@@ -345,7 +351,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                                                 atomicAdd(&s_odd[2][k], dpy);
                                             });
                 } else {
-                    p2g_global_f32(A.g, A.flags, A.G.ntx, P.halo, A.Q.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01,
+                    p2g_global_f32(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01,
                                    s10, s11);
                 }
             }
@@ -486,7 +492,7 @@ static __global__ void __launch_bounds__(TILE_THREADS, 3)
             __syncthreads();
             if (tid < 9 && ((s_touch >> tid) & 1u)) {
                 const int ntx = tx + tid % 3 - 1, nty = ty + tid / 3 - 1;
-                A.flags[nty * A.G.ntx + ntx] = 1u;
+                mark_tile(A.flags, A.tlist, A.tlist_n, A.inst, nty * A.G.ntx + ntx);
             }
             moved = __reduce_add_sync(0xffffffffu, moved);
             if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
@@ -495,70 +501,67 @@ static __global__ void __launch_bounds__(TILE_THREADS, 3)
     }
 }
 
-// Grid update in FP32 (simulation/kernels.cuh:175-300); the indenter geometry
-// and the force bins in FP64.
-static __global__ void __launch_bounds__(256) k_update_nodes_f32(StepParams P, SplitConsts Q, TileGeom G, GridViewF g,
-                                                          const unsigned *__restrict__ flags, long n_nodes,
-                                                          double ind_x, double ind_y, double *acc)
+// Grid update of one node in FP32 (simulation/kernels.cuh:175-300), the
+// indenter geometry and the force in FP64: writes the velocity, zeroes the
+// accumulators and returns the force bin of a contact node (-1 if none).
+__device__ __forceinline__ int update_node_f32(const StepParams &P, const SplitConsts &Q, const GridViewF &g, int gx,
+                                               int gy, long q, double ind_x, double ind_y, double &fxd, double &fyd)
 {
-    extern __shared__ double s_acc[];
-    for (int k = threadIdx.x; k < 2 * P.nsub; k += blockDim.x) s_acc[k] = 0;
-    __syncthreads();
-    bool any = false;
-    const int nn = (int)n_nodes;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nn; q += gridDim.x * blockDim.x) {
-        const int col = q / g.ny;
-        const int gx = col - g.halo, gy = q - col * g.ny;
-        if (!flags[(gy / TY) * G.ntx + (gx + g.halo) / TX]) continue;
-        const float mass = g.m[q];
-        float vx = 0.f, vy = 0.f;
-        if (mass != 0.f) {
-            vx = g.px[q] / mass;
-            vy = g.py[q] / mass;
-            vy -= Q.dtg;
-            const float v2 = vx * vx + vy * vy;
-            if (v2 > Q.vmax_sq) {
-                const float r = sqrtf(v2);
-                vx = vx / r * Q.vmax;
-                vy = vy / r * Q.vmax;
-            }
-            double nx = (double)gx * P.h - ind_x, ny = (double)gy * P.h - ind_y;
-            if (nx * nx + ny * ny < P.ind_rsq) {
-                const double r = sqrt(nx * nx + ny * ny);
-                if (r > 0) { nx /= r; ny /= r; }
-                const float fnx = (float)nx, fny = (float)ny;
-                const float vrx = vx - (float)P.ind_v, vry = vy;
-                const float vn = vrx * fnx + vry * fny;
-                if (vn < 0.f) {
-                    const float vtx = vrx - fnx * vn, vty = vry - fny * vn;
-                    const float pvx = vx, pvy = vy;
-                    vx = (float)P.ind_v + vtx;
-                    vy = vty;
-                    const double fxd = (double)(pvx - vx) * mass / P.dt, fyd = (double)(pvy - vy) * mass / P.dt;
-                    float angle = atan2f(fnx, fny);
-                    angle = (float)((double)angle + kPi);
-                    angle = (float)((double)angle * (P.nsub / (2 * kPi)));
-                    const int bin = min(max((int)angle, 0), P.nsub - 1);
-                    atomicAdd(&s_acc[2 * bin], fxd);
-                    atomicAdd(&s_acc[2 * bin + 1], fyd);
-                    any = true;
-                }
-            }
-            if (gy <= 2) { vx = 0.f; vy = 0.f; }
-            if (gy >= P.gridy - 3 && vy > 0.f) vy = 0.f;
-            if (gx <= 2 && vx < 0.f) vx = 0.f;
-            else if (gx >= P.gridx - 3 && vx > 0.f) vx = 0.f;
+    const float mass = g.m[q];
+    float vx = 0.f, vy = 0.f;
+    int bin = -1;
+    if (mass != 0.f) {
+        vx = g.px[q] / mass;
+        vy = g.py[q] / mass;
+        vy -= Q.dtg;
+        const float v2 = vx * vx + vy * vy;
+        if (v2 > Q.vmax_sq) {
+            const float r = sqrtf(v2);
+            vx = vx / r * Q.vmax;
+            vy = vy / r * Q.vmax;
         }
-        g.vx[q] = vx;
-        g.vy[q] = vy;
-        g.m[q] = 0.f;
-        g.px[q] = 0.f;
-        g.py[q] = 0.f;
+        double nx = (double)gx * P.h - ind_x, ny = (double)gy * P.h - ind_y;
+        if (nx * nx + ny * ny < P.ind_rsq) {
+            const double r = sqrt(nx * nx + ny * ny);
+            if (r > 0) { nx /= r; ny /= r; }
+            const float fnx = (float)nx, fny = (float)ny;
+            const float vrx = vx - (float)P.ind_v, vry = vy;
+            const float vn = vrx * fnx + vry * fny;
+            if (vn < 0.f) {
+                const float vtx = vrx - fnx * vn, vty = vry - fny * vn;
+                const float pvx = vx, pvy = vy;
+                vx = (float)P.ind_v + vtx;
+                vy = vty;
+                fxd = (double)(pvx - vx) * mass / P.dt;
+                fyd = (double)(pvy - vy) * mass / P.dt;
+                float angle = atan2f(fnx, fny);
+                angle = (float)((double)angle + kPi);
+                angle = (float)((double)angle * (P.nsub / (2 * kPi)));
+                bin = min(max((int)angle, 0), P.nsub - 1);
+            }
+        }
+        if (gy <= 2) { vx = 0.f; vy = 0.f; }
+        if (gy >= P.gridy - 3 && vy > 0.f) vy = 0.f;
+        if (gx <= 2 && vx < 0.f) vx = 0.f;
+        else if (gx >= P.gridx - 3 && vx > 0.f) vx = 0.f;
     }
-    if (!__syncthreads_or(any)) return;
-    for (int k = threadIdx.x; k < 2 * P.nsub; k += blockDim.x)
-        if (s_acc[k] != 0.0) atomicAdd(acc + k, s_acc[k]);
+    g.vx[q] = vx;
+    g.vy[q] = vy;
+    g.m[q] = 0.f;
+    g.px[q] = 0.f;
+    g.py[q] = 0.f;
+    return bin;
 }
+
+struct BatchClock;
+
+// Grid update of the listed node tiles (see k_update_list in kernels_tiled.cuh),
+// defined after BatchClock below.
+template <bool BATCH>
+static __global__ void __launch_bounds__(256) k_update_list_f32(SplitArgs A1, const SplitArgs *__restrict__ Aarr,
+                                                                const BatchClock *__restrict__ clk,
+                                                                const int2 *__restrict__ tlist, unsigned *tlist_n,
+                                                                double ind_x, double ind_y);
 
 // ---------------------------------------------------------------- binning / conversion
 static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__restrict__ st, long pitch, int n,
@@ -701,87 +704,53 @@ static __global__ void k_batch_advance(BatchClock *clk, int *rec, int nslots)
     clk[i] = c;
 }
 
-__device__ __forceinline__ int find_slot(const long *off, int nslots, long q)
+// Grid update of the listed node tiles: each half-CTA takes one 16 x 8 node
+// tile (one thread per node), clears the tile's mark, and the last CTA empties
+// the list.  Alone (BATCH = false) the forces are summed per CTA in shared
+// memory; in a batch every entry names its member, whose indenter position
+// comes from the member's clock and whose force bins take the force directly.
+template <bool BATCH>
+static __global__ void __launch_bounds__(256) k_update_list_f32(SplitArgs A1, const SplitArgs *__restrict__ Aarr,
+                                                                const BatchClock *__restrict__ clk,
+                                                                const int2 *__restrict__ tlist, unsigned *tlist_n,
+                                                                double ind_x, double ind_y)
 {
-    int lo = 0, hi = nslots;   // off[lo] <= q < off[hi]
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (off[mid] <= q) lo = mid;
-        else hi = mid;
+    extern __shared__ double s_acc[];   // 2*nsub (alone only)
+    if (!BATCH) {
+        for (int k = threadIdx.x; k < 2 * A1.P.nsub; k += blockDim.x) s_acc[k] = 0;
+        __syncthreads();
     }
-    return lo;
-}
-
-// Grid update of all members' marked nodes (see k_update_nodes_f32); the force
-// of a contact node goes straight to its member's bins.
-static __global__ void __launch_bounds__(256) k_update_batch_f32(const SplitArgs *__restrict__ Aarr,
-                                                                 const BatchClock *__restrict__ clk,
-                                                                 const long *__restrict__ node_off, int nslots)
-{
-    const long total = node_off[nslots];
-    for (long gq = (long)blockIdx.x * blockDim.x + threadIdx.x; gq < total; gq += (long)gridDim.x * blockDim.x) {
-        const int s = find_slot(node_off, nslots, gq);
-        if (!clk[s].live) continue;
-        const SplitArgs &A = Aarr[s];
-        const StepParams &P = A.P;
-        const GridViewF &g = A.g;
-        const int q = (int)(gq - node_off[s]);
-        const int col = q / g.ny;
-        const int gx = col - g.halo, gy = q - col * g.ny;
-        if (!A.flags[(gy / TY) * A.G.ntx + (gx + g.halo) / TX]) continue;
-        const float mass = g.m[q];
-        float vx = 0.f, vy = 0.f;
-        if (mass != 0.f) {
-            vx = g.px[q] / mass;
-            vy = g.py[q] / mass;
-            vy -= A.Q.dtg;
-            const float v2 = vx * vx + vy * vy;
-            if (v2 > A.Q.vmax_sq) {
-                const float r = sqrtf(v2);
-                vx = vx / r * A.Q.vmax;
-                vy = vy / r * A.Q.vmax;
+    bool any = false;
+    const unsigned n = *(volatile unsigned *)tlist_n;
+    static_assert(TT == 128, "two node tiles per 256-thread CTA");
+    const int l = threadIdx.x & (TT - 1);
+    for (unsigned e = blockIdx.x * 2 + (threadIdx.x >> 7); e < n; e += gridDim.x * 2) {
+        const int2 it = tlist[e];
+        const SplitArgs &A = BATCH ? Aarr[it.x] : A1;
+        const int t = it.y;
+        const int ty = t / A.G.ntx, tx = t - ty * A.G.ntx;
+        if (l == 0) A.flags[t] = 0u;
+        const int gx = tx * TX + l / TY - A.P.halo, gy = ty * TY + (l & (TY - 1));
+        if (gx >= A.P.gridx + A.P.halo || gy >= A.P.gridy) continue;   // past the grid edge
+        double fx = 0, fy = 0;
+        const int bin = update_node_f32(A.P, A.Q, A.g, gx, gy, A.g.idx(gx, gy), BATCH ? clk[it.x].ind_x : ind_x,
+                                        BATCH ? clk[it.x].y0 : ind_y, fx, fy);
+        if (bin >= 0) {
+            if (BATCH) {
+                atomicAdd(A.acc + 2 * bin, fx);
+                atomicAdd(A.acc + 2 * bin + 1, fy);
+            } else {
+                atomicAdd(&s_acc[2 * bin], fx);
+                atomicAdd(&s_acc[2 * bin + 1], fy);
+                any = true;
             }
-            double nx = (double)gx * P.h - clk[s].ind_x, ny = (double)gy * P.h - clk[s].y0;
-            if (nx * nx + ny * ny < P.ind_rsq) {
-                const double r = sqrt(nx * nx + ny * ny);
-                if (r > 0) { nx /= r; ny /= r; }
-                const float fnx = (float)nx, fny = (float)ny;
-                const float vrx = vx - (float)P.ind_v, vry = vy;
-                const float vn = vrx * fnx + vry * fny;
-                if (vn < 0.f) {
-                    const float vtx = vrx - fnx * vn, vty = vry - fny * vn;
-                    const float pvx = vx, pvy = vy;
-                    vx = (float)P.ind_v + vtx;
-                    vy = vty;
-                    float angle = atan2f(fnx, fny);
-                    angle = (float)((double)angle + kPi);
-                    angle = (float)((double)angle * (P.nsub / (2 * kPi)));
-                    const int bin = min(max((int)angle, 0), P.nsub - 1);
-                    atomicAdd(A.acc + 2 * bin, (double)(pvx - vx) * mass / P.dt);
-                    atomicAdd(A.acc + 2 * bin + 1, (double)(pvy - vy) * mass / P.dt);
-                }
-            }
-            if (gy <= 2) { vx = 0.f; vy = 0.f; }
-            if (gy >= P.gridy - 3 && vy > 0.f) vy = 0.f;
-            if (gx <= 2 && vx < 0.f) vx = 0.f;
-            else if (gx >= P.gridx - 3 && vx > 0.f) vx = 0.f;
         }
-        g.vx[q] = vx;
-        g.vy[q] = vy;
-        g.m[q] = 0.f;
-        g.px[q] = 0.f;
-        g.py[q] = 0.f;
     }
-}
-
-static __global__ void k_clear_flags_batch(const SplitArgs *__restrict__ Aarr, const BatchClock *__restrict__ clk,
-                                           const long *__restrict__ tile_off, int nslots)
-{
-    const long total = tile_off[nslots];
-    for (long gt = (long)blockIdx.x * blockDim.x + threadIdx.x; gt < total; gt += (long)gridDim.x * blockDim.x) {
-        const int s = find_slot(tile_off, nslots, gt);
-        if (clk[s].live) Aarr[s].flags[gt - tile_off[s]] = 0u;
-    }
+    if (!BATCH && __syncthreads_or(any))
+        for (int k = threadIdx.x; k < 2 * A1.P.nsub; k += blockDim.x)
+            if (s_acc[k] != 0.0) atomicAdd(A1.acc + k, s_acc[k]);
+    if (BATCH) __syncthreads();
+    if (threadIdx.x == 0) tile_list_done(tlist_n);
 }
 
 // (instance, tile) work list: offsets by an exclusive scan over the members'

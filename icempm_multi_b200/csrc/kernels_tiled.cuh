@@ -55,11 +55,33 @@ struct TileArgs {
     const int *active;       // tiles with points, ascending
     const int *n_active;
     unsigned *flags;         // node tiles written by P2G since the last update
+    int2 *tlist;             // those tiles, each once: (instance, tile)
+    unsigned *tlist_n;       // [0] entries in tlist, [1] CTAs done (reset by the update)
     int *status;
     unsigned long long *moved;  // points whose base is not their sorted cell (re-binning hint)
     const GrainConst *grain_tab;  // failure-surface constants per grain slot
     int record_pq;
 };
+
+// Marks node tile t as written by P2G since the last grid update and appends
+// (inst, t) to the list the update visits, once per tile.
+__device__ __forceinline__ void mark_tile(unsigned *flags, int2 *tlist, unsigned *tlist_n, int inst, int t)
+{
+    if (*(volatile unsigned *)(flags + t) == 0u && atomicExch(flags + t, 1u) == 0u)
+        tlist[atomicAdd(tlist_n, 1u)] = make_int2(inst, t);
+}
+
+// Called by thread 0 of every CTA of a list-driven grid update after its last
+// read of the list: the last CTA to finish empties the list for the next step.
+__device__ __forceinline__ void tile_list_done(unsigned *tlist_n)
+{
+    __threadfence();
+    if (atomicAdd(tlist_n + 1, 1u) == gridDim.x - 1) {
+        tlist_n[0] = 0u;
+        tlist_n[1] = 0u;
+        __threadfence();
+    }
+}
 
 static __global__ void k_grain_table(StepParams P, GrainConst *tab)
 {
@@ -261,9 +283,9 @@ __device__ __forceinline__ void point_contributions(double h, double fx, double 
 }
 
 // P2G of one point straight into the global grid (its base left the staged region).
-static __device__ __noinline__ void p2g_global(GridView g, unsigned *flags, int ntx, int halo, double h, int bx, int by,
-                                        double fx, double fy, double mass, double mvx, double mvy, double s00,
-                                        double s01, double s10, double s11)
+static __device__ __noinline__ void p2g_global(GridView g, unsigned *flags, int2 *tlist, unsigned *tlist_n, int ntx,
+                                               int halo, double h, int bx, int by, double fx, double fy, double mass,
+                                               double mvx, double mvy, double s00, double s01, double s10, double s11)
 {
     point_contributions(h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
                         [&](int a, int b, double dm, double dpx, double dpy) {
@@ -274,10 +296,12 @@ static __device__ __noinline__ void p2g_global(GridView g, unsigned *flags, int 
                         });
     const int t0x = (bx + halo) / TX, t1x = (bx + 2 + halo) / TX;
     const int t0y = by / TY, t1y = (by + 2) / TY;
-    flags[t0y * ntx + t0x] = 1u;
-    flags[t0y * ntx + t1x] = 1u;
-    flags[t1y * ntx + t0x] = 1u;
-    flags[t1y * ntx + t1x] = 1u;
+    mark_tile(flags, tlist, tlist_n, 0, t0y * ntx + t0x);
+    if (t1x != t0x) mark_tile(flags, tlist, tlist_n, 0, t0y * ntx + t1x);
+    if (t1y != t0y) {
+        mark_tile(flags, tlist, tlist_n, 0, t1y * ntx + t0x);
+        if (t1x != t0x) mark_tile(flags, tlist, tlist_n, 0, t1y * ntx + t1x);
+    }
 }
 
 // ---------------------------------------------------------------- per point
@@ -455,7 +479,7 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
                                             atomicAdd(&s_odd[2][k], dpy);
                                         });
                 } else {
-                    p2g_global(A.g, A.flags, A.G.ntx, P.halo, P.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01, s10,
+                    p2g_global(A.g, A.flags, A.tlist, A.tlist_n, A.G.ntx, P.halo, P.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01, s10,
                                s11);
                 }
             }
@@ -504,7 +528,7 @@ __device__ __forceinline__ void mark_node_tiles(const TileArgs &A, int tx, int t
 {
     if (lane9 < 9 && ((touch >> lane9) & 1u)) {
         const int ntx = tx + lane9 % 3 - 1, nty = ty + lane9 / 3 - 1;
-        A.flags[nty * A.G.ntx + ntx] = 1u;
+        mark_tile(A.flags, A.tlist, A.tlist_n, 0, nty * A.G.ntx + ntx);
     }
 }
 
@@ -778,22 +802,29 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(TileArgs A
     if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
 }
 
-// Grid update of the nodes of marked tiles (simulation/kernels.cuh:164-301),
-// one thread per node; zeroes the accumulators for the next step.  The marks
-// are cleared by the caller afterwards.
-static __global__ void __launch_bounds__(256) k_update_nodes(StepParams P, TileGeom G, GridView g,
-                                                      const unsigned *__restrict__ flags, long n_nodes,
-                                                      double ind_x, double ind_y, double *acc)
+// Grid update of the nodes of the listed tiles (simulation/kernels.cuh:164-301):
+// each half-CTA takes one 16 x 8 node tile (one thread per node, the 8 nodes of
+// a tile column contiguous in memory), computes the velocities, zeroes the
+// accumulators for the next step and clears the tile's mark; the last CTA
+// empties the list.
+static __global__ void __launch_bounds__(256) k_update_list(StepParams P, TileGeom G, GridView g, unsigned *flags,
+                                                            const int2 *__restrict__ tlist, unsigned *tlist_n,
+                                                            double ind_x, double ind_y, double *acc)
 {
     extern __shared__ double s_acc[];   // 2*nsub
     for (int k = threadIdx.x; k < 2 * P.nsub; k += blockDim.x) s_acc[k] = 0;
     __syncthreads();
     bool any = false;
-    const int nn = (int)n_nodes;   // < 2^31 nodes per instance
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nn; q += gridDim.x * blockDim.x) {
-        const int col = q / g.ny;
-        const int gx = col - g.halo, gy = q - col * g.ny;
-        if (!flags[(gy / TY) * G.ntx + (gx + g.halo) / TX]) continue;
+    const unsigned n = *(volatile unsigned *)tlist_n;
+    static_assert(TT == 128, "two node tiles per 256-thread CTA");
+    const int l = threadIdx.x & (TT - 1);
+    for (unsigned e = blockIdx.x * 2 + (threadIdx.x >> 7); e < n; e += gridDim.x * 2) {
+        const int t = tlist[e].y;
+        const int ty = t / G.ntx, tx = t - ty * G.ntx;
+        if (l == 0) flags[t] = 0u;
+        const int gx = tx * TX + l / TY - P.halo, gy = ty * TY + (l & (TY - 1));
+        if (gx >= P.gridx + P.halo || gy >= P.gridy) continue;   // past the grid edge
+        const long q = g.idx(gx, gy);
         double vx = 0, vy = 0, fx, fy;
         int bin;
         if (node_update(P, gx, gy, g.m[q], g.px[q], g.py[q], ind_x, ind_y, vx, vy, bin, fx, fy) && bin >= 0) {
@@ -807,9 +838,10 @@ static __global__ void __launch_bounds__(256) k_update_nodes(StepParams P, TileG
         g.px[q] = 0.0;
         g.py[q] = 0.0;
     }
-    if (!__syncthreads_or(any)) return;
-    for (int k = threadIdx.x; k < 2 * P.nsub; k += blockDim.x)
-        if (s_acc[k] != 0.0) atomicAdd(acc + k, s_acc[k]);
+    if (__syncthreads_or(any))
+        for (int k = threadIdx.x; k < 2 * P.nsub; k += blockDim.x)
+            if (s_acc[k] != 0.0) atomicAdd(acc + k, s_acc[k]);
+    if (threadIdx.x == 0) tile_list_done(tlist_n);
 }
 
 }  // namespace icy_dev
