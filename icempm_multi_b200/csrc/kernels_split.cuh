@@ -87,6 +87,23 @@ struct PointF {
     M2<float> D, B;
 };
 
+// The return mapping of a crushed point in FP64 (kernels.cuh:540-545, 623-674)
+// from its FP32 state, out of line: few points take it, and keeping its FP64
+// registers out of the tile kernel's main path leaves room for more warps.
+struct SplitRm { float d00, d01, d10, d11, jp; };
+static __device__ __noinline__ SplitRm return_map_split(const StepParams &P, float d00, float d01, float d10,
+                                                        float d11, float jp)
+{
+    M2<double> F{1.0 + (double)d00, (double)d01, (double)d10, 1.0 + (double)d11};
+    double Jp = jp;
+    double Je64 = det2(F), p64 = (-(P.kappa / 2.)) * (Je64 * Je64 - 1.);
+    M2<double> dv = dev_ffT(F);
+    double q64 = ((kCoeff1 * P.mu) * (1. / Je64)) *
+                 sqrt(((dv.a00 * dv.a00 + dv.a10 * dv.a10) + dv.a01 * dv.a01) + dv.a11 * dv.a11);
+    return_map(P, F, Jp, p64, q64, Je64);
+    return SplitRm{(float)(F.a00 - 1.0), (float)F.a01, (float)F.a10, (float)(F.a11 - 1.0), (float)Jp};
+}
+
 template <typename VSrc>
 __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitConsts &Q, const GrainConstF *tab,
                                                PointF &s, int *status, VSrc &&vsrc)
@@ -102,6 +119,8 @@ __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitC
     bspline_weights(fy, wy);
     float vx = 0.f, vy = 0.f;
     M2<float> B{0.f, 0.f, 0.f, 0.f};
+    float2 nv[9];
+    vsrc(bx, by, nv);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         const float d0 = (float)a - fx;
@@ -109,8 +128,7 @@ __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitC
         for (int b = 0; b < 3; b++) {
             const float d1 = (float)b - fy;
             const float w = wx[a] * wy[b];
-            float nvx, nvy;
-            vsrc(bx, by, a, b, nvx, nvy);
+            const float nvx = nv[a * 3 + b].x, nvy = nv[a * 3 + b].y;
             vx += w * nvx;
             vy += w * nvy;
             const float sw = Q.s4 * w;
@@ -149,16 +167,9 @@ __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitC
             if (crushed) s.util |= (unsigned)kCrushed;
         }
         if (s.util & (unsigned)kCrushed) {
-            // return mapping in FP64 (kernels.cuh:540-545, 623-674)
-            M2<double> F{1.0 + (double)s.D.a00, (double)s.D.a01, (double)s.D.a10, 1.0 + (double)s.D.a11};
-            double Jp = s.Jp;
-            double Je64 = det2(F), p64 = (-(P.kappa / 2.)) * (Je64 * Je64 - 1.);
-            M2<double> dv = dev_ffT(F);
-            double q64 = ((kCoeff1 * P.mu) * (1. / Je64)) *
-                         sqrt(((dv.a00 * dv.a00 + dv.a10 * dv.a10) + dv.a01 * dv.a01) + dv.a11 * dv.a11);
-            return_map(P, F, Jp, p64, q64, Je64);
-            s.D = {(float)(F.a00 - 1.0), (float)F.a01, (float)F.a10, (float)(F.a11 - 1.0)};
-            s.Jp = (float)Jp;
+            const SplitRm r = return_map_split(P, s.D.a00, s.D.a01, s.D.a10, s.D.a11, s.Jp);
+            s.D = {r.d00, r.d01, r.d10, r.d11};
+            s.Jp = r.jp;
         }
     }
     s.vx = vx;
@@ -399,16 +410,42 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
 // Work items of a batch: (instance, tile) pairs over all instances.
 struct BatchItem { int inst, tile; };
 
+// L2 prefetch of [p, p + bytes) rounded inward to 16-byte boundaries (never
+// past either end): cp.async.bulk.prefetch.L2 from this GPU's global memory.
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes)
+{
+    const uintptr_t a = ((uintptr_t)p + 15) & ~uintptr_t(15), e = ((uintptr_t)p + bytes) & ~uintptr_t(15);
+    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
+// Starts moving the next work item's point lines (line `which` < S_JP + 1) or
+// cell ranges (which == S_JP + 1) into L2 while this CTA is in its cell phase.
+template <bool BATCH>
+__device__ __forceinline__ void prefetch_next_item(const SplitArgs &A1, const SplitArgs *Aarr, const BatchItem *work,
+                                                   int next, int na, int which)
+{
+    if (next >= na) return;
+    const BatchItem w = BATCH ? work[next] : BatchItem{0, A1.active[next]};
+    const SplitArgs &A = BATCH ? Aarr[w.inst] : A1;
+    const int *cs = A.cell_start + (long)w.tile * TT;
+    if (which == S_JP + 1) {
+        prefetch_l2(cs, (TT + 1) * sizeof(int));
+        return;
+    }
+    const int ps = cs[0], pe = cs[TT];
+    if (pe > ps) prefetch_l2(A.st + A.pitch * which + ps, (size_t)(pe - ps) * sizeof(unsigned));
+}
+
 // Tile kernel over the FP32 state: <G2P, P2G, write vel/Bp> as k_tile.
 // With BATCH, the CTAs walk the (instance, tile) list of many independent
 // instances, each with its own parameters, grid and points (Aarr[inst]), and
 // the record-PQ flag of each instance comes from rec[inst].
 template <bool DO_G2P, bool DO_P2G, bool WRITE_VB, bool BATCH = false>
-static __global__ void __launch_bounds__(TILE_THREADS, 3)
-    k_tile_f32(SplitArgs A1, const SplitArgs *__restrict__ Aarr = nullptr, const BatchItem *__restrict__ work = nullptr,
+static __global__ void __launch_bounds__(TILE_THREADS, 4)
+    k_tile_f32(const __grid_constant__ SplitArgs A1, const SplitArgs *__restrict__ Aarr = nullptr, const BatchItem *__restrict__ work = nullptr,
                const int *__restrict__ nwork = nullptr, const int *__restrict__ rec = nullptr)
 {
-    __shared__ float s_v[2][RN];
+    __shared__ float2 s_v[RN];
     __shared__ float s_odd[3][RN];
     __shared__ int s_cs[TT + 1];
     __shared__ unsigned s_touch;
@@ -437,22 +474,29 @@ static __global__ void __launch_bounds__(TILE_THREADS, 3)
                     vx = A.g.vx[q];
                     vy = A.g.vy[q];
                 }
-                s_v[0][k] = vx;
-                s_v[1][k] = vy;
+                s_v[k] = make_float2(vx, vy);
             }
         }
         __syncthreads();
         const int ps = s_cs[0], pe = s_cs[TT];
-        auto vsrc = [&](int bx, int by, int a, int b, float &nvx, float &nvy) {
+        // the 3 x 3 node velocities of a stencil: from the staged region (one check
+        // per point), else from the grid
+        auto vsrc = [&](int bx, int by, float2 *nv) {
             const int lx = bx - RX0, ly = by - RY0;
             if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
-                const int k = (lx + a) * RY + (ly + b);
-                nvx = s_v[0][k];
-                nvy = s_v[1][k];
+                const float2 *r = s_v + lx * RY + ly;
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++) nv[a * 3 + b] = r[a * RY + b];
             } else {
-                const long k = A.g.idx(bx + a, by + b);
-                nvx = A.g.vx[k];
-                nvy = A.g.vy[k];
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++) {
+                        const long k = A.g.idx(bx + a, by + b);
+                        nv[a * 3 + b] = make_float2(A.g.vx[k], A.g.vy[k]);
+                    }
             }
         };
         unsigned touch = 0;
@@ -482,6 +526,9 @@ static __global__ void __launch_bounds__(TILE_THREADS, 3)
                 if (DO_P2G) p2g_moments_f32(P, A.Q, s, s_momf, j, A.status);
             }
             __syncthreads();
+            // threads without a cell in the cell phase start the next item's loads
+            if (DO_P2G && cs == ps && tid >= TT && tid < TT + S_JP + 2)
+                prefetch_next_item<BATCH>(A1, Aarr, work, ti + gridDim.x, na, tid - TT);
             if (DO_P2G)
                 p2g_cells_and_flush_f32<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
                                                       [] { __syncthreads(); });
@@ -501,18 +548,19 @@ static __global__ void __launch_bounds__(TILE_THREADS, 3)
     }
 }
 
-// Grid update of one node in FP32 (simulation/kernels.cuh:175-300), the
-// indenter geometry and the force in FP64: writes the velocity, zeroes the
-// accumulators and returns the force bin of a contact node (-1 if none).
-__device__ __forceinline__ int update_node_f32(const StepParams &P, const SplitConsts &Q, const GridViewF &g, int gx,
-                                               int gy, long q, double ind_x, double ind_y, double &fxd, double &fyd)
+// Grid update of one node in FP32 (simulation/kernels.cuh:175-300) from its
+// mass and momentum, the indenter geometry and the force in FP64: the new
+// velocity, and the force bin of a contact node (-1 if none).
+__device__ __forceinline__ int node_velocity_f32(const StepParams &P, const SplitConsts &Q, int gx, int gy, float mass,
+                                                 float px, float py, double ind_x, double ind_y, float &vx, float &vy,
+                                                 double &fxd, double &fyd)
 {
-    const float mass = g.m[q];
-    float vx = 0.f, vy = 0.f;
+    vx = 0.f;
+    vy = 0.f;
     int bin = -1;
     if (mass != 0.f) {
-        vx = g.px[q] / mass;
-        vy = g.py[q] / mass;
+        vx = px / mass;
+        vy = py / mass;
         vy -= Q.dtg;
         const float v2 = vx * vx + vy * vy;
         if (v2 > Q.vmax_sq) {
@@ -545,20 +593,17 @@ __device__ __forceinline__ int update_node_f32(const StepParams &P, const SplitC
         if (gx <= 2 && vx < 0.f) vx = 0.f;
         else if (gx >= P.gridx - 3 && vx > 0.f) vx = 0.f;
     }
-    g.vx[q] = vx;
-    g.vy[q] = vy;
-    g.m[q] = 0.f;
-    g.px[q] = 0.f;
-    g.py[q] = 0.f;
     return bin;
 }
 
 struct BatchClock;
+constexpr int UPD_TILES = 4;
 
 // Grid update of the listed node tiles (see k_update_list in kernels_tiled.cuh),
 // defined after BatchClock below.
 template <bool BATCH>
-static __global__ void __launch_bounds__(256) k_update_list_f32(SplitArgs A1, const SplitArgs *__restrict__ Aarr,
+static __global__ void __launch_bounds__(256) k_update_list_f32(const __grid_constant__ SplitArgs A1,
+                                                                const SplitArgs *__restrict__ Aarr,
                                                                 const BatchClock *__restrict__ clk,
                                                                 const int2 *__restrict__ tlist, unsigned *tlist_n,
                                                                 double ind_x, double ind_y);
@@ -710,7 +755,8 @@ static __global__ void k_batch_advance(BatchClock *clk, int *rec, int nslots)
 // memory; in a batch every entry names its member, whose indenter position
 // comes from the member's clock and whose force bins take the force directly.
 template <bool BATCH>
-static __global__ void __launch_bounds__(256) k_update_list_f32(SplitArgs A1, const SplitArgs *__restrict__ Aarr,
+static __global__ void __launch_bounds__(256) k_update_list_f32(const __grid_constant__ SplitArgs A1,
+                                                                const SplitArgs *__restrict__ Aarr,
                                                                 const BatchClock *__restrict__ clk,
                                                                 const int2 *__restrict__ tlist, unsigned *tlist_n,
                                                                 double ind_x, double ind_y)
@@ -724,25 +770,54 @@ static __global__ void __launch_bounds__(256) k_update_list_f32(SplitArgs A1, co
     const unsigned n = *(volatile unsigned *)tlist_n;
     static_assert(TT == 128, "two node tiles per 256-thread CTA");
     const int l = threadIdx.x & (TT - 1);
-    for (unsigned e = blockIdx.x * 2 + (threadIdx.x >> 7); e < n; e += gridDim.x * 2) {
-        const int2 it = tlist[e];
-        const SplitArgs &A = BATCH ? Aarr[it.x] : A1;
-        const int t = it.y;
-        const int ty = t / A.G.ntx, tx = t - ty * A.G.ntx;
-        if (l == 0) A.flags[t] = 0u;
-        const int gx = tx * TX + l / TY - A.P.halo, gy = ty * TY + (l & (TY - 1));
-        if (gx >= A.P.gridx + A.P.halo || gy >= A.P.gridy) continue;   // past the grid edge
-        double fx = 0, fy = 0;
-        const int bin = update_node_f32(A.P, A.Q, A.g, gx, gy, A.g.idx(gx, gy), BATCH ? clk[it.x].ind_x : ind_x,
-                                        BATCH ? clk[it.x].y0 : ind_y, fx, fy);
-        if (bin >= 0) {
-            if (BATCH) {
-                atomicAdd(A.acc + 2 * bin, fx);
-                atomicAdd(A.acc + 2 * bin + 1, fy);
-            } else {
-                atomicAdd(&s_acc[2 * bin], fx);
-                atomicAdd(&s_acc[2 * bin + 1], fy);
-                any = true;
+    const unsigned stride = gridDim.x * 2;
+    // UPD_TILES tiles per pass, their loads issued together
+    for (unsigned e0 = blockIdx.x * 2 + (threadIdx.x >> 7); e0 < n; e0 += stride * UPD_TILES) {
+        long q[UPD_TILES];
+        int inst[UPD_TILES], gx[UPD_TILES], gy[UPD_TILES];
+        float m[UPD_TILES], px[UPD_TILES], py[UPD_TILES];
+#pragma unroll
+        for (int u = 0; u < UPD_TILES; u++) {
+            const unsigned e = e0 + u * stride;
+            q[u] = -1;
+            if (e >= n) continue;
+            const int2 it = tlist[e];
+            inst[u] = it.x;
+            const SplitArgs &A = BATCH ? Aarr[it.x] : A1;
+            const int t = it.y;
+            const int ty = t / A.G.ntx, tx = t - ty * A.G.ntx;
+            if (l == 0) A.flags[t] = 0u;
+            gx[u] = tx * TX + l / TY - A.P.halo;
+            gy[u] = ty * TY + (l & (TY - 1));
+            if (gx[u] >= A.P.gridx + A.P.halo || gy[u] >= A.P.gridy) continue;   // past the grid edge
+            q[u] = A.g.idx(gx[u], gy[u]);
+            m[u] = A.g.m[q[u]];
+            px[u] = A.g.px[q[u]];
+            py[u] = A.g.py[q[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < UPD_TILES; u++) {
+            if (q[u] < 0) continue;
+            const SplitArgs &A = BATCH ? Aarr[inst[u]] : A1;
+            float vx, vy;
+            double fx = 0, fy = 0;
+            const int bin = node_velocity_f32(A.P, A.Q, gx[u], gy[u], m[u], px[u], py[u],
+                                              BATCH ? clk[inst[u]].ind_x : ind_x, BATCH ? clk[inst[u]].y0 : ind_y,
+                                              vx, vy, fx, fy);
+            A.g.vx[q[u]] = vx;
+            A.g.vy[q[u]] = vy;
+            A.g.m[q[u]] = 0.f;
+            A.g.px[q[u]] = 0.f;
+            A.g.py[q[u]] = 0.f;
+            if (bin >= 0) {
+                if (BATCH) {
+                    atomicAdd(A.acc + 2 * bin, fx);
+                    atomicAdd(A.acc + 2 * bin + 1, fy);
+                } else {
+                    atomicAdd(&s_acc[2 * bin], fx);
+                    atomicAdd(&s_acc[2 * bin + 1], fy);
+                    any = true;
+                }
             }
         }
     }
