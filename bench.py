@@ -77,7 +77,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -121,7 +121,11 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend=None):
+    """One process per GPU under torchrun (RANK / WORLD_SIZE / LOCAL_RANK from
+    the environment, rendezvous at MASTER_ADDR): NCCL on GPUs, gloo on a host
+    without CUDA (the CPU tests of this logic).  Each rank runs an independent
+    replica; the only collectives are the barrier and the max of the timings."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -130,26 +134,42 @@ def dist_setup(n_gpus):
         import datetime
         import torch.distributed as dist
         import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
         pg = dist
     return rank, world, local, pg
+
+
+def _on_gpu(pg):
+    return pg is not None and pg.get_backend() == "nccl"
 
 
 def max_over_ranks(pg, value, local):
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}" if _on_gpu(pg) else "cpu")
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
 
 def barrier(pg, local):
     if pg is not None:
-        import torch
-        pg.barrier(device_ids=[local])
+        if _on_gpu(pg):
+            pg.barrier(device_ids=[local])
+        else:
+            pg.barrier()
+
+
+def replica_rate(points_per_rank, steps, world, ms_max):
+    """Whole-job particle-steps/s of `world` independent replicas, timed by the
+    slowest rank."""
+    return points_per_rank * steps * world / (ms_max / 1e3)
 
 
 def cpu_reference_rate(p, soa, target_s=15.0, max_steps=50, min_steps=2):
@@ -234,6 +254,11 @@ def measure_instance(p, soa, precision, steps, warmup, local, pg, opts=(), profi
     g.update_constants()
     g.transfer_ponts_to_device()
     g.reset_indenter_force_accumulator()
+    # the clock sampler runs from before the warm-up to the end of the timed region
+    sampler = ClockSampler(local) if clocks else None
+    if sampler:
+        sampler.__enter__()
+        time.sleep(0.5)
     t_sim = g.run_steps(0, warmup, 0.0)
     torch.cuda.synchronize()
     barrier(pg, local)
@@ -242,9 +267,6 @@ def measure_instance(p, soa, precision, steps, warmup, local, pg, opts=(), profi
     if profile:
         g.profile(True)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    sampler = ClockSampler(local) if clocks else None
-    if sampler:
-        sampler.__enter__()
     ev0.record(stream)
     t_sim = g.run_steps(warmup, steps, t_sim)
     ev1.record(stream)
@@ -377,13 +399,13 @@ def main():
     # ---- headline path, device-resident timed region ----------------------------------
     g, stream, r = measure_instance(p, soa, args.precision, args.steps, args.warmup, local, pg, args.opt)
     ms = max_over_ranks(pg, r["ms"], local)
-    value = n * args.steps * world / (ms / 1e3)
+    value = replica_rate(n, args.steps, world, ms)
 
     # ---- end to end through the C-ABI with host buffers ----------------------------------
     frame = p.UpdateEveryNthStep
     ms_e2e, downloads = measure_e2e(g, stream, soa, args.steps, frame, local, pg)
     ms_e2e = max_over_ranks(pg, ms_e2e, local)
-    e2e_value = n * args.steps * world / (ms_e2e / 1e3)
+    e2e_value = replica_rate(n, args.steps, world, ms_e2e)
     g.close()
 
     # ---- roofline of the dominant kernel ------------------------------------------------
