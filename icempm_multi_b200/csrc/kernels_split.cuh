@@ -318,14 +318,11 @@ static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags,
     }
 }
 
-// phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32, with
-// the cell partials in a buffer of their own (part, 27 x TT), so that one
-// barrier separates the cell phase from the node phase; ends with a barrier.
+// phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32
 template <int NT, typename Sync>
 __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int tid, int tx, int ty, int cs, int ce,
-                                                        const int *s_cs, const float *mom, float *part,
-                                                        float (*s_odd)[RN], unsigned &touch, unsigned &moved,
-                                                        Sync &&sync)
+                                                        const int *s_cs, float *mom, float (*s_odd)[RN],
+                                                        unsigned &touch, unsigned &moved, Sync &&sync)
 {
     const StepParams &P = A.P;
     const int X0 = tx * TX - P.halo, Y0 = ty * TY;
@@ -371,9 +368,10 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
             }
         }
     }
+    sync();
     if (tid < TT) {
 #pragma unroll
-        for (int q = 0; q < 27; q++) part[q * TT + tid] = acc[q];
+        for (int q = 0; q < 27; q++) mom[q * TT + tid] = acc[q];
     }
     sync();
     for (int k = tid; k < RN; k += NT) {
@@ -389,9 +387,9 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                 const int cy = ny - b;
                 if (cy < 0 || cy >= TY) continue;
                 const int c = cx * TY + cy, q = (a * 3 + b) * 3;
-                m += part[q * TT + c];
-                px += part[(q + 1) * TT + c];
-                py += part[(q + 2) * TT + c];
+                m += mom[q * TT + c];
+                px += mom[(q + 1) * TT + c];
+                py += mom[(q + 2) * TT + c];
             }
         }
         m += s_odd[0][k]; px += s_odd[1][k]; py += s_odd[2][k];
@@ -449,8 +447,8 @@ static __global__ void __launch_bounds__(TILE_THREADS, 4)
 {
     __shared__ float2 s_v[RN];
     __shared__ float s_odd[3][RN];
-    __shared__ float s_part[27 * TT];
     __shared__ int s_cs[TT + 1];
+    __shared__ unsigned s_touch;
     extern __shared__ float s_momf[];
     const int na = BATCH ? *nwork : *A1.n_active;
     const int tid = threadIdx.x;
@@ -466,6 +464,7 @@ static __global__ void __launch_bounds__(TILE_THREADS, 4)
         const int tx = t % A.G.ntx, ty = t / A.G.ntx;
         const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
         for (int c = tid; c <= TT; c += blockDim.x) s_cs[c] = A.cell_start[(long)t * TT + c];
+        if (tid == 0) s_touch = 0;
         if (DO_G2P) {
             for (int k = tid; k < RN; k += blockDim.x) {
                 const int gx = RX0 + k / RY, gy = RY0 + k % RY;
@@ -531,23 +530,21 @@ static __global__ void __launch_bounds__(TILE_THREADS, 4)
             if (DO_P2G && cs == ps && tid >= TT && tid < TT + S_JP + 2)
                 prefetch_next_item<BATCH>(A1, Aarr, work, ti + gridDim.x, na, tid - TT);
             if (DO_P2G)
-                p2g_cells_and_flush_f32<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_part, s_odd, touch,
-                                                      moved, [] { __syncthreads(); });
+                p2g_cells_and_flush_f32<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
+                                                      [] { __syncthreads(); });
         }
         if (DO_P2G) {
-            // each warp marks the node tiles its nodes went to (mark_tile appends a tile once)
             touch = __reduce_or_sync(0xffffffffu, touch);
-            const int lane = tid & 31;
-            if (lane < 9 && ((touch >> lane) & 1u)) {
-                const int ntx = tx + lane % 3 - 1, nty = ty + lane / 3 - 1;
+            if ((tid & 31) == 0 && touch) atomicOr(&s_touch, touch);
+            __syncthreads();
+            if (tid < 9 && ((s_touch >> tid) & 1u)) {
+                const int ntx = tx + tid % 3 - 1, nty = ty + tid / 3 - 1;
                 mark_tile(A.flags, A.tlist, A.tlist_n, A.inst, nty * A.G.ntx + ntx);
             }
             moved = __reduce_add_sync(0xffffffffu, moved);
-            if (lane == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
+            if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
         }
-        // the cell phase ends with a barrier; without one, the staged data of this
-        // item must be released before the next item overwrites it
-        if (!DO_P2G || pe == ps) __syncthreads();
+        __syncthreads();
     }
 }
 
