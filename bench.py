@@ -321,6 +321,9 @@ def measure_batch(n_instances=256, steps=100, seed=7):
         p, soa = mk(w)
         b.add(p, soa)
         npts += soa.size
+    from icempm_multi_b200.autotune import tune_batch
+    # launch shape by timing this batch (120 steps; the re-binning interval stays 256)
+    tuned = tune_batch(b, steps=10, resort=False)
     b.step(steps)            # captures the graph for this step count, warms up
     b.synchronize()
     stream = torch.cuda.ExternalStream(b.info()["stream"])
@@ -335,14 +338,18 @@ def measure_batch(n_instances=256, steps=100, seed=7):
     b.close()
     return {"value": npts * steps / (ms / 1e3), "unit": METRIC, "instances": n_instances, "points": npts,
             "steps": steps, "ms_per_step": ms / steps, "gpu_launches": int(launches),
+            "autotuned": tuned["settings"],
             "workload": "floe scenarios: points log-uniform 10k-500k, grids 128x128..1024x512 (h=0.1 m), "
                         "E U(5e8,2e9), phi U(45,70), indenter U(0.5,3) m/s, CFL dt, FP32 split, CUDA graph"}
 
 
-def measure_serve(rate_load=0.7, duration=12.0, batch_rate=None, seed=11):
+def measure_serve(rate=10.0, duration=12.0, seed=11):
     """Served Poisson request stream: scenarios of 5k-2M points (log-uniform),
-    200-5000 steps, admitted by a 150 GB device-memory budget, continuous
-    batching in rounds of 50 steps; p50/p99 completion latency."""
+    200-5000 steps, `rate` arrivals per second for `duration` seconds (a fixed
+    trace: same requests and arrival times every run), admitted by a 150 GB
+    device-memory budget, continuous batching in rounds of 50 steps; p50/p99
+    completion latency; the offered load (requested particle-steps per second
+    of arrivals) is reported beside the served throughput."""
     import numpy as np
     from icempm_multi_b200.serve import Server, poisson_requests
     from icempm_multi_b200.workloads import floe_scenario, make_workload as mk
@@ -353,15 +360,13 @@ def measure_serve(rate_load=0.7, duration=12.0, batch_rate=None, seed=11):
         w = floe_scenario(n, E=float(rng.uniform(5e8, 2e9)), phi=float(rng.uniform(45, 70)),
                           v_ind=float(rng.uniform(0.5, 3.0)), seed=seed * 100 + k)
         scenes.append(mk(w))
-    mean_pts = float(np.mean([s.size for _, s in scenes]))
-    mean_steps = 2600.0
-    rate = rate_load * (batch_rate or 2e10) / (mean_pts * mean_steps)
     n_req = max(8, int(rate * duration))
     reqs = poisson_requests(scenes, rate, n_req, round_steps=50, seed=seed)
+    offered = sum(r.soa.size * r.steps for r in reqs) / max(reqs[-1].arrival, 1e-9)
     srv = Server(budget_bytes=150e9, round_steps=50, keep_results=False)
     st = srv.run(reqs)
     srv.close()
-    st.update({"arrival_rate_per_s": rate, "budget_bytes": 150e9, "round_steps": 50, "unit": METRIC,
+    st.update({"arrival_rate_per_s": rate, "offered_particle_steps_per_s": offered, "budget_bytes": 150e9, "round_steps": 50, "unit": METRIC,
                "workload": "Poisson arrivals, points log-uniform 5k-2M, steps U(200,5000), FP32 split, "
                            "150 GB budget, continuous batching"})
     return st
@@ -458,7 +463,7 @@ def main():
         if not args.no_extra:
             try:
                 out["batched"] = measure_batch()
-                out["served"] = measure_serve(batch_rate=out["batched"]["value"])
+                out["served"] = measure_serve()
             except Exception as e:
                 out["batched_or_served_error"] = str(e)[:300]
         # ---- CPU baseline ------------------------------------------------------------------

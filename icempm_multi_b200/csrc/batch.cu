@@ -351,8 +351,13 @@ int icy_batch_set_option(icy_batch *b, const char *name, double value)
         b->resort_every = (int)value;
         return ICY_OK;
     }
-    if (std::strcmp(name, "tile_ctas") == 0 && value >= 1) {   // persistent CTAs of the tile kernel
+    if (std::strcmp(name, "tile_ctas") == 0 && value >= 1 && value <= (1 << 20)) {   // persistent CTAs, tile kernel
         b->tile_grid = (int)value;
+        drop_graphs(b);
+        return ICY_OK;
+    }
+    if (std::strcmp(name, "update_ctas") == 0 && value >= 1 && value <= (1 << 20)) {   // CTAs of the grid update
+        b->update_grid = (int)value;
         drop_graphs(b);
         return ICY_OK;
     }

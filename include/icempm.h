@@ -299,7 +299,9 @@ int icy_batch_download(icy_batch *b, int slot, double *hssoa, unsigned capacity,
                        unsigned *size, double *bins, double *sim_time, int64_t *step);
 int icy_batch_synchronize(icy_batch *b);
 /* "resort_every" (steps between re-binning, 0 = never), "tile_ctas"
-   (persistent CTAs of the tile kernel). */
+   (persistent CTAs of the tile kernel), "update_ctas" (CTAs of the grid
+   update); the CTA counts take effect from the next step call (the captured
+   graphs are dropped).  icempm_multi_b200/autotune.py picks them by timing. */
 int icy_batch_set_option(icy_batch *b, const char *name, double value);
 /* Live members, their total points, kernels launched so far, the batch stream. */
 int icy_batch_info(icy_batch *b, int *live, int64_t *points, int64_t *kernel_launches,
