@@ -117,26 +117,26 @@ __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitC
     float wx[3], wy[3];
     bspline_weights(fx, wx);
     bspline_weights(fy, wy);
-    float vx = 0.f, vy = 0.f;
-    M2<float> B{0.f, 0.f, 0.f, 0.f};
+    // v = sum W v_i and Bp = 4/h sum W v_i (i - f)^T (kernels.cuh:357-372),
+    // separably: sums over b with wy per column a, then over a with wx;
+    // sum W v_i (i - f) = sum W v_i i - f v
     float2 nv[9];
     vsrc(bx, by, nv);
+    float cvx[3], cvy[3], cbx[3], cby[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const float d0 = (float)a - fx;
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-            const float d1 = (float)b - fy;
-            const float w = wx[a] * wy[b];
-            const float nvx = nv[a * 3 + b].x, nvy = nv[a * 3 + b].y;
-            vx += w * nvx;
-            vy += w * nvy;
-            const float sw = Q.s4 * w;
-            const float snx = sw * nvx, sny = sw * nvy;
-            B.a00 += snx * d0; B.a01 += snx * d1;
-            B.a10 += sny * d0; B.a11 += sny * d1;
-        }
+        const float2 n0 = nv[a * 3], n1 = nv[a * 3 + 1], n2 = nv[a * 3 + 2];
+        cvx[a] = wy[0] * n0.x + wy[1] * n1.x + wy[2] * n2.x;
+        cvy[a] = wy[0] * n0.y + wy[1] * n1.y + wy[2] * n2.y;
+        cbx[a] = wy[1] * n1.x + 2.f * (wy[2] * n2.x);
+        cby[a] = wy[1] * n1.y + 2.f * (wy[2] * n2.y);
     }
+    const float vx = wx[0] * cvx[0] + wx[1] * cvx[1] + wx[2] * cvx[2];
+    const float vy = wx[0] * cvy[0] + wx[1] * cvy[1] + wx[2] * cvy[2];
+    const float sax = wx[1] * cvx[1] + 2.f * (wx[2] * cvx[2]), say = wx[1] * cvy[1] + 2.f * (wx[2] * cvy[2]);
+    const float sbx = wx[0] * cbx[0] + wx[1] * cbx[1] + wx[2] * cbx[2];
+    const float sby = wx[0] * cby[0] + wx[1] * cby[1] + wx[2] * cby[2];
+    const M2<float> B{Q.s4 * (sax - fx * vx), Q.s4 * (sbx - fy * vx), Q.s4 * (say - fx * vy), Q.s4 * (sby - fy * vy)};
     // advection in cell units, x += v dt (kernels.cuh:375)
     s.ox += vx * Q.dt_hinv;
     s.oy += vy * Q.dt_hinv;
@@ -208,12 +208,27 @@ __device__ __forceinline__ void load_point_f32(const unsigned *__restrict__ st, 
 }
 
 // ---------------------------------------------------------------- P2G (FP32)
-constexpr int NMOMF = 10;   // fx, fy, m, m*vx, m*vy, S00, S01, S10, S11, base
-constexpr size_t MOMF_BYTES = sizeof(float) * NMOMF * CAP_P;
+// Moments of a point as three vectors in shared memory, one padding column
+// after every 4 points (the cell phase reads points about 4 apart per lane):
+//   m0 = (fx, fy, mass, m vx),  m1 = (m vy, S00, S01, S10),  m2 = (S11, base)
+// with S = m Bp - dt vol Dp_inv tau (simulation/kernels.cuh:57-92).
+constexpr int MOMF_N = CAP + CAP / 4;
+constexpr size_t MOMF_BYTES = (2 * sizeof(float4) + sizeof(float2)) * MOMF_N;
+static_assert(9 * TT * sizeof(float4) <= MOMF_BYTES, "cell partials alias the moment buffer");
+__device__ __forceinline__ int momf_col(int j) { return j + (j >> 2); }
+struct MomF {
+    float4 *m0, *m1;
+    float2 *m2;
+    __device__ __forceinline__ explicit MomF(float *base)
+        : m0(reinterpret_cast<float4 *>(base)), m1(reinterpret_cast<float4 *>(base) + MOMF_N),
+          m2(reinterpret_cast<float2 *>(reinterpret_cast<float4 *>(base) + 2 * MOMF_N)) {}
+    __device__ __forceinline__ void none(int j) const { m2[momf_col(j)] = make_float2(0.f, __int_as_float(BASE_NONE)); }
+};
 
 __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const SplitConsts &Q, const PointF &s,
                                                 float *mom, int j, int *status)
 {
+    const MomF M(mom);
     const bool liquid = (s.util & (unsigned)kLiquid) != 0;
     const float mass = liquid ? Q.mass_water : Q.mass_ice;
     int bx, by;
@@ -223,7 +238,7 @@ __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const Split
     const int e = base_error(P, bx, by);
     if (e) {
         *status = e;
-        mom[mom_idx(9, j)] = __int_as_float(BASE_NONE);
+        M.none(j);
         return;
     }
     M2<float> tau;
@@ -238,16 +253,11 @@ __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const Split
         const float s1 = Q.mu / Je, s2 = (Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
         tau = {s1 * d00 + s2, s1 * d01, s1 * d01, -s1 * d00 + s2};
     }
-    mom[mom_idx(0, j)] = fx;
-    mom[mom_idx(1, j)] = fy;
-    mom[mom_idx(2, j)] = mass;
-    mom[mom_idx(3, j)] = s.vx * mass;
-    mom[mom_idx(4, j)] = s.vy * mass;
-    mom[mom_idx(5, j)] = mass * s.B.a00 - Q.dtvd * tau.a00;
-    mom[mom_idx(6, j)] = mass * s.B.a01 - Q.dtvd * tau.a01;
-    mom[mom_idx(7, j)] = mass * s.B.a10 - Q.dtvd * tau.a10;
-    mom[mom_idx(8, j)] = mass * s.B.a11 - Q.dtvd * tau.a11;
-    mom[mom_idx(9, j)] = __int_as_float(pack_base(bx, by));
+    const int c = momf_col(j);
+    M.m0[c] = make_float4(fx, fy, mass, s.vx * mass);
+    M.m1[c] = make_float4(s.vy * mass, mass * s.B.a00 - Q.dtvd * tau.a00, mass * s.B.a01 - Q.dtvd * tau.a01,
+                          mass * s.B.a10 - Q.dtvd * tau.a10);
+    M.m2[c] = make_float2(mass * s.B.a11 - Q.dtvd * tau.a11, __int_as_float(pack_base(bx, by)));
 }
 
 struct GridViewF {
@@ -276,6 +286,11 @@ struct SplitArgs {
     long n_nodes;       // nodes of the grid
 };
 
+// P2G contributions of one point to its 3 x 3 nodes (simulation/kernels.cuh:
+// 100-120): node (a, b) gets W m and W (m v + S d) with W = wx[a] wy[b] and
+// d = ((a - fx) h, (b - fy) h).  S d is affine in (a, b), so it is evaluated
+// as c0 + a S(:,0) h + b S(:,1) h: per node one product for W and one
+// multiply-add per component.
 template <typename Sink>
 __device__ __forceinline__ void point_contributions_f32(float h, float fx, float fy, float mass, float mvx,
                                                         float mvy, float s00, float s01, float s10, float s11,
@@ -284,14 +299,15 @@ __device__ __forceinline__ void point_contributions_f32(float h, float fx, float
     float wx[3], wy[3];
     bspline_weights(fx, wx);
     bspline_weights(fy, wy);
+    const float s00h = s00 * h, s01h = s01 * h, s10h = s10 * h, s11h = s11 * h;
+    const float c0x = mvx - (s00h * fx + s01h * fy), c0y = mvy - (s10h * fx + s11h * fy);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const float d0 = ((float)a - fx) * h;
+        const float ax = c0x + (float)a * s00h, ay = c0y + (float)a * s10h;
 #pragma unroll
         for (int b = 0; b < 3; b++) {
             const float W = wx[a] * wy[b];
-            const float d1 = ((float)b - fy) * h;
-            sink(a, b, W * mass, W * (mvx + (s00 * d0 + s01 * d1)), W * (mvy + (s10 * d0 + s11 * d1)));
+            sink(a, b, W, W * mass, ax + (float)b * s01h, ay + (float)b * s11h);
         }
     }
 }
@@ -302,11 +318,11 @@ static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags,
                                                    float s10, float s11)
 {
     point_contributions_f32(h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
-                            [&](int a, int b, float dm, float dpx, float dpy) {
+                            [&](int a, int b, float W, float dm, float tx, float ty) {
                                 const long k = g.idx(bx + a, by + b);
                                 atomicAdd(g.m + k, dm);
-                                atomicAdd(g.px + k, dpx);
-                                atomicAdd(g.py + k, dpy);
+                                atomicAdd(g.px + k, W * tx);
+                                atomicAdd(g.py + k, W * ty);
                             });
     const int t0x = (bx + halo) / TX, t1x = (bx + 2 + halo) / TX;
     const int t0y = by / TY, t1y = (by + 2) / TY;
@@ -333,33 +349,35 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
     if (tid < TT) {
         const int bxc = X0 + tid / TY, byc = Y0 + tid % TY;
         const int r0 = max(s_cs[tid], cs) - cs, r1 = min(s_cs[tid + 1], ce) - cs;
+        const MomF M(mom);
         for (int j = r0; j < r1; j++) {
-            const int pb = __float_as_int(mom[mom_idx(9, j)]);
+            const int c = momf_col(j);
+            const float2 q2 = M.m2[c];
+            const int pb = __float_as_int(q2.y);
             if (pb == BASE_NONE) continue;
             int bx, by;
             unpack_base(pb, bx, by);
-            const float fx = mom[mom_idx(0, j)], fy = mom[mom_idx(1, j)], mass = mom[mom_idx(2, j)];
-            const float mvx = mom[mom_idx(3, j)], mvy = mom[mom_idx(4, j)];
-            const float s00 = mom[mom_idx(5, j)], s01 = mom[mom_idx(6, j)];
-            const float s10 = mom[mom_idx(7, j)], s11 = mom[mom_idx(8, j)];
+            const float4 q0 = M.m0[c], q1 = M.m1[c];
+            const float fx = q0.x, fy = q0.y, mass = q0.z, mvx = q0.w, mvy = q1.x;
+            const float s00 = q1.y, s01 = q1.z, s10 = q1.w, s11 = q2.x;
             if (bx == bxc && by == byc) {
                 point_contributions_f32(A.Q.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
-                                        [&](int a, int b, float dm, float dpx, float dpy) {
+                                        [&](int a, int b, float W, float dm, float tx, float ty) {
                                             const int q = (a * 3 + b) * 3;
                                             acc[q] += dm;
-                                            acc[q + 1] += dpx;
-                                            acc[q + 2] += dpy;
+                                            acc[q + 1] += W * tx;
+                                            acc[q + 2] += W * ty;
                                         });
             } else {
                 moved++;
                 const int lx = bx - RX0, ly = by - RY0;
                 if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
                     point_contributions_f32(A.Q.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
-                                            [&](int a, int b, float dm, float dpx, float dpy) {
+                                            [&](int a, int b, float W, float dm, float tx, float ty) {
                                                 const int k = (lx + a) * RY + (ly + b);
                                                 atomicAdd(&s_odd[0][k], dm);
-                                                atomicAdd(&s_odd[1][k], dpx);
-                                                atomicAdd(&s_odd[2][k], dpy);
+                                                atomicAdd(&s_odd[1][k], W * tx);
+                                                atomicAdd(&s_odd[2][k], W * ty);
                                             });
                 } else {
                     p2g_global_f32(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01,
@@ -369,9 +387,10 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
         }
     }
     sync();
+    float4 *part = reinterpret_cast<float4 *>(mom);   // [9 node offsets][TT cells], aliasing the moments
     if (tid < TT) {
 #pragma unroll
-        for (int q = 0; q < 27; q++) mom[q * TT + tid] = acc[q];
+        for (int q = 0; q < 9; q++) part[q * TT + tid] = make_float4(acc[3 * q], acc[3 * q + 1], acc[3 * q + 2], 0.f);
     }
     sync();
     for (int k = tid; k < RN; k += NT) {
@@ -386,10 +405,10 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
             for (int b = 0; b < 3; b++) {
                 const int cy = ny - b;
                 if (cy < 0 || cy >= TY) continue;
-                const int c = cx * TY + cy, q = (a * 3 + b) * 3;
-                m += mom[q * TT + c];
-                px += mom[(q + 1) * TT + c];
-                py += mom[(q + 2) * TT + c];
+                const float4 v = part[(a * 3 + b) * TT + cx * TY + cy];
+                m += v.x;
+                px += v.y;
+                py += v.z;
             }
         }
         m += s_odd[0][k]; px += s_odd[1][k]; py += s_odd[2][k];
@@ -449,7 +468,8 @@ static __global__ void __launch_bounds__(TILE_THREADS, 4)
     __shared__ float s_odd[3][RN];
     __shared__ int s_cs[TT + 1];
     __shared__ unsigned s_touch;
-    extern __shared__ float s_momf[];
+    extern __shared__ float4 s_momf4[];
+    float *const s_momf = reinterpret_cast<float *>(s_momf4);
     const int na = BATCH ? *nwork : *A1.n_active;
     const int tid = threadIdx.x;
     for (int k = tid; k < RN; k += blockDim.x) { s_odd[0][k] = 0.f; s_odd[1][k] = 0.f; s_odd[2][k] = 0.f; }
@@ -507,13 +527,13 @@ static __global__ void __launch_bounds__(TILE_THREADS, 4)
                 PointF s;
                 s.util = A.st[i];
                 if (s.util & (unsigned)kDisabled) {
-                    if (DO_P2G) s_momf[mom_idx(9, j)] = __int_as_float(BASE_NONE);
+                    if (DO_P2G) MomF(s_momf).none(j);
                     continue;
                 }
                 load_point_f32(A.st, A.pitch, i, s);
                 if (DO_G2P) {
                     if (!g2p_update_f32(P, A.Q, A.grain_tab, s, A.status, vsrc)) {
-                        if (DO_P2G) s_momf[mom_idx(9, j)] = __int_as_float(BASE_NONE);
+                        if (DO_P2G) MomF(s_momf).none(j);
                         continue;
                     }
                     store_point_f32(A.st, A.pitch, i, s, WRITE_VB, record);
