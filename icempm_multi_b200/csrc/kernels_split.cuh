@@ -157,7 +157,7 @@ __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitC
         split_dev(s.D, jm1, d00, d01);
         const float Je = 1.f + jm1;
         s.ptr = -(Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
-        s.qtr = 2.f * Q.mu / Je * sqrtf(d00 * d00 + d01 * d01);   // sqrt(2) mu/J |dev|, |dev| = sqrt(2(d00^2+d01^2))
+        s.qtr = __fdividef(2.f * Q.mu, Je) * sqrtf(d00 * d00 + d01 * d01);   // sqrt(2) mu/J |dev|, |dev| = sqrt(2(d00^2+d01^2))
         if (!(s.util & (unsigned)kCrushed)) {
             const GrainConstF *gc = tab + grain_slot((short)s.util);
             const float pmin2 = __ldg(&gc->pmin2), k = __ldg(&gc->k), msq = __ldg(&gc->msq);
@@ -250,7 +250,7 @@ __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const Split
         float jm1, d00, d01;
         split_dev(s.D, jm1, d00, d01);
         const float Je = 1.f + jm1;
-        const float s1 = Q.mu / Je, s2 = (Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
+        const float s1 = __fdividef(Q.mu, Je), s2 = (Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
         tau = {s1 * d00 + s2, s1 * d01, s1 * d01, -s1 * d00 + s2};
     }
     const int c = momf_col(j);
@@ -579,8 +579,9 @@ __device__ __forceinline__ int node_velocity_f32(const StepParams &P, const Spli
     vy = 0.f;
     int bin = -1;
     if (mass != 0.f) {
-        vx = px / mass;
-        vy = py / mass;
+        const float rm = __fdividef(1.f, mass);   // fast reciprocal (FP32 path)
+        vx = px * rm;
+        vy = py * rm;
         vy -= Q.dtg;
         const float v2 = vx * vx + vy * vy;
         if (v2 > Q.vmax_sq) {

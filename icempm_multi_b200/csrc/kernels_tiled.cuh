@@ -589,16 +589,17 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
             for (int j = tid; j < ce - cs; j += blockDim.x) {
                 const long i = cs + j;
                 PointState s;
-                s.util = __double_as_longlong(A.pts[i]);
-                if (s.util & kDisabled) {
-                    if (DO_P2G) mom_none(s_mom, j);
-                    continue;
-                }
+                // all eight lines requested before the first is tested (one memory latency)
                 const long pitch = A.pitch;
+                s.util = __double_as_longlong(A.pts[i]);
                 s.x = A.pts[i + pitch * 4];
                 s.y = A.pts[i + pitch * 5];
                 s.Jp = A.pts[i + pitch * 3];
                 s.F = {A.pts[i + pitch * 8], A.pts[i + pitch * 9], A.pts[i + pitch * 10], A.pts[i + pitch * 11]};
+                if (s.util & kDisabled) {
+                    if (DO_P2G) mom_none(s_mom, j);
+                    continue;
+                }
                 if (DO_G2P) {
                     if (!g2p_update(P, A.grain_tab, s, A.status, vsrc)) {
                         if (DO_P2G) mom_none(s_mom, j);
