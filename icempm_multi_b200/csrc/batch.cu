@@ -138,7 +138,7 @@ static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
     cudaGraph_t g = nullptr;
     int n = 0;
     CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    k_tile_f32<false, true, false, true><<<b->tile_grid, TILE_THREADS, MOMF_BYTES, b->stream>>>(
+    k_tile_f32<false, true, false, true><<<b->tile_grid, TILE_THREADS_F32, MOMF_BYTES, b->stream>>>(
         none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
     n++;
     for (int k = 0; k < nsteps; k++) {
@@ -146,10 +146,10 @@ static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
         k_update_list_f32<true><<<b->update_grid, 256, 0, b->stream>>>(SplitArgs{}, b->d_args, b->d_clk, b->d_tlist,
                                                                           b->d_tlist_n, 0.0, 0.0);
         if (k + 1 < nsteps)
-            k_tile_f32<true, true, false, true><<<b->tile_grid, TILE_THREADS, MOMF_BYTES, b->stream>>>(
+            k_tile_f32<true, true, false, true><<<b->tile_grid, TILE_THREADS_F32, MOMF_BYTES, b->stream>>>(
                 none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
         else
-            k_tile_f32<true, false, true, true><<<b->tile_grid, TILE_THREADS, 0, b->stream>>>(
+            k_tile_f32<true, false, true, true><<<b->tile_grid, TILE_THREADS_F32, 0, b->stream>>>(
                 none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
         n += 3;
     }
@@ -219,7 +219,7 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
     cudaMemsetAsync(b->d_tlist_n, 0, sizeof(unsigned) * 2, b->stream);
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false, true>, TILE_THREADS,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false, true>, TILE_THREADS_F32,
                                                   MOMF_BYTES);
     b->tile_grid = std::max(1, sms * std::max(per_sm, 1));
     b->update_grid = std::max(1, sms * 8);

@@ -122,7 +122,7 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(cudaFuncSetAttribute(k_tile_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PIPE_SMEM));
     h->pipe_grid = sms;
     per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false>, TILE_THREADS,
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false>, TILE_THREADS_F32,
                                                      MOMF_BYTES));
     h->tile_grid_f32 = std::max(1, sms * std::max(per_sm, 1));
     h->update_grid = (int)std::max(1L, std::min((long)(h->ntiles + 1) / 2, (long)sms * 8));
@@ -331,15 +331,15 @@ static int launch_tile_split(icy_mpm *h, int which, bool record)
     switch (which) {
     case 0:
         icy_prof_begin(h, K_TILE_G2P2G);
-        k_tile_f32<true, true, false><<<h->tile_grid_f32, TILE_THREADS, MOMF_BYTES, h->stream>>>(A);
+        k_tile_f32<true, true, false><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
         break;
     case 1:
         icy_prof_begin(h, K_TILE_P2G);
-        k_tile_f32<false, true, false><<<h->tile_grid_f32, TILE_THREADS, MOMF_BYTES, h->stream>>>(A);
+        k_tile_f32<false, true, false><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
         break;
     default:
         icy_prof_begin(h, K_TILE_G2P);
-        k_tile_f32<true, false, true><<<h->tile_grid_f32, TILE_THREADS, 0, h->stream>>>(A);
+        k_tile_f32<true, false, true><<<h->tile_grid_f32, TILE_THREADS_F32, 0, h->stream>>>(A);
         break;
     }
     icy_prof_end(h);

@@ -326,11 +326,11 @@ static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags,
                             });
     const int t0x = (bx + halo) / TX, t1x = (bx + 2 + halo) / TX;
     const int t0y = by / TY, t1y = (by + 2) / TY;
-    mark_tile(flags, tlist, tlist_n, inst, t0y * ntx + t0x);
-    if (t1x != t0x) mark_tile(flags, tlist, tlist_n, inst, t0y * ntx + t1x);
+    mark_tile(flags, tlist, tlist_n, inst, t0x, t0y, ntx);
+    if (t1x != t0x) mark_tile(flags, tlist, tlist_n, inst, t1x, t0y, ntx);
     if (t1y != t0y) {
-        mark_tile(flags, tlist, tlist_n, inst, t1y * ntx + t0x);
-        if (t1x != t0x) mark_tile(flags, tlist, tlist_n, inst, t1y * ntx + t1x);
+        mark_tile(flags, tlist, tlist_n, inst, t0x, t1y, ntx);
+        if (t1x != t0x) mark_tile(flags, tlist, tlist_n, inst, t1x, t1y, ntx);
     }
 }
 
@@ -426,6 +426,9 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
     sync();
 }
 
+// Threads and resident CTAs per SM of the FP32 tile kernel.
+constexpr int TILE_THREADS_F32 = 256, TILE_CTAS_F32 = 4;
+
 // Work items of a batch: (instance, tile) pairs over all instances.
 struct BatchItem { int inst, tile; };
 
@@ -460,7 +463,7 @@ __device__ __forceinline__ void prefetch_next_item(const SplitArgs &A1, const Sp
 // instances, each with its own parameters, grid and points (Aarr[inst]), and
 // the record-PQ flag of each instance comes from rec[inst].
 template <bool DO_G2P, bool DO_P2G, bool WRITE_VB, bool BATCH = false>
-static __global__ void __launch_bounds__(TILE_THREADS, 4)
+static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     k_tile_f32(const __grid_constant__ SplitArgs A1, const SplitArgs *__restrict__ Aarr = nullptr, const BatchItem *__restrict__ work = nullptr,
                const int *__restrict__ nwork = nullptr, const int *__restrict__ rec = nullptr)
 {
@@ -550,7 +553,7 @@ static __global__ void __launch_bounds__(TILE_THREADS, 4)
             if (DO_P2G && cs == ps && tid >= TT && tid < TT + S_JP + 2)
                 prefetch_next_item<BATCH>(A1, Aarr, work, ti + gridDim.x, na, tid - TT);
             if (DO_P2G)
-                p2g_cells_and_flush_f32<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
+                p2g_cells_and_flush_f32<TILE_THREADS_F32>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
                                                       [] { __syncthreads(); });
         }
         if (DO_P2G) {
@@ -559,7 +562,7 @@ static __global__ void __launch_bounds__(TILE_THREADS, 4)
             __syncthreads();
             if (tid < 9 && ((s_touch >> tid) & 1u)) {
                 const int ntx = tx + tid % 3 - 1, nty = ty + tid / 3 - 1;
-                mark_tile(A.flags, A.tlist, A.tlist_n, A.inst, nty * A.G.ntx + ntx);
+                mark_tile(A.flags, A.tlist, A.tlist_n, A.inst, ntx, nty, A.G.ntx);
             }
             moved = __reduce_add_sync(0xffffffffu, moved);
             if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
@@ -805,9 +808,8 @@ static __global__ void __launch_bounds__(256) k_update_list_f32(const __grid_con
             const int2 it = tlist[e];
             inst[u] = it.x;
             const SplitArgs &A = BATCH ? Aarr[it.x] : A1;
-            const int t = it.y;
-            const int ty = t / A.G.ntx, tx = t - ty * A.G.ntx;
-            if (l == 0) A.flags[t] = 0u;
+            const int tx = it.y & 0xffff, ty = it.y >> 16;
+            if (l == 0) A.flags[ty * A.G.ntx + tx] = 0u;
             gx[u] = tx * TX + l / TY - A.P.halo;
             gy[u] = ty * TY + (l & (TY - 1));
             if (gx[u] >= A.P.gridx + A.P.halo || gy[u] >= A.P.gridy) continue;   // past the grid edge

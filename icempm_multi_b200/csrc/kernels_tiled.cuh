@@ -63,12 +63,14 @@ struct TileArgs {
     int record_pq;
 };
 
-// Marks node tile t as written by P2G since the last grid update and appends
-// (inst, t) to the list the update visits, once per tile.
-__device__ __forceinline__ void mark_tile(unsigned *flags, int2 *tlist, unsigned *tlist_n, int inst, int t)
+// Marks node tile (tx, ty) as written by P2G since the last grid update and
+// appends (inst, ty << 16 | tx) to the list the update visits, once per tile.
+__device__ __forceinline__ void mark_tile(unsigned *flags, int2 *tlist, unsigned *tlist_n, int inst, int tx, int ty,
+                                          int ntx)
 {
+    const int t = ty * ntx + tx;
     if (*(volatile unsigned *)(flags + t) == 0u && atomicExch(flags + t, 1u) == 0u)
-        tlist[atomicAdd(tlist_n, 1u)] = make_int2(inst, t);
+        tlist[atomicAdd(tlist_n, 1u)] = make_int2(inst, (ty << 16) | tx);
 }
 
 // Called by thread 0 of every CTA of a list-driven grid update after its last
@@ -296,11 +298,11 @@ static __device__ __noinline__ void p2g_global(GridView g, unsigned *flags, int2
                         });
     const int t0x = (bx + halo) / TX, t1x = (bx + 2 + halo) / TX;
     const int t0y = by / TY, t1y = (by + 2) / TY;
-    mark_tile(flags, tlist, tlist_n, 0, t0y * ntx + t0x);
-    if (t1x != t0x) mark_tile(flags, tlist, tlist_n, 0, t0y * ntx + t1x);
+    mark_tile(flags, tlist, tlist_n, 0, t0x, t0y, ntx);
+    if (t1x != t0x) mark_tile(flags, tlist, tlist_n, 0, t1x, t0y, ntx);
     if (t1y != t0y) {
-        mark_tile(flags, tlist, tlist_n, 0, t1y * ntx + t0x);
-        if (t1x != t0x) mark_tile(flags, tlist, tlist_n, 0, t1y * ntx + t1x);
+        mark_tile(flags, tlist, tlist_n, 0, t0x, t1y, ntx);
+        if (t1x != t0x) mark_tile(flags, tlist, tlist_n, 0, t1x, t1y, ntx);
     }
 }
 
@@ -528,7 +530,7 @@ __device__ __forceinline__ void mark_node_tiles(const TileArgs &A, int tx, int t
 {
     if (lane9 < 9 && ((touch >> lane9) & 1u)) {
         const int ntx = tx + lane9 % 3 - 1, nty = ty + lane9 / 3 - 1;
-        mark_tile(A.flags, A.tlist, A.tlist_n, 0, nty * A.G.ntx + ntx);
+        mark_tile(A.flags, A.tlist, A.tlist_n, 0, ntx, nty, A.G.ntx);
     }
 }
 
@@ -820,9 +822,9 @@ static __global__ void __launch_bounds__(256) k_update_list(StepParams P, TileGe
     static_assert(TT == 128, "two node tiles per 256-thread CTA");
     const int l = threadIdx.x & (TT - 1);
     for (unsigned e = blockIdx.x * 2 + (threadIdx.x >> 7); e < n; e += gridDim.x * 2) {
-        const int t = tlist[e].y;
-        const int ty = t / G.ntx, tx = t - ty * G.ntx;
-        if (l == 0) flags[t] = 0u;
+        const int e2 = tlist[e].y;
+        const int tx = e2 & 0xffff, ty = e2 >> 16;
+        if (l == 0) flags[ty * G.ntx + tx] = 0u;
         const int gx = tx * TX + l / TY - P.halo, gy = ty * TY + (l & (TY - 1));
         if (gx >= P.gridx + P.halo || gy >= P.gridy) continue;   // past the grid edge
         const long q = g.idx(gx, gy);
