@@ -626,7 +626,7 @@ constexpr int UPD_TILES = 4;
 // Grid update of the listed node tiles (see k_update_list in kernels_tiled.cuh),
 // defined after BatchClock below.
 template <bool BATCH>
-static __global__ void __launch_bounds__(256) k_update_list_f32(const __grid_constant__ SplitArgs A1,
+static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_constant__ SplitArgs A1,
                                                                 const SplitArgs *__restrict__ Aarr,
                                                                 const BatchClock *__restrict__ clk,
                                                                 const int2 *__restrict__ tlist, unsigned *tlist_n,
@@ -779,7 +779,7 @@ static __global__ void k_batch_advance(BatchClock *clk, int *rec, int nslots)
 // memory; in a batch every entry names its member, whose indenter position
 // comes from the member's clock and whose force bins take the force directly.
 template <bool BATCH>
-static __global__ void __launch_bounds__(256) k_update_list_f32(const __grid_constant__ SplitArgs A1,
+static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_constant__ SplitArgs A1,
                                                                 const SplitArgs *__restrict__ Aarr,
                                                                 const BatchClock *__restrict__ clk,
                                                                 const int2 *__restrict__ tlist, unsigned *tlist_n,
