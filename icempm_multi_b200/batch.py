@@ -77,3 +77,38 @@ class Batch:
 def device_bytes(params, capacity, precision=PRECISION_FP32_SPLIT):
     """Device memory an instance of this size allocates."""
     return lib().icy_mpm_device_bytes(C.byref(params), int(capacity), int(precision))
+
+
+def main():
+    """python -m icempm_multi_b200.batch [--instances 256] [--steps 10] [--seed 7] [--repeat 2]
+
+    Builds the batched workload (icempm_multi_b200.workloads.batch_scenarios)
+    and advances it `repeat` times by `steps` sub-steps (the first call
+    captures the CUDA graph), printing the device time of each call."""
+    import argparse
+    import time
+
+    from .workloads import batch_scenarios, make_workload
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--repeat", type=int, default=2)
+    a = ap.parse_args()
+    b = Batch(a.instances)
+    n = 0
+    for w in batch_scenarios(a.instances, seed=a.seed):
+        p, soa = make_workload(w)
+        b.add(p, soa)
+        n += soa.size
+    for r in range(a.repeat):
+        t0 = time.perf_counter()
+        b.step(a.steps)
+        b.synchronize()
+        print(f"call {r}: {a.steps} steps of {a.instances} members ({n} points) in "
+              f"{1e3 * (time.perf_counter() - t0):.2f} ms", flush=True)
+    b.close()
+
+
+if __name__ == "__main__":
+    main()
