@@ -359,7 +359,7 @@ def measure_serve(rate=10.0, duration=12.0, seed=11):
         n = int(round(np.exp(rng.uniform(np.log(5e3), np.log(2e6)))))
         w = floe_scenario(n, E=float(rng.uniform(5e8, 2e9)), phi=float(rng.uniform(45, 70)),
                           v_ind=float(rng.uniform(0.5, 3.0)), seed=seed * 100 + k)
-        scenes.append(mk(w))
+        scenes.append(mk(w, pinned=True))
     n_req = max(8, int(rate * duration))
     reqs = poisson_requests(scenes, rate, n_req, round_steps=50, seed=seed)
     offered = sum(r.soa.size * r.steps for r in reqs) / max(reqs[-1].arrival, 1e-9)

@@ -219,6 +219,10 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
     cudaMemsetAsync(b->d_tlist_n, 0, sizeof(unsigned) * 2, b->stream);
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaFuncSetAttribute(k_tile_f32<true, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)MOMF_BYTES);
+    cudaFuncSetAttribute(k_tile_f32<false, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)MOMF_BYTES);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false, true>, TILE_THREADS_F32,
                                                   MOMF_BYTES);
     b->tile_grid = std::max(1, sms * std::max(per_sm, 1));

@@ -3,6 +3,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "instance.cuh"
 #include "kernels_split.cuh"
@@ -36,10 +39,61 @@ static GridView grid_view(icy_mpm *h)
 
 static TileGeom tile_geom(icy_mpm *h) { return TileGeom{h->ntx, h->nty, h->ntiles}; }
 
-template <typename T>
-static cudaError_t dalloc(T **p, size_t count)
+// Device memory of instances comes from one stream-ordered pool per device
+// that keeps freed blocks for reuse (release threshold: never), so that
+// creating and destroying instances -- as the serving loop does all the
+// time -- neither synchronises the device nor goes back to the driver.
+static cudaMemPool_t instance_pool(int device)
 {
-    return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(count, 1));
+    static std::mutex m;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> g(m);
+    auto it = pools.find(device);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[device] = pool;
+    return pool;
+}
+
+template <typename T>
+static cudaError_t dalloc(icy_mpm *h, T **p, size_t count)
+{
+    cudaMemPool_t pool = instance_pool(h->device);
+    if (!pool) return cudaErrorMemoryAllocation;
+    return cudaMallocFromPoolAsync((void **)p, sizeof(T) * std::max<size_t>(count, 1), pool, h->stream);
+}
+
+// One pinned int per instance for reading the device status back, from a
+// process-wide page-locked block (pinning four bytes costs as much as pinning
+// megabytes, and instances come and go).
+static std::mutex g_slot_mutex;
+static std::vector<int *> g_free_slots;
+
+static int *status_slot_get()
+{
+    std::lock_guard<std::mutex> g(g_slot_mutex);
+    if (g_free_slots.empty()) {
+        int *block = nullptr;
+        if (cudaMallocHost(&block, sizeof(int) * 1024) != cudaSuccess) return nullptr;
+        for (int k = 1023; k >= 0; k--) g_free_slots.push_back(block + k);
+    }
+    int *s = g_free_slots.back();
+    g_free_slots.pop_back();
+    return s;
+}
+
+static void status_slot_put(int *s)
+{
+    if (!s) return;
+    std::lock_guard<std::mutex> g(g_slot_mutex);
+    g_free_slots.push_back(s);
 }
 
 int icy_instance_allocate(icy_mpm *h, unsigned capacity)
@@ -61,51 +115,52 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
         // FP32 state (two buffers for the binning permutation), FP32 grid,
         // FP64 staging for the HSSOA conversion at upload/download
         h->stage_n = std::min<long>(h->pitch, 1L << 20);
-        if ((e = dalloc(&h->d_st, S_NLINES * h->pitch)) != cudaSuccess ||
-            (e = dalloc(&h->d_st_alt, S_NLINES * h->pitch)) != cudaSuccess ||
-            (e = dalloc(&h->d_stage, 16 * h->stage_n)) != cudaSuccess) {
+        if ((e = dalloc(h, &h->d_st, S_NLINES * h->pitch)) != cudaSuccess ||
+            (e = dalloc(h, &h->d_st_alt, S_NLINES * h->pitch)) != cudaSuccess ||
+            (e = dalloc(h, &h->d_stage, 16 * h->stage_n)) != cudaSuccess) {
             icy_set_error("cudaMalloc(particles)", e);
             return ICY_ERR_OUT_OF_MEMORY;
         }
-        if ((e = dalloc(&h->d_gridf, 5 * h->n_nodes)) != cudaSuccess) {
+        if ((e = dalloc(h, &h->d_gridf, 5 * h->n_nodes)) != cudaSuccess) {
             icy_set_error("cudaMalloc(grid)", e);
             return ICY_ERR_OUT_OF_MEMORY;
         }
-        CK(cudaMalloc(&h->d_grainf, sizeof(GrainConstF) * GRAIN_TAB));
+        CK(dalloc(h, reinterpret_cast<GrainConstF **>(&h->d_grainf), GRAIN_TAB));
         CK(cudaMemsetAsync(h->d_st, 0, sizeof(unsigned) * S_NLINES * h->pitch, h->stream));
         CK(cudaMemsetAsync(h->d_gridf, 0, sizeof(float) * 5 * h->n_nodes, h->stream));
     } else {
-        if ((e = dalloc(&h->d_pts, 16 * h->pitch)) != cudaSuccess ||
-            (e = dalloc(&h->d_pts_alt, 16 * h->pitch)) != cudaSuccess) {
+        if ((e = dalloc(h, &h->d_pts, 16 * h->pitch)) != cudaSuccess ||
+            (e = dalloc(h, &h->d_pts_alt, 16 * h->pitch)) != cudaSuccess) {
             icy_set_error("cudaMalloc(particles)", e);
             return ICY_ERR_OUT_OF_MEMORY;
         }
-        if ((e = dalloc(&h->d_grid, 5 * h->n_nodes)) != cudaSuccess) {
+        if ((e = dalloc(h, &h->d_grid, 5 * h->n_nodes)) != cudaSuccess) {
             icy_set_error("cudaMalloc(grid)", e);
             return ICY_ERR_OUT_OF_MEMORY;
         }
         CK(cudaMemsetAsync(h->d_pts, 0, sizeof(double) * 16 * h->pitch, h->stream));
         CK(cudaMemsetAsync(h->d_grid, 0, sizeof(double) * 5 * h->n_nodes, h->stream));
     }
-    CK(dalloc(&h->d_oidx, h->pitch));
-    CK(dalloc(&h->d_oidx_alt, h->pitch));
-    CK(dalloc(&h->d_keys, h->pitch));
-    CK(dalloc(&h->d_ranks, h->pitch));
+    CK(dalloc(h, &h->d_oidx, h->pitch));
+    CK(dalloc(h, &h->d_oidx_alt, h->pitch));
+    CK(dalloc(h, &h->d_keys, h->pitch));
+    CK(dalloc(h, &h->d_ranks, h->pitch));
     const long nkeys = (long)h->ntiles * TT + 1;   // cells + the disabled / out-of-grid bucket
     h->scan_blocks = (int)((nkeys + SCAN_BLOCK - 1) / SCAN_BLOCK);
-    CK(dalloc(&h->d_counts, nkeys));
-    CK(dalloc(&h->d_start, nkeys + 1));
-    CK(dalloc(&h->d_block_sums, h->scan_blocks));
-    CK(dalloc(&h->d_active, h->ntiles));
-    CK(dalloc(&h->d_nactive, 1));
-    CK(dalloc(&h->d_flags, h->ntiles));
-    CK(cudaMalloc(&h->d_tlist, sizeof(int2) * h->ntiles));
-    CK(dalloc(&h->d_tlist_n, 2));
-    CK(dalloc(&h->d_moved, 1));
-    CK(dalloc(&h->d_acc, 2 * h->prm.n_indenter_subdivisions));
-    CK(dalloc(&h->d_status, 1));
-    CK(dalloc(&h->d_grain, GRAIN_TAB));
-    CK(cudaMallocHost(&h->h_status, sizeof(int)));
+    CK(dalloc(h, &h->d_counts, nkeys));
+    CK(dalloc(h, &h->d_start, nkeys + 1));
+    CK(dalloc(h, &h->d_block_sums, h->scan_blocks));
+    CK(dalloc(h, &h->d_active, h->ntiles));
+    CK(dalloc(h, &h->d_nactive, 1));
+    CK(dalloc(h, &h->d_flags, h->ntiles));
+    CK(dalloc(h, &h->d_tlist, h->ntiles));
+    CK(dalloc(h, &h->d_tlist_n, 2));
+    CK(dalloc(h, &h->d_moved, 1));
+    CK(dalloc(h, &h->d_acc, 2 * h->prm.n_indenter_subdivisions));
+    CK(dalloc(h, &h->d_status, 1));
+    CK(dalloc(h, &h->d_grain, GRAIN_TAB));
+    h->h_status = status_slot_get();
+    if (!h->h_status) return ICY_ERR_OUT_OF_MEMORY;
     CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
     CK(cudaMemsetAsync(h->d_tlist_n, 0, sizeof(unsigned) * 2, h->stream));
     CK(cudaMemsetAsync(h->d_nactive, 0, sizeof(int), h->stream));
@@ -122,6 +177,10 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(cudaFuncSetAttribute(k_tile_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PIPE_SMEM));
     h->pipe_grid = sms;
     per_sm = 0;
+    CK(cudaFuncSetAttribute(k_tile_f32<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)MOMF_BYTES));
+    CK(cudaFuncSetAttribute(k_tile_f32<false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)MOMF_BYTES));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false>, TILE_THREADS_F32,
                                                      MOMF_BYTES));
     h->tile_grid_f32 = std::max(1, sms * std::max(per_sm, 1));
@@ -140,12 +199,14 @@ void icy_instance_free(icy_mpm *h)
                     h->d_counts, h->d_start, h->d_active, h->d_nactive, h->d_flags, h->d_moved, h->d_acc,
                     h->d_status, h->d_block_sums, h->d_grain, h->d_st, h->d_st_alt, h->d_stage, h->d_gridf,
                     h->d_grainf, h->d_tlist, h->d_tlist_n};
-    for (void *p : ptrs) cudaFree(p);
+    cudaStream_t fs = h->stream ? h->stream : h->own_stream;
+    for (void *p : ptrs)
+        if (p) cudaFreeAsync(p, fs);   // back to the pool, after the stream's work
     h->d_st = h->d_st_alt = nullptr;
     h->d_stage = nullptr;
     h->d_gridf = nullptr;
     h->d_grainf = nullptr;
-    cudaFreeHost(h->h_status);
+    status_slot_put(h->h_status);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     h->d_pts = h->d_pts_alt = h->d_grid = h->d_acc = nullptr;
     h->d_oidx = h->d_oidx_alt = h->d_keys = h->d_ranks = h->d_counts = h->d_start = nullptr;

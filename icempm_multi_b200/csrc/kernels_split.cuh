@@ -212,7 +212,8 @@ __device__ __forceinline__ void load_point_f32(const unsigned *__restrict__ st, 
 // after every 4 points (the cell phase reads points about 4 apart per lane):
 //   m0 = (fx, fy, mass, m vx),  m1 = (m vy, S00, S01, S10),  m2 = (S11, base)
 // with S = m Bp - dt vol Dp_inv tau (simulation/kernels.cuh:57-92).
-constexpr int MOMF_N = CAP + CAP / 4;
+constexpr int CAPF = 1280;                // points per chunk of the FP32 tile kernel
+constexpr int MOMF_N = CAPF + CAPF / 4;
 constexpr size_t MOMF_BYTES = (2 * sizeof(float4) + sizeof(float2)) * MOMF_N;
 static_assert(9 * TT * sizeof(float4) <= MOMF_BYTES, "cell partials alias the moment buffer");
 __device__ __forceinline__ int momf_col(int j) { return j + (j >> 2); }
@@ -427,7 +428,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
 }
 
 // Threads and resident CTAs per SM of the FP32 tile kernel.
-constexpr int TILE_THREADS_F32 = 256, TILE_CTAS_F32 = 4;
+constexpr int TILE_THREADS_F32 = 256, TILE_CTAS_F32 = 3;
 
 // Work items of a batch: (instance, tile) pairs over all instances.
 struct BatchItem { int inst, tile; };
@@ -523,8 +524,8 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             }
         };
         unsigned touch = 0;
-        for (int cs = ps; cs < pe; cs += CAP) {
-            const int ce = min(cs + CAP, pe);
+        for (int cs = ps; cs < pe; cs += CAPF) {
+            const int ce = min(cs + CAPF, pe);
             for (int j = tid; j < ce - cs; j += blockDim.x) {
                 const long i = cs + j;
                 PointF s;
@@ -549,9 +550,11 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                 if (DO_P2G) p2g_moments_f32(P, A.Q, s, s_momf, j, A.status);
             }
             __syncthreads();
-            // threads without a cell in the cell phase start the next item's loads
-            if (DO_P2G && cs == ps && tid >= TT && tid < TT + S_JP + 2)
-                prefetch_next_item<BATCH>(A1, Aarr, work, ti + gridDim.x, na, tid - TT);
+            // threads without a cell in the cell phase (else the last ones) start the
+            // next item's loads
+            constexpr int PF0 = TT < TILE_THREADS_F32 ? TT : TILE_THREADS_F32 - (S_JP + 2);
+            if (DO_P2G && cs == ps && tid >= PF0 && tid < PF0 + S_JP + 2)
+                prefetch_next_item<BATCH>(A1, Aarr, work, ti + gridDim.x, na, tid - PF0);
             if (DO_P2G)
                 p2g_cells_and_flush_f32<TILE_THREADS_F32>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
                                                       [] { __syncthreads(); });
@@ -773,8 +776,8 @@ static __global__ void k_batch_advance(BatchClock *clk, int *rec, int nslots)
     clk[i] = c;
 }
 
-// Grid update of the listed node tiles: each half-CTA takes one 16 x 8 node
-// tile (one thread per node), clears the tile's mark, and the last CTA empties
+// Grid update of the listed node tiles: each group of TT threads takes one
+// TX x TY node tile (one thread per node), clears its mark, and the last CTA empties
 // the list.  Alone (BATCH = false) the forces are summed per CTA in shared
 // memory; in a batch every entry names its member, whose indenter position
 // comes from the member's clock and whose force bins take the force directly.
@@ -792,11 +795,12 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
     }
     bool any = false;
     const unsigned n = *(volatile unsigned *)tlist_n;
-    static_assert(TT == 128, "two node tiles per 256-thread CTA");
-    const int l = threadIdx.x & (TT - 1);
-    const unsigned stride = gridDim.x * 2;
+    constexpr int TPC = 256 / TT;   // node tiles per CTA pass
+    static_assert(256 % TT == 0, "whole node tiles per 256-thread CTA");
+    const int l = threadIdx.x % TT;
+    const unsigned stride = gridDim.x * TPC;
     // UPD_TILES tiles per pass, their loads issued together
-    for (unsigned e0 = blockIdx.x * 2 + (threadIdx.x >> 7); e0 < n; e0 += stride * UPD_TILES) {
+    for (unsigned e0 = blockIdx.x * TPC + threadIdx.x / TT; e0 < n; e0 += stride * UPD_TILES) {
         long q[UPD_TILES];
         int inst[UPD_TILES], gx[UPD_TILES], gy[UPD_TILES];
         float m[UPD_TILES], px[UPD_TILES], py[UPD_TILES];

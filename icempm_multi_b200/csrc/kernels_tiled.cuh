@@ -25,11 +25,11 @@
 
 namespace icy_dev {
 
-constexpr int TX = 16, TY = 8, TT = TX * TY;   // stencil bases (cells) per tile
+constexpr int TX = 32, TY = 8, TT = TX * TY;   // stencil bases (cells) per tile
 constexpr int RM = 1;                          // drift margin (cells) of the staged region
 constexpr int RX = TX + 2 + 2 * RM, RY = TY + 2 + 2 * RM, RN = RX * RY;
 constexpr int TILE_THREADS = 256;
-constexpr int CAP = 640;                       // points staged per chunk
+constexpr int CAP = 704;                       // points staged per chunk
 constexpr int BASE_NONE = 0x7fffffff;
 constexpr int ICY_TIMEOUT_CODE = 108;          // ICY_ERR_TIMEOUT
 
@@ -806,8 +806,8 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(TileArgs A
 }
 
 // Grid update of the nodes of the listed tiles (simulation/kernels.cuh:164-301):
-// each half-CTA takes one 16 x 8 node tile (one thread per node, the 8 nodes of
-// a tile column contiguous in memory), computes the velocities, zeroes the
+// each group of TT threads takes one TX x TY node tile (one thread per node, the
+// TY nodes of a tile column contiguous in memory), computes the velocities, zeroes the
 // accumulators for the next step and clears the tile's mark; the last CTA
 // empties the list.
 static __global__ void __launch_bounds__(256) k_update_list(StepParams P, TileGeom G, GridView g, unsigned *flags,
@@ -819,9 +819,10 @@ static __global__ void __launch_bounds__(256) k_update_list(StepParams P, TileGe
     __syncthreads();
     bool any = false;
     const unsigned n = *(volatile unsigned *)tlist_n;
-    static_assert(TT == 128, "two node tiles per 256-thread CTA");
-    const int l = threadIdx.x & (TT - 1);
-    for (unsigned e = blockIdx.x * 2 + (threadIdx.x >> 7); e < n; e += gridDim.x * 2) {
+    constexpr int TPC = 256 / TT;   // node tiles per CTA pass
+    static_assert(256 % TT == 0, "whole node tiles per 256-thread CTA");
+    const int l = threadIdx.x % TT;
+    for (unsigned e = blockIdx.x * TPC + threadIdx.x / TT; e < n; e += gridDim.x * TPC) {
         const int e2 = tlist[e].y;
         const int tx = e2 & 0xffff, ty = e2 >> 16;
         if (l == 0) flags[ty * G.ntx + tx] = 0u;

@@ -60,6 +60,7 @@ class Server:
         self.rounds = 0
         self.peak_live = 0
         self.peak_bytes = 0.0
+        self._scratch = {}      # page-locked download buffers by capacity, when results are not kept
 
     def close(self):
         self.batch.close()
@@ -81,10 +82,20 @@ class Server:
         self.peak_live = max(self.peak_live, len(self.running))
         self.peak_bytes = max(self.peak_bytes, self.used)
 
+    def _out_buffer(self, capacity):
+        """Result buffer: a new one when results are kept, else a reused page-locked one."""
+        if self.keep_results:
+            return HostSideSOA(capacity)
+        cap = 1 << max(int(capacity) - 1, 1).bit_length()
+        buf = self._scratch.get(cap)
+        if buf is None:
+            buf = self._scratch[cap] = HostSideSOA(cap, pinned=True)
+        return buf
+
     def _complete(self, t0):
         for slot, r in list(self.running.items()):
             if r.steps_done >= r.steps:
-                out = HostSideSOA(r.soa.capacity)
+                out = self._out_buffer(r.soa.capacity)
                 r.sim_time, _, r.bins = self.batch.download(slot, out)
                 self.batch.remove(slot)
                 r.done = time.perf_counter() - t0
