@@ -36,17 +36,20 @@ from icempm_multi_b200.workloads import LARGE, MEDIUM  # noqa: E402
 from icempm_multi_b200.workloads import make_workload as _make, workload_params  # noqa: E402
 
 METRIC = "particle-steps/s"
-# algorithmic bytes per particle-step of the FP64 path, per kernel (FP64 HSSOA fields
-# each phase must touch): P2G reads utility, pos, vel, Fe, Bp = 13 doubles; G2P reads
-# utility, pos, Fe, Jp = 8 doubles and writes 14 doubles
-ALG_BYTES = {"k_p2g_simple": 13 * 8, "k_g2p_simple": (8 + 14) * 8,
-             # fused G2P(n)+P2G(n+1): the persistent point state (utility, pos, Fe, Jp)
-             # read once and written once; vel and Bp are not stored between steps
-             "k_tile_g2p2g": (8 + 8) * 8,
-             "k_tile_p2g": 14 * 8, "k_tile_g2p": (8 + 14) * 8}
-# FP32 split state: 4-byte utility, packed cell, offset (2), Fe - I (4), Jp = 9 words
-# read and written by the fused step
-ALG_BYTES_F32 = {"k_tile_g2p2g": (9 + 9) * 4, "k_tile_p2g": 15 * 4, "k_tile_g2p": (9 + 15) * 4}
+# Algorithmic bytes per particle-step, per kernel: the fields of the particle
+# layout each phase of the reference step must touch (P2G reads utility, pos,
+# vel, Fe, Bp; G2P reads utility, pos, Fe, Jp and writes pos, vel, Fe, Bp, Jp,
+# utility), at the stored width of the layout:
+#   FP64 HSSOA: P2G 13 x 8 = 104 B, G2P 8 x 8 + 14 x 8 = 176 B, step 280 B
+#   FP32 split: P2G 56 B (utility 4, pos 12, vel 8, Fe 16, Bp 16), G2P 36 + 60 B, step 152 B
+# A fused G2P(n)+P2G(n+1) launch does one whole step's work: 280 / 152 B.
+ALG_BYTES = {"k_p2g_simple": 104, "k_g2p_simple": 176, "k_tile_g2p2g": 280, "k_tile_p2g": 104,
+             "k_tile_g2p": 176}
+ALG_BYTES_F32 = {"k_tile_g2p2g": 152, "k_tile_p2g": 56, "k_tile_g2p": 96}
+# Bytes per particle-step the fused launch itself has to move: the persistent
+# state read once and written once (velocity and Bp stay in registers from
+# G2P(n) to P2G(n+1)): FP64 8 + 8 doubles, FP32 split 9 + 9 words.
+MOVED_BYTES = {"fp64": 128, "fp32": 72}
 
 
 WORKLOAD = LARGE
@@ -420,6 +423,7 @@ def main():
     per_launch_ms = tot_ms / max(cnt, 1)
     alg = (ALG_BYTES_F32 if args.precision == "fp32" else ALG_BYTES).get(name, 0) * n
     achieved = alg / (per_launch_ms / 1e3) / 1e9 if per_launch_ms > 0 else 0.0
+    moved = MOVED_BYTES[args.precision] * n if name == "k_tile_g2p2g" else alg
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
@@ -445,7 +449,11 @@ def main():
                     for k, v in prof.items()},
         "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if peak else None, "traffic": traffic, "peak_kind": peak_kind,
-                     "alg_bytes_per_launch": alg},
+                     "alg_bytes_per_launch": alg,
+                     # the same launch against the bytes the fused design moves (no vel/Bp round trip)
+                     "moved_bytes_per_launch": moved,
+                     "moved_frac": (moved / (per_launch_ms / 1e3) / 1e9) / peak if peak and per_launch_ms > 0
+                     else None},
         "clocks": r["clocks"],
     }
 
@@ -464,6 +472,9 @@ def main():
             try:
                 out["batched"] = measure_batch()
                 out["served"] = measure_serve()
+                # the same trace at twice the arrival rate: more than the GPU can take,
+                # so throughput shows the serving capacity and latency the queueing
+                out["served_overload"] = measure_serve(rate=20.0, duration=6.0)
             except Exception as e:
                 out["batched_or_served_error"] = str(e)[:300]
         # ---- CPU baseline ------------------------------------------------------------------
