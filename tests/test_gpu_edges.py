@@ -1,0 +1,154 @@
+"""GPU edge cases of the hot path, through the C-ABI, against the FP64 oracle:
+an empty instance, stencil bases exactly on the truncation boundary of
+(int)(x/h - 0.5) (simulation/kernels.cuh:90), the indenter centre exactly on
+a node with mass (normalize of a zero vector, kernels.cuh:270), points next
+to every wall, tiles holding more points than one staged chunk, and the full
+9.6 M-point instance through size-independent checks (FP32 against FP64,
+tiled FP64 against the one-thread-per-item kernels)."""
+import numpy as np
+import pytest
+
+from icempm_multi_b200 import GPUImplementation
+from icempm_multi_b200._lib import PRECISION_FP32_SPLIT, PRECISION_FP64
+from icempm_multi_b200.hssoa import HostSideSOA, make_block
+from scenarios import params_for, standard
+from test_gpu_parity import TOL, assert_close, field_errors, run_gpu
+from test_gpu_split import POS_TOL, run_split
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def oracle(built):
+    from oracle.oracle import Oracle
+    return Oracle()
+
+
+@pytest.mark.parametrize("precision", [PRECISION_FP64, PRECISION_FP32_SPLIT])
+def test_empty_instance(precision):
+    p, _ = standard()
+    p.nPtsTotal = 0
+    empty = HostSideSOA(16)
+    g = GPUImplementation(p, empty, precision=precision)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.reset_indenter_force_accumulator()
+    t = g.run_steps(0, 25, 0.0)
+    assert t == pytest.approx(25 * p.InitialTimeStep)
+    g.transfer_from_device()
+    assert empty.size == 0 and np.all(g.indenter_bins == 0)
+    g.close()
+
+
+def _exact_positions(p, soa):
+    """Move some points onto exact truncation boundaries: x/h - 0.5 integer
+    (base = that integer, weight w2 = 0), x/h integer, and one ulp either side."""
+    h = p.cellsize
+    n = soa.size
+    idx = np.arange(0, n, max(n // 24, 1))[:24]
+    cx = np.floor(soa.pos[0, idx] / h)
+    cy = np.floor(soa.pos[1, idx] / h)
+    kinds = np.arange(len(idx)) % 4
+    fx = np.where(kinds == 0, cx + 0.5, np.where(kinds == 1, cx + 1.0, cx + 0.5))
+    x = fx * h
+    x = np.where(kinds == 2, np.nextafter(x, -np.inf), np.where(kinds == 3, np.nextafter(x, np.inf), x))
+    y = (cy + np.where(kinds % 2 == 0, 0.5, 1.0)) * h
+    soa.pos[0, idx] = x
+    soa.pos[1, idx] = y
+    return idx
+
+
+def test_truncation_boundaries_match_oracle(oracle):
+    p, soa = standard(seed=31)
+    _exact_positions(p, soa)
+    ref = soa.clone()
+    assert oracle.run(p, ref, 0, 60)[0] == 0
+    out, _, _, _ = run_gpu(p, soa, 60)
+    assert_close(field_errors(out, ref))
+    out32, _, _ = run_split(p, soa, 60)
+    assert field_errors(out32, ref)["pos"] <= POS_TOL
+
+
+def test_indenter_centre_on_a_node(oracle):
+    p, soa = standard(seed=32, IndVelocity=0.0)
+    h = p.cellsize
+    k = soa.size // 2
+    bx = int(soa.pos[0, k] / h - 0.5)
+    by = int(soa.pos[1, k] / h - 0.5)
+    # the centre exactly on node (bx + 1, by + 1), which holds mass from point k
+    p.indenter_x = p.indenter_x_initial = (bx + 1) * h
+    p.indenter_y = p.indenter_y_initial = (by + 1) * h
+    ref = soa.clone()
+    err, _, bins_ref = oracle.run(p, ref, 0, 40)
+    assert err == 0
+    out, _, bins, _ = run_gpu(p, soa, 40)
+    assert np.all(np.isfinite(out.pos)) and np.all(np.isfinite(out.vel)) and np.all(np.isfinite(bins))
+    assert_close(field_errors(out, ref))
+    fr, fo = bins_ref.reshape(-1, 2).sum(0), bins.reshape(-1, 2).sum(0)
+    assert np.allclose(fo, fr, rtol=1e-6, atol=1e-6 * (np.abs(fr).max() + 1))
+    out32, _, bins32 = run_split(p, soa, 40)
+    assert np.all(np.isfinite(out32.pos)) and np.all(np.isfinite(bins32))
+    assert field_errors(out32, ref)["pos"] <= POS_TOL
+
+
+def test_points_at_every_wall(oracle):
+    """A block lifted off the floor and moved against the left wall, with a
+    downward and leftward velocity: the wall conditions of kernels.cuh:290-294
+    act on the nodes next to the floor and to the left and right walls."""
+    p = params_for(64, 48, 0.25, 1e-4, IndVelocity=0.0, IndDepth=0.0)
+    soa = make_block(p, 10 * 0.25, 6 * 0.25, ppc=4, seed=33, n_grains=4)
+    h = p.cellsize
+    half = soa.size // 2
+    # left half of the points against the left wall (base x = 1), the rest at the right wall
+    soa.pos[0, :half] += (1.6 * h) - soa.pos[0, :half].min()
+    soa.pos[0, half:] += (p.GridXTotal - 4.4) * h - soa.pos[0, half:].max()
+    soa.pos[1] += (1.6 * h) - soa.pos[1].min()
+    soa.vel[0, :half] = -2.0
+    soa.vel[0, half:] = 2.0
+    soa.vel[1] = -1.0
+    p.indenter_x = p.indenter_x_initial = -100.0   # far away
+    ref = soa.clone()
+    assert oracle.run(p, ref, 0, 30)[0] == 0
+    out, _, _, _ = run_gpu(p, soa, 30)
+    assert_close(field_errors(out, ref))
+    out32, _, _ = run_split(p, soa, 30)
+    assert field_errors(out32, ref)["pos"] <= POS_TOL
+
+
+def test_tiles_with_more_points_than_a_chunk(oracle):
+    """16 points per cell: a 32 x 8-cell tile holds up to 4,096 points, more
+    than one staged chunk (704 FP64 / 1,280 FP32), so the chunk loop runs."""
+    p = params_for(96, 48, 0.25, 5e-5)
+    soa = make_block(p, 40 * 0.25, 10 * 0.25, ppc=16, seed=34, n_grains=8)
+    assert soa.size == 40 * 10 * 16
+    ref = soa.clone()
+    assert oracle.run(p, ref, 0, 40)[0] == 0
+    out, _, _, _ = run_gpu(p, soa, 40)
+    assert_close(field_errors(out, ref))
+    out32, _, _ = run_split(p, soa, 40)
+    assert field_errors(out32, ref)["pos"] <= POS_TOL
+
+
+def test_full_size_instance_consistency():
+    """The 9.6 M-point bench instance, 20 steps: tiled FP64 against the
+    one-thread-per-item FP64 kernels (same arithmetic, other summation order)
+    and FP32 split against FP64."""
+    from icempm_multi_b200.workloads import LARGE, make_workload
+    p, soa = make_workload(LARGE, pinned=True)
+    res = {}
+    for name, prec, opts in (("tiled", PRECISION_FP64, {}), ("simple", PRECISION_FP64, {"tiled": 0}),
+                             ("fp32", PRECISION_FP32_SPLIT, {})):
+        out = soa.clone(pinned=True)
+        g = GPUImplementation(p, out, precision=prec)
+        for k, v in opts.items():
+            g.set_option(k, v)
+        g.update_constants()
+        g.transfer_ponts_to_device()
+        g.run_steps(0, 20, 0.0)
+        g.transfer_from_device()
+        g.close()
+        res[name] = out
+    e = field_errors(res["tiled"], res["simple"])
+    assert e["pos"] <= TOL["pos"] and e["vel"] <= TOL["vel"] and e["status"] == 0.0, e
+    e32 = field_errors(res["fp32"], res["tiled"])
+    assert e32["pos"] <= 1e-6, e32
