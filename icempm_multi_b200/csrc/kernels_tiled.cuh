@@ -269,17 +269,20 @@ __device__ __forceinline__ void point_contributions(double h, double fx, double 
                                                     double mvy, double s00, double s01, double s10, double s11,
                                                     Sink &&sink)
 {
+    // node (a, b) gets W m and W (m v + S d), d = ((a - fx) h, (b - fy) h),
+    // W = wx[a] wy[b]; S d is affine in (a, b): c0 + a S(:,0) h + b S(:,1) h
     double wx[3], wy[3];
     bspline_weights(fx, wx);
     bspline_weights(fy, wy);
+    const double s00h = s00 * h, s01h = s01 * h, s10h = s10 * h, s11h = s11 * h;
+    const double c0x = mvx - (s00h * fx + s01h * fy), c0y = mvy - (s10h * fx + s11h * fy);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const double d0 = ((double)a - fx) * h;
+        const double ax = c0x + (double)a * s00h, ay = c0y + (double)a * s10h;
 #pragma unroll
         for (int b = 0; b < 3; b++) {
             const double W = wx[a] * wy[b];
-            const double d1 = ((double)b - fy) * h;
-            sink(a, b, W * mass, W * (mvx + (s00 * d0 + s01 * d1)), W * (mvy + (s10 * d0 + s11 * d1)));
+            sink(a, b, W, W * mass, ax + (double)b * s01h, ay + (double)b * s11h);
         }
     }
 }
@@ -290,11 +293,11 @@ static __device__ __noinline__ void p2g_global(GridView g, unsigned *flags, int2
                                                double mvx, double mvy, double s00, double s01, double s10, double s11)
 {
     point_contributions(h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
-                        [&](int a, int b, double dm, double dpx, double dpy) {
+                        [&](int a, int b, double W, double dm, double tx, double ty) {
                             const long k = g.idx(bx + a, by + b);
                             atomicAdd(g.m + k, dm);
-                            atomicAdd(g.px + k, dpx);
-                            atomicAdd(g.py + k, dpy);
+                            atomicAdd(g.px + k, W * tx);
+                            atomicAdd(g.py + k, W * ty);
                         });
     const int t0x = (bx + halo) / TX, t1x = (bx + 2 + halo) / TX;
     const int t0y = by / TY, t1y = (by + 2) / TY;
@@ -315,7 +318,7 @@ struct PointState {
 };
 
 // G2P + return mapping of one point (simulation/kernels.cuh:305-407).
-// vsrc(bx, by, a, b, nvx, nvy) supplies node velocities.  Returns false (and
+// vsrc(bx, by, nv) supplies the 3 x 3 node velocities.  Returns false (and
 // records the reference's error code) if the stencil leaves the grid.
 template <typename VSrc>
 __device__ __forceinline__ bool g2p_update(const StepParams &P, const GrainConst *grain_tab, PointState &s,
@@ -328,26 +331,26 @@ __device__ __forceinline__ bool g2p_update(const StepParams &P, const GrainConst
     double wx[3], wy[3];
     bspline_weights(fx, wx);
     bspline_weights(fy, wy);
-    double vx = 0, vy = 0;
-    M2<double> B{0, 0, 0, 0};
-    const double s4 = 4. * P.hinv;
+    // v = sum W v_i, Bp = 4/h sum W v_i (i - f)^T (kernels.cuh:357-372), as
+    // per-column sums over b with wy, then over a with wx
+    double2 nv[9];
+    vsrc(bx, by, nv);
+    double cvx[3], cvy[3], cbx[3], cby[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const double d0 = (double)a - fx;
-#pragma unroll
-        for (int b = 0; b < 3; b++) {
-            const double d1 = (double)b - fy;
-            const double w = wx[a] * wy[b];
-            double nvx, nvy;
-            vsrc(bx, by, a, b, nvx, nvy);
-            vx = vx + w * nvx;
-            vy = vy + w * nvy;
-            const double sw = s4 * w;
-            const double snx = sw * nvx, sny = sw * nvy;
-            B.a00 = B.a00 + snx * d0; B.a01 = B.a01 + snx * d1;
-            B.a10 = B.a10 + sny * d0; B.a11 = B.a11 + sny * d1;
-        }
+        const double2 n0 = nv[a * 3], n1 = nv[a * 3 + 1], n2 = nv[a * 3 + 2];
+        cvx[a] = wy[0] * n0.x + wy[1] * n1.x + wy[2] * n2.x;
+        cvy[a] = wy[0] * n0.y + wy[1] * n1.y + wy[2] * n2.y;
+        cbx[a] = wy[1] * n1.x + 2.0 * (wy[2] * n2.x);
+        cby[a] = wy[1] * n1.y + 2.0 * (wy[2] * n2.y);
     }
+    const double vx = wx[0] * cvx[0] + wx[1] * cvx[1] + wx[2] * cvx[2];
+    const double vy = wx[0] * cvy[0] + wx[1] * cvy[1] + wx[2] * cvy[2];
+    const double sax = wx[1] * cvx[1] + 2.0 * (wx[2] * cvx[2]), say = wx[1] * cvy[1] + 2.0 * (wx[2] * cvy[2]);
+    const double sbx = wx[0] * cbx[0] + wx[1] * cbx[1] + wx[2] * cbx[2];
+    const double sby = wx[0] * cby[0] + wx[1] * cby[1] + wx[2] * cby[2];
+    const double s4 = 4. * P.hinv;
+    const M2<double> B{s4 * (sax - fx * vx), s4 * (sbx - fy * vx), s4 * (say - fx * vy), s4 * (sby - fy * vy)};
     s.x = s.x + vx * P.dt;
     s.y = s.y + vy * P.dt;
     const M2<double> Am{1.0 + P.dt * B.a00, P.dt * B.a01, P.dt * B.a10, 1.0 + P.dt * B.a11};
@@ -391,45 +394,44 @@ __device__ __forceinline__ void store_point(double *__restrict__ pts, long pitch
     if (record_pq) { pts[i + pitch * 1] = s.ptr; pts[i + pitch * 2] = s.qtr; }
 }
 
-// Shared buffer of P2G moments, one column per staged point, padded by one
-// slot every 16 points so that cell threads reading points ~4 apart hit
-// distinct banks.  After phase 2 the same buffer holds the cell partials.
-constexpr int NMOM = 10;                          // fx, fy, m, m*vx, m*vy, S00, S01, S10, S11, base
-constexpr int CAP_P = CAP + CAP / 16;
-constexpr size_t MOM_BYTES = sizeof(double) * NMOM * CAP_P;
-static_assert(27 * TT <= NMOM * CAP_P, "cell partials alias the moment buffer");
-__device__ __forceinline__ int mom_idx(int k, int j) { return k * CAP_P + j + (j >> 4); }
+// Shared buffer of P2G moments: five vectors of two doubles per staged point,
+//   (fx, fy), (m, m vx), (m vy, S00), (S01, S10), (S11, base)
+// with one padding column after every 4 points (cell threads read points about
+// 4 apart).  After the cell phase the same buffer holds the cell partials
+// (27 x TT doubles).
+constexpr int MOM_N = CAP + CAP / 4;
+constexpr size_t MOM_BYTES = sizeof(double2) * 5 * MOM_N;
+static_assert(27 * TT * sizeof(double) <= MOM_BYTES, "cell partials alias the moment buffer");
+__device__ __forceinline__ int mom_col(int j) { return j + (j >> 2); }
 constexpr size_t TILE_DYN_SMEM = MOM_BYTES;
 
 // P2G moments of a point (simulation/kernels.cuh:57-92) into column j.
 __device__ __forceinline__ void p2g_moments(const StepParams &P, const PointState &s, double *mom, int j,
                                             int *status)
 {
+    double2 *m = reinterpret_cast<double2 *>(mom);
+    const int c = mom_col(j);
     const bool liquid = (s.util & kLiquid) != 0;
     const double mass = liquid ? P.mass_water : P.mass_ice;
     const int bx = (int)(s.x * P.hinv - 0.5), by = (int)(s.y * P.hinv - 0.5);
     const int e = base_error(P, bx, by);
     if (e) {
         *status = e;
-        mom[mom_idx(9, j)] = __longlong_as_double((long long)BASE_NONE);
+        m[4 * MOM_N + c].y = __longlong_as_double((long long)BASE_NONE);
         return;
     }
     const M2<double> tau = liquid ? water_stress(s.Jp, P.kappa) : kirchhoff(s.F, P.mu, P.kappa);
-    mom[mom_idx(0, j)] = s.x * P.hinv - (double)bx;
-    mom[mom_idx(1, j)] = s.y * P.hinv - (double)by;
-    mom[mom_idx(2, j)] = mass;
-    mom[mom_idx(3, j)] = s.vx * mass;
-    mom[mom_idx(4, j)] = s.vy * mass;
-    mom[mom_idx(5, j)] = mass * s.B.a00 - P.dt_vol_Dpinv * tau.a00;
-    mom[mom_idx(6, j)] = mass * s.B.a01 - P.dt_vol_Dpinv * tau.a01;
-    mom[mom_idx(7, j)] = mass * s.B.a10 - P.dt_vol_Dpinv * tau.a10;
-    mom[mom_idx(8, j)] = mass * s.B.a11 - P.dt_vol_Dpinv * tau.a11;
-    mom[mom_idx(9, j)] = __longlong_as_double((long long)pack_base(bx, by));
+    m[c] = make_double2(s.x * P.hinv - (double)bx, s.y * P.hinv - (double)by);
+    m[MOM_N + c] = make_double2(mass, s.vx * mass);
+    m[2 * MOM_N + c] = make_double2(s.vy * mass, mass * s.B.a00 - P.dt_vol_Dpinv * tau.a00);
+    m[3 * MOM_N + c] = make_double2(mass * s.B.a01 - P.dt_vol_Dpinv * tau.a01, mass * s.B.a10 - P.dt_vol_Dpinv * tau.a10);
+    m[4 * MOM_N + c] = make_double2(mass * s.B.a11 - P.dt_vol_Dpinv * tau.a11,
+                                    __longlong_as_double((long long)pack_base(bx, by)));
 }
 
 __device__ __forceinline__ void mom_none(double *mom, int j)
 {
-    mom[mom_idx(9, j)] = __longlong_as_double((long long)BASE_NONE);
+    reinterpret_cast<double2 *>(mom)[4 * MOM_N + mom_col(j)].y = __longlong_as_double((long long)BASE_NONE);
 }
 
 // Phases 2 and 3 for one chunk of points [cs, ce) of tile (tx, ty): cell
@@ -453,32 +455,34 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
         const int bxc = X0 + tid / TY, byc = Y0 + tid % TY;
         const int r0 = max(s_cs[tid], cs) - cs, r1 = min(s_cs[tid + 1], ce) - cs;
         for (int j = r0; j < r1; j++) {
-            const int pb = (int)__double_as_longlong(mom[mom_idx(9, j)]);
+            const double2 *mv = reinterpret_cast<const double2 *>(mom);
+            const int c = mom_col(j);
+            const double2 q4 = mv[4 * MOM_N + c];
+            const int pb = (int)__double_as_longlong(q4.y);
             if (pb == BASE_NONE) continue;
             int bx, by;
             unpack_base(pb, bx, by);
-            const double fx = mom[mom_idx(0, j)], fy = mom[mom_idx(1, j)], mass = mom[mom_idx(2, j)];
-            const double mvx = mom[mom_idx(3, j)], mvy = mom[mom_idx(4, j)];
-            const double s00 = mom[mom_idx(5, j)], s01 = mom[mom_idx(6, j)];
-            const double s10 = mom[mom_idx(7, j)], s11 = mom[mom_idx(8, j)];
+            const double2 q0 = mv[c], q1 = mv[MOM_N + c], q2 = mv[2 * MOM_N + c], q3 = mv[3 * MOM_N + c];
+            const double fx = q0.x, fy = q0.y, mass = q1.x, mvx = q1.y, mvy = q2.x;
+            const double s00 = q2.y, s01 = q3.x, s10 = q3.y, s11 = q4.x;
             if (bx == bxc && by == byc) {
                 point_contributions(P.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
-                                    [&](int a, int b, double dm, double dpx, double dpy) {
+                                    [&](int a, int b, double W, double dm, double tx, double ty) {
                                         const int q = (a * 3 + b) * 3;
                                         acc[q] += dm;
-                                        acc[q + 1] += dpx;
-                                        acc[q + 2] += dpy;
+                                        acc[q + 1] += W * tx;
+                                        acc[q + 2] += W * ty;
                                     });
             } else {
                 moved++;
                 const int lx = bx - RX0, ly = by - RY0;
                 if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
                     point_contributions(P.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
-                                        [&](int a, int b, double dm, double dpx, double dpy) {
+                                        [&](int a, int b, double W, double dm, double tx, double ty) {
                                             const int k = (lx + a) * RY + (ly + b);
                                             atomicAdd(&s_odd[0][k], dm);
-                                            atomicAdd(&s_odd[1][k], dpx);
-                                            atomicAdd(&s_odd[2][k], dpy);
+                                            atomicAdd(&s_odd[1][k], W * tx);
+                                            atomicAdd(&s_odd[2][k], W * ty);
                                         });
                 } else {
                     p2g_global(A.g, A.flags, A.tlist, A.tlist_n, A.G.ntx, P.halo, P.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01, s10,
@@ -542,11 +546,12 @@ __device__ __forceinline__ void mark_node_tiles(const TileArgs &A, int tx, int t
 template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
 static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
 {
-    __shared__ double s_v[2][RN];      // staged node velocities (G2P)
+    __shared__ double2 s_v[RN];        // staged node velocities (G2P)
     __shared__ double s_odd[3][RN];    // contributions of points off their sorted cell
     __shared__ int s_cs[TT + 1];       // cell ranges of the tile
     __shared__ unsigned s_touch;
-    extern __shared__ double s_mom[];  // NMOM x CAP_P moments | 27 x TT cell partials
+    extern __shared__ double2 s_mom2[];   // moments | 27 x TT cell partials
+    double *const s_mom = reinterpret_cast<double *>(s_mom2);
     const StepParams &P = A.P;
     const int na = *A.n_active;
     const int tid = threadIdx.x;
@@ -567,22 +572,29 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
                     vx = A.g.vx[q];
                     vy = A.g.vy[q];
                 }
-                s_v[0][k] = vx;
-                s_v[1][k] = vy;
+                s_v[k] = make_double2(vx, vy);
             }
         }
         __syncthreads();
         const int ps = s_cs[0], pe = s_cs[TT];
-        auto vsrc = [&](int bx, int by, int a, int b, double &nvx, double &nvy) {
+        // the 3 x 3 node velocities of a stencil: from the staged region (one check
+        // per point), else from the grid
+        auto vsrc = [&](int bx, int by, double2 *nv) {
             const int lx = bx - RX0, ly = by - RY0;
             if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
-                const int k = (lx + a) * RY + (ly + b);
-                nvx = s_v[0][k];
-                nvy = s_v[1][k];
+                const double2 *r = s_v + lx * RY + ly;
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++) nv[a * 3 + b] = r[a * RY + b];
             } else {
-                const long k = A.g.idx(bx + a, by + b);
-                nvx = A.g.vx[k];
-                nvy = A.g.vy[k];
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++) {
+                        const long k = A.g.idx(bx + a, by + b);
+                        nv[a * 3 + b] = make_double2(A.g.vx[k], A.g.vy[k]);
+                    }
             }
         };
         unsigned touch = 0;
@@ -651,10 +663,10 @@ constexpr long PIPE_WAIT_LIMIT = 1L << 26;        // polls before a wait gives u
 
 struct PipeSmem {
     double line[NSTAGE][NLINE][LINE_CAP];        // staged point lines
-    double v[NSTAGE][2][RN];                     // staged node velocities
+    double2 v[NSTAGE][RN];                       // staged node velocities
     int cs[NSTAGE][TT + 1];                      // staged cell ranges
     int meta[NSTAGE][4];                         // tile, cs, ce, first aligned index
-    double mom[NMOM * CAP_P];                    // moments | cell partials
+    alignas(16) double mom[MOM_BYTES / sizeof(double)];   // moments | cell partials
     double odd[3][RN];
     unsigned long long full[NSTAGE], empty[NSTAGE];
     unsigned touch;
@@ -710,8 +722,7 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(TileArgs A
                         vx = A.g.vx[q];
                         vy = A.g.vy[q];
                     }
-                    S.v[st][0][k] = vx;
-                    S.v[st][1][k] = vy;
+                    S.v[st][k] = make_double2(vx, vy);
                 }
                 for (int k = lane; k <= TT; k += 32) S.cs[st][k] = A.cell_start[(long)t * TT + k];
                 if (lane == 0) {
@@ -760,17 +771,25 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(TileArgs A
             csync();
             if (S.abort) { ok = false; break; }
             const int ce = S.meta[st][2], off = cs - S.meta[st][3];
-            const double(*sv)[RN] = S.v[st];
-            auto vsrc = [&](int bx, int by, int a, int b, double &nvx, double &nvy) {
+            const double2 *sv = S.v[st];
+            // the 3 x 3 node velocities of a stencil: from the staged region (one check
+            // per point), else from the grid
+            auto vsrc = [&](int bx, int by, double2 *nv) {
                 const int lx = bx - RX0, ly = by - RY0;
                 if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
-                    const int k = (lx + a) * RY + (ly + b);
-                    nvx = sv[0][k];
-                    nvy = sv[1][k];
+                    const double2 *r = sv + lx * RY + ly;
+    #pragma unroll
+                    for (int a = 0; a < 3; a++)
+    #pragma unroll
+                        for (int b = 0; b < 3; b++) nv[a * 3 + b] = r[a * RY + b];
                 } else {
-                    const long k = A.g.idx(bx + a, by + b);
-                    nvx = A.g.vx[k];
-                    nvy = A.g.vy[k];
+    #pragma unroll
+                    for (int a = 0; a < 3; a++)
+    #pragma unroll
+                        for (int b = 0; b < 3; b++) {
+                            const long k = A.g.idx(bx + a, by + b);
+                            nv[a * 3 + b] = make_double2(A.g.vx[k], A.g.vy[k]);
+                        }
                 }
             };
             // phase 1: one thread per point, state from the staged lines
