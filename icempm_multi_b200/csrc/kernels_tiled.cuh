@@ -317,6 +317,17 @@ struct PointState {
     M2<double> F, B;
 };
 
+// The return mapping (simulation/kernels.cuh:540-545, 623-674) out of line:
+// only crushed points take it, and its registers stay out of the tile
+// kernel's main path.
+struct ReturnMapped { M2<double> F; double Jp; };
+static __device__ __noinline__ ReturnMapped return_map_out(const StepParams &P, M2<double> F, double Jp, double ptr,
+                                                           double qtr, double Je)
+{
+    return_map(P, F, Jp, ptr, qtr, Je);
+    return ReturnMapped{F, Jp};
+}
+
 // G2P + return mapping of one point (simulation/kernels.cuh:305-407).
 // vsrc(bx, by, nv) supplies the 3 x 3 node velocities.  Returns false (and
 // records the reference's error code) if the stencil leaves the grid.
@@ -369,7 +380,11 @@ __device__ __forceinline__ bool g2p_update(const StepParams &P, const GrainConst
             const GrainConst c{__ldg(&gc->pmin2), __ldg(&gc->k), __ldg(&gc->msq)};
             if (failure_surface_crushed_tab(P, c, s.ptr, s.qtr)) s.util |= kCrushed;
         }
-        if (s.util & kCrushed) return_map(P, s.F, s.Jp, s.ptr, s.qtr, Je);
+        if (s.util & kCrushed) {
+            const ReturnMapped r = return_map_out(P, s.F, s.Jp, s.ptr, s.qtr, Je);
+            s.F = r.F;
+            s.Jp = r.Jp;
+        }
     }
     s.vx = vx;
     s.vy = vy;
@@ -492,9 +507,15 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
         }
     }
     sync();   // all moments read: the buffer becomes the cell partials
+    // partials per (node offset, cell): (m, px) as a vector, then py
+    double2 *pmx = reinterpret_cast<double2 *>(mom);
+    double *ppy = mom + 2 * 9 * TT;
     if (tid < TT) {
 #pragma unroll
-        for (int q = 0; q < 27; q++) mom[q * TT + tid] = acc[q];
+        for (int q = 0; q < 9; q++) {
+            pmx[q * TT + tid] = make_double2(acc[3 * q], acc[3 * q + 1]);
+            ppy[q * TT + tid] = acc[3 * q + 2];
+        }
     }
     sync();
     for (int k = tid; k < RN; k += NT) {
@@ -509,10 +530,11 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
             for (int b = 0; b < 3; b++) {
                 const int cy = ny - b;
                 if (cy < 0 || cy >= TY) continue;
-                const int c = cx * TY + cy, q = (a * 3 + b) * 3;
-                m += mom[q * TT + c];
-                px += mom[(q + 1) * TT + c];
-                py += mom[(q + 2) * TT + c];
+                const int c = cx * TY + cy, q = a * 3 + b;
+                const double2 v = pmx[q * TT + c];
+                m += v.x;
+                px += v.y;
+                py += ppy[q * TT + c];
             }
         }
         m += s_odd[0][k]; px += s_odd[1][k]; py += s_odd[2][k];
@@ -544,7 +566,7 @@ __device__ __forceinline__ void mark_node_tiles(const TileArgs &A, int tx, int t
 // only) and the last (<true, false, true>: G2P only, writes vel and Bp), and
 // by the per-phase calls.
 template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
-static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(TileArgs A)
+static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_constant__ TileArgs A)
 {
     __shared__ double2 s_v[RN];        // staged node velocities (G2P)
     __shared__ double s_odd[3][RN];    // contributions of points off their sorted cell
@@ -674,7 +696,7 @@ struct PipeSmem {
 };
 constexpr size_t PIPE_SMEM = sizeof(PipeSmem) + 128;
 
-static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(TileArgs A)
+static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __grid_constant__ TileArgs A)
 {
     extern __shared__ unsigned char s_raw[];
     PipeSmem &S = *reinterpret_cast<PipeSmem *>((reinterpret_cast<uintptr_t>(s_raw) + 127) & ~uintptr_t(127));
