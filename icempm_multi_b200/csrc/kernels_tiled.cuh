@@ -846,12 +846,14 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __gr
     if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
 }
 
+constexpr int UPD_TILES64 = 2;
+
 // Grid update of the nodes of the listed tiles (simulation/kernels.cuh:164-301):
 // each group of TT threads takes one TX x TY node tile (one thread per node, the
 // TY nodes of a tile column contiguous in memory), computes the velocities, zeroes the
 // accumulators for the next step and clears the tile's mark; the last CTA
 // empties the list.
-static __global__ void __launch_bounds__(256) k_update_list(StepParams P, TileGeom G, GridView g, unsigned *flags,
+static __global__ void __launch_bounds__(256, 4) k_update_list(StepParams P, TileGeom G, GridView g, unsigned *flags,
                                                             const int2 *__restrict__ tlist, unsigned *tlist_n,
                                                             double ind_x, double ind_y, double *acc)
 {
@@ -863,25 +865,44 @@ static __global__ void __launch_bounds__(256) k_update_list(StepParams P, TileGe
     constexpr int TPC = 256 / TT;   // node tiles per CTA pass
     static_assert(256 % TT == 0, "whole node tiles per 256-thread CTA");
     const int l = threadIdx.x % TT;
-    for (unsigned e = blockIdx.x * TPC + threadIdx.x / TT; e < n; e += gridDim.x * TPC) {
-        const int e2 = tlist[e].y;
-        const int tx = e2 & 0xffff, ty = e2 >> 16;
-        if (l == 0) flags[ty * G.ntx + tx] = 0u;
-        const int gx = tx * TX + l / TY - P.halo, gy = ty * TY + (l & (TY - 1));
-        if (gx >= P.gridx + P.halo || gy >= P.gridy) continue;   // past the grid edge
-        const long q = g.idx(gx, gy);
-        double vx = 0, vy = 0, fx, fy;
-        int bin;
-        if (node_update(P, gx, gy, g.m[q], g.px[q], g.py[q], ind_x, ind_y, vx, vy, bin, fx, fy) && bin >= 0) {
-            atomicAdd(&s_acc[2 * bin], fx);
-            atomicAdd(&s_acc[2 * bin + 1], fy);
-            any = true;
+    const unsigned stride = gridDim.x * TPC;
+    // UPD_TILES64 tiles per pass, their loads issued together
+    for (unsigned e0 = blockIdx.x * TPC + threadIdx.x / TT; e0 < n; e0 += stride * UPD_TILES64) {
+        long q[UPD_TILES64];
+        int gx[UPD_TILES64], gy[UPD_TILES64];
+        double m[UPD_TILES64], px[UPD_TILES64], py[UPD_TILES64];
+#pragma unroll
+        for (int u = 0; u < UPD_TILES64; u++) {
+            const unsigned e = e0 + u * stride;
+            q[u] = -1;
+            if (e >= n) continue;
+            const int e2 = tlist[e].y;
+            const int tx = e2 & 0xffff, ty = e2 >> 16;
+            if (l == 0) flags[ty * G.ntx + tx] = 0u;
+            gx[u] = tx * TX + l / TY - P.halo;
+            gy[u] = ty * TY + (l & (TY - 1));
+            if (gx[u] >= P.gridx + P.halo || gy[u] >= P.gridy) continue;   // past the grid edge
+            q[u] = g.idx(gx[u], gy[u]);
+            m[u] = g.m[q[u]];
+            px[u] = g.px[q[u]];
+            py[u] = g.py[q[u]];
         }
-        g.vx[q] = vx;
-        g.vy[q] = vy;
-        g.m[q] = 0.0;
-        g.px[q] = 0.0;
-        g.py[q] = 0.0;
+#pragma unroll
+        for (int u = 0; u < UPD_TILES64; u++) {
+            if (q[u] < 0) continue;
+            double vx = 0, vy = 0, fx, fy;
+            int bin;
+            if (node_update(P, gx[u], gy[u], m[u], px[u], py[u], ind_x, ind_y, vx, vy, bin, fx, fy) && bin >= 0) {
+                atomicAdd(&s_acc[2 * bin], fx);
+                atomicAdd(&s_acc[2 * bin + 1], fy);
+                any = true;
+            }
+            g.vx[q[u]] = vx;
+            g.vy[q[u]] = vy;
+            g.m[q[u]] = 0.0;
+            g.px[q[u]] = 0.0;
+            g.py[q[u]] = 0.0;
+        }
     }
     if (__syncthreads_or(any))
         for (int k = threadIdx.x; k < 2 * P.nsub; k += blockDim.x)
