@@ -88,6 +88,7 @@ EXPORTED = [
     "icy_batch_create", "icy_batch_destroy", "icy_batch_add", "icy_batch_remove", "icy_batch_step",
     "icy_batch_download", "icy_batch_synchronize", "icy_batch_set_option", "icy_batch_info",
     "icy_batch_device_bytes", "icy_mpm_device_bytes", "icy_scene_place", "icy_host_alloc", "icy_host_free",
+    "icy_batch_set_clock",
 ]
 
 _lib = None
@@ -145,6 +146,7 @@ def lib():
         "icy_batch_step": (C.c_int, [vp, C.c_int]),
         "icy_batch_download": (C.c_int, [vp, C.c_int, vp, C.c_uint, up, vp, dp, C.POINTER(C.c_int64)]),
         "icy_batch_synchronize": (C.c_int, [vp]),
+        "icy_batch_set_clock": (C.c_int, [vp, C.c_int, C.c_double, C.c_int64]),
         "icy_batch_set_option": (C.c_int, [vp, C.c_char_p, C.c_double]),
         "icy_batch_info": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                      C.POINTER(vp)]),

@@ -60,6 +60,10 @@ class Batch:
         check(rc, "icy_batch_download")
         return t.value, st.value, bins
 
+    def set_clock(self, slot, sim_time, step):
+        """Resume a member at (sim_time, step): its clock and indenter position."""
+        check(lib().icy_batch_set_clock(self._b, int(slot), float(sim_time), int(step)), "icy_batch_set_clock")
+
     def set_option(self, name, value):
         check(lib().icy_batch_set_option(self._b, name.encode(), float(value)), "icy_batch_set_option")
 

@@ -327,6 +327,21 @@ int icy_batch_step(icy_batch *b, int nsteps)
     return ICY_OK;
 }
 
+int icy_batch_set_clock(icy_batch *b, int slot, double sim_time, int64_t step)
+{
+    if (!b || slot < 0 || slot >= b->nslots || !b->members[slot] || step < 0) return ICY_ERR_INVALID_ARGUMENT;
+    CKB(cudaSetDevice(b->device));
+    BatchClock c;
+    CKB(cudaMemcpyAsync(&c, b->d_clk + slot, sizeof(c), cudaMemcpyDeviceToHost, b->stream));
+    CKB(cudaStreamSynchronize(b->stream));
+    c.t = sim_time;
+    c.step = step;
+    c.ind_x = c.x0 + c.t * c.v;   // recomputed on the device before every step
+    CKB(cudaMemcpyAsync(b->d_clk + slot, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
+    CKB(cudaStreamSynchronize(b->stream));
+    return ICY_OK;
+}
+
 int icy_batch_download(icy_batch *b, int slot, double *hssoa, unsigned capacity, unsigned *size, double *bins,
                        double *sim_time, int64_t *step)
 {

@@ -298,6 +298,7 @@ icy::Model::Model()
     prms.Reset();
     gpu.model = this;
     SetForceLog("logs/indenter_force.csv");
+    SetTimingsLog("logs/timings.csv");
 }
 
 icy::Model::~Model() = default;
@@ -310,6 +311,47 @@ void icy::Model::SetForceLog(const std::string &path)
     if (p.has_parent_path()) std::filesystem::create_directories(p.parent_path());
     log_indenter_force = std::make_unique<std::ofstream>(path, std::ios::trunc);
     if (!*log_indenter_force) throw std::runtime_error("cannot open " + path);
+}
+
+void icy::Model::SetTimingsLog(const std::string &path)
+{
+    log_timings.reset();
+    if (path.empty()) return;
+    std::filesystem::path p(path);
+    if (p.has_parent_path()) std::filesystem::create_directories(p.parent_path());
+    log_timings = std::make_unique<std::ofstream>(path, std::ios::trunc);
+    if (!*log_timings) throw std::runtime_error("cannot open " + path);
+}
+
+void icy::Model::write_timings(int cycles)
+{
+    // simulation/model.cpp:91-95 (one partition): frame, partition, points, free, disabled,
+    // points sent, max deviation, P2G+halo, accept halo, update, G2P, sent, accepted, total
+    const int mx = 32;
+    std::vector<char> names(48 * mx);
+    std::vector<double> ms(mx);
+    std::vector<int64_t> n(mx);
+    int count = 0;
+    icy::check(icy_mpm_profile_read(gpu.handle(), mx, names.data(), ms.data(), n.data(), &count), "timings");
+    double p2g = 0, upd = 0, g2p = 0, total = 0;
+    for (int k = 0; k < std::min(count, mx); k++) {
+        const std::string name(&names[48 * k]);
+        total += ms[k];
+        if (name == "k_tile_g2p2g" || name == "k_tile_p2g" || name == "k_p2g_simple" || name == "memset_grid")
+            p2g += ms[k];
+        else if (name == "k_update_nodes" || name == "k_update_simple") upd += ms[k];
+        else if (name == "k_tile_g2p" || name == "k_g2p_simple") g2p += ms[k];
+    }
+    const double coeff = 1000.0 / std::max(cycles, 1);
+    const HostSideSOA &s = gpu.hssoa;
+    int disabled = 0;
+    for (unsigned i = 0; i < s.size; i++) disabled += s.disabled(i) ? 1 : 0;
+    char line[256];
+    std::snprintf(line, sizeof(line), "%d, %2d,%8u,%8u,%7d,%3d,%3d,%5.1f,%5.1f,%5.1f,%5.1f,%5.1f,%5.1f,%6.1f",
+                  prms.AnimationFrameNumber(), 0, s.size, s.capacity - s.size, disabled, 0, 0, p2g * coeff, 0.0,
+                  upd * coeff, g2p * coeff, 0.0, 0.0, total * coeff);
+    *log_timings << line << '\n';
+    log_timings->flush();
 }
 
 void icy::Model::Reset()
@@ -334,6 +376,7 @@ bool icy::Model::Step()
     double simulation_time = prms.SimulationTime;
     int count_unupdated_steps = 0;
     gpu.reset_indenter_force_accumulator();
+    if (log_timings) icy::check(icy_mpm_profile(gpu.handle(), 1), "timings");
 
     if (per_phase_loop) {
         do {
@@ -363,6 +406,10 @@ bool icy::Model::Step()
         prms.SimulationTime = simulation_time;
         prms.SimulationStep += count_unupdated_steps;
         gpu.indenter_force /= (double)count_unupdated_steps;
+        if (log_timings) {
+            write_timings(count_unupdated_steps);
+            icy::check(icy_mpm_profile(gpu.handle(), 0), "timings");
+        }
         if (log_indenter_force) {
             *log_indenter_force << icy::format_double(prms.SimulationTime) << ','
                                 << icy::format_double(gpu.indenter_force.norm()) << ','

@@ -194,10 +194,15 @@ public:
 
     // "logs/indenter_force.csv" as the reference opens it (truncated); another path or "" (none)
     void SetForceLog(const std::string &path);
+    // "logs/timings.csv": per frame the columns of simulation/model.cpp:91-95 from per-kernel
+    // CUDA events (microseconds per sub-step; the fused G2P+P2G launch is under P2G)
+    void SetTimingsLog(const std::string &path);
 
 private:
     bool abortRequested = false;
     std::unique_ptr<std::ofstream> log_indenter_force;
+    std::unique_ptr<std::ofstream> log_timings;
+    void write_timings(int cycles);
 };
 
 class icy::SnapshotManager {

@@ -12,6 +12,11 @@ So requests that arrive while others run join the running batch as memory
 frees up, and their work overlaps on the device.  Completion latency is
 measured from arrival to the end of the result download.
 
+A request can be cancelled (dropped from the queue or the batch) or evicted:
+its state, simulation time, step index and force bins are downloaded, its
+device memory is freed and it goes back to the head of the queue, to resume
+where it stopped when memory allows.
+
 This is host-side scheduling over the icy_batch_* C-ABI; the reference has
 no counterpart (it runs one scenario per process).
 """
@@ -40,6 +45,11 @@ class Request:
     result: HostSideSOA = None
     sim_time: float = None
     bins: np.ndarray = None
+    cancelled: bool = False
+    evictions: int = 0
+    resume_time: float = 0.0     # simulation time / step index to resume from after an eviction
+    resume_step: int = 0
+    bins_before: np.ndarray = None
 
     @property
     def points(self):
@@ -57,6 +67,7 @@ class Server:
         self.running = {}
         self.queue = collections.deque()
         self.completed = []
+        self.cancelled = []
         self.rounds = 0
         self.peak_live = 0
         self.peak_bytes = 0.0
@@ -75,8 +86,11 @@ class Server:
                 break
             self.queue.popleft()
             r.slot = self.batch.add(r.params, r.soa)
+            if r.evictions:
+                self.batch.set_clock(r.slot, r.resume_time, r.resume_step)
             r.bytes = need
-            r.admitted = now
+            if r.admitted is None:
+                r.admitted = now
             self.used += need
             self.running[r.slot] = r
         self.peak_live = max(self.peak_live, len(self.running))
@@ -97,6 +111,8 @@ class Server:
             if r.steps_done >= r.steps:
                 out = self._out_buffer(r.soa.capacity)
                 r.sim_time, _, r.bins = self.batch.download(slot, out)
+                if r.bins_before is not None:
+                    r.bins = r.bins + r.bins_before
                 self.batch.remove(slot)
                 r.done = time.perf_counter() - t0
                 if self.keep_results:
@@ -105,8 +121,50 @@ class Server:
                 del self.running[slot]
                 self.completed.append(r)
 
-    def run(self, requests):
-        """Serve `requests` (arrival times relative to now); returns stats."""
+    def _running(self, rid):
+        for slot, r in self.running.items():
+            if r.rid == rid:
+                return slot, r
+        return None, None
+
+    def cancel(self, rid):
+        """Drop request rid, queued or running; returns whether it was found."""
+        for r in list(self.queue):
+            if r.rid == rid:
+                self.queue.remove(r)
+                r.cancelled = True
+                self.cancelled.append(r)
+                return True
+        slot, r = self._running(rid)
+        if r is None:
+            return False
+        self.batch.remove(slot)
+        self.used -= r.bytes
+        del self.running[slot]
+        r.cancelled = True
+        self.cancelled.append(r)
+        return True
+
+    def evict(self, rid):
+        """Move running request rid off the device (state kept on the host) and
+        put it at the head of the queue; returns whether it was running."""
+        slot, r = self._running(rid)
+        if r is None:
+            return False
+        state = HostSideSOA(r.soa.capacity)
+        r.resume_time, r.resume_step, bins = self.batch.download(slot, state)
+        r.bins_before = bins if r.bins_before is None else r.bins_before + bins
+        self.batch.remove(slot)
+        self.used -= r.bytes
+        del self.running[slot]
+        r.soa = state
+        r.evictions += 1
+        self.queue.appendleft(r)
+        return True
+
+    def run(self, requests, on_round=None):
+        """Serve `requests` (arrival times relative to now); returns stats.
+        on_round(server, round_index) is called after every round."""
         pending = sorted(requests, key=lambda r: r.arrival)
         pi = 0
         work = 0.0
@@ -128,10 +186,14 @@ class Server:
                 r.steps_done += self.round_steps
                 work += r.points * self.round_steps
             self._complete(t0)
+            if on_round is not None:
+                on_round(self, self.rounds)
         makespan = time.perf_counter() - t0
         lat = np.array([r.done - r.arrival for r in self.completed]) if self.completed else np.zeros(1)
         return {
             "requests": len(self.completed),
+            "cancelled": len(self.cancelled),
+            "evictions": sum(r.evictions for r in self.completed),
             "makespan_s": makespan,
             "particle_steps": work,
             "particle_steps_per_s": work / makespan if makespan > 0 else 0.0,

@@ -298,6 +298,10 @@ int icy_batch_step(icy_batch *b, int nsteps);
 int icy_batch_download(icy_batch *b, int slot, double *hssoa, unsigned capacity,
                        unsigned *size, double *bins, double *sim_time, int64_t *step);
 int icy_batch_synchronize(icy_batch *b);
+/* Set a member's simulation time and next step index (and its indenter
+   position x0 + t V), e.g. to resume a member evicted with
+   icy_batch_download at that time and step. */
+int icy_batch_set_clock(icy_batch *b, int slot, double sim_time, int64_t step);
 /* "resort_every" (steps between re-binning, 0 = never), "tile_ctas"
    (persistent CTAs of the tile kernel), "update_ctas" (CTAs of the grid
    update); the CTA counts take effect from the next step call (the captured

@@ -83,6 +83,13 @@ def test_cli_frames_force_log_and_state_match_oracle(oracle, tmp_path):
     assert prm.SimulationTime == t
     assert any(float(l.split(",")[1]) > 0 for l in lines)      # the indenter touched the ice
     assert_close(field_errors(out, ref))
+    # logs/timings.csv: one line per frame in the reference's column layout (model.cpp:91-95)
+    tl = (tmp_path / "logs" / "timings.csv").read_text().splitlines()
+    assert len(tl) == 3
+    for k, l in enumerate(tl):
+        f = [x.strip() for x in l.split(",")]
+        assert len(f) == 14 and int(f[0]) == k + 1 and int(f[2]) == soa.size
+        assert float(f[7]) > 0 and float(f[13]) >= float(f[7])
 
 
 def test_cli_per_phase_loop_matches_fused(tmp_path):

@@ -4,6 +4,7 @@ the budget bounds how many are resident, and every result is the same alone
 and in the mix (relative L2 position difference <= 1e-6; FP32 grid sums are
 accumulated in a different order in a different mix) and within the FP32
 target of the FP64 oracle."""
+import numpy as np
 import pytest
 
 from icempm_multi_b200.batch import device_bytes
@@ -72,3 +73,35 @@ def test_serving_budget_bounds_residency():
     assert stats["requests"] == 5
     assert stats["peak_live"] <= 2
     assert stats["peak_device_bytes"] <= 2.2 * one
+
+
+def test_serving_evict_resume_and_cancel():
+    """Host-side interventions in a running serve: request 0 is evicted after
+    the second round (state, time, step and force bins to the host, device
+    memory freed) and resumes; request 2 is cancelled.  The evicted request
+    ends where it would have ended alone."""
+    sc = scenes()[:3]
+    events = {}
+
+    def on_round(srv, k):
+        if k == 2:
+            events["evicted"] = srv.evict(0)
+        if k == 3:
+            events["cancelled"] = srv.cancel(2)
+
+    srv = Server(budget_bytes=8e9, round_steps=20)
+    stats = srv.run(requests(sc, [0.0, 0.0, 0.0], [100, 60, 200]), on_round=on_round)
+    srv.close()
+    assert events == {"evicted": True, "cancelled": True}
+    assert stats["requests"] == 2 and stats["cancelled"] == 1 and stats["evictions"] == 1
+    done = {r.rid: r for r in srv.completed}
+    assert set(done) == {0, 1} and srv.cancelled[0].rid == 2
+    r0 = done[0]
+    assert r0.evictions == 1 and r0.steps_done == 100
+    alone = Server(budget_bytes=8e9, round_steps=20)
+    alone.run(requests(sc, [0.0], [100]))
+    a = alone.completed[0]
+    alone.close()
+    assert r0.sim_time == a.sim_time
+    assert field_errors(r0.result, a.result)["pos"] <= MIX_TOL
+    assert np.allclose(r0.bins, a.bins, rtol=1e-5, atol=1e-6 * (np.abs(a.bins).max() + 1))
