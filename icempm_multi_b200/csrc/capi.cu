@@ -262,6 +262,8 @@ int icy_mpm_set_option(icy_mpm *h, const char *name, double value)
         h->resort_every = (int)value;
     } else if (k == "pipe") {
         h->pipe = value != 0;
+    } else if (k == "pipe_fault_test") {
+        h->pipe_fault_test = value != 0;
     } else if (k == "tiled") {
         h->tiled = value != 0;
         h->primed = false;

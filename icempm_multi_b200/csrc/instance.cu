@@ -345,6 +345,7 @@ static TileArgs tile_args(icy_mpm *h, bool record)
     A.moved = h->d_moved;
     A.grain_tab = h->d_grain;
     A.record_pq = record ? 1 : 0;
+    A.fault_test = h->pipe_fault_test ? 1 : 0;
     return A;
 }
 

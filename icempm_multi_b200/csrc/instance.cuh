@@ -56,6 +56,7 @@ struct icy_mpm {
     int resort_every = 64;      // re-bin interval in steps (0 = never)
     bool tiled = true;          // tiled kernels (false: one-thread-per-item kernels)
     bool pipe = false;          // fused step fed by the bulk-copy producer warp
+    bool pipe_fault_test = false;   // pipe kernel leaves its first stage unfilled (timeout test)
 
     double *d_acc = nullptr;      // indenter force bins, 2*n_indenter_subdivisions
     int *d_status = nullptr;      // device error code (reference codes 70..73, 5)

@@ -61,6 +61,7 @@ struct TileArgs {
     unsigned long long *moved;  // points whose base is not their sorted cell (re-binning hint)
     const GrainConst *grain_tab;  // failure-surface constants per grain slot
     int record_pq;
+    int fault_test;          // pipe kernel: leave the first stage unfilled (timeout test)
 };
 
 // Marks node tile (tx, ty) as written by P2G since the last grid update and
@@ -681,7 +682,8 @@ constexpr int NLINE = 8;                          // utility, Jp, x, y, Fe00..Fe
 constexpr int LINE_CAP = CAP + 2;                 // slack for 16-byte alignment of the copy
 static_assert((LINE_CAP * sizeof(double)) % 16 == 0, "16-byte aligned staged lines");
 static __device__ __constant__ const int kPipeLines[NLINE] = {0, 3, 4, 5, 8, 9, 10, 11};
-constexpr long PIPE_WAIT_LIMIT = 1L << 26;        // polls before a wait gives up
+constexpr uint64_t PIPE_WAIT_NS = 1000000000ull;  // a wait gives up after 1 s ...
+constexpr long PIPE_WAIT_POLLS = 1L << 26;         // ... or this many polls
 
 struct PipeSmem {
     double line[NSTAGE][NLINE][LINE_CAP];        // staged point lines
@@ -728,7 +730,7 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __gr
             for (int cs = ps; cs < pe; cs += CAP, c++) {
                 const int st = c % NSTAGE, use = c / NSTAGE;
                 if (use > 0 && !mbar_wait(reinterpret_cast<uint64_t *>(&S.empty[st]), (use - 1) & 1,
-                                          PIPE_WAIT_LIMIT)) {
+                                          PIPE_WAIT_NS, PIPE_WAIT_POLLS)) {
                     *A.status = ICY_TIMEOUT_CODE;
                     ok = false;
                     break;
@@ -754,7 +756,9 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __gr
                     S.meta[st][3] = a0;
                 }
                 __syncwarp();
-                if (lane == 0) {
+                // fault_test: the first stage is never filled, so every wait on it
+                // runs out (the timeout path, exercised by a test)
+                if (lane == 0 && !(A.fault_test && c == 0)) {
                     const uint32_t bytes = (uint32_t)((a1 - a0) * sizeof(double));
                     uint64_t *bar = reinterpret_cast<uint64_t *>(&S.full[st]);
                     mbar_arrive_expect_tx(bar, bytes * NLINE);
@@ -764,10 +768,12 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __gr
                 __syncwarp();
             }
         }
-        // on a timeout, wait (bounded) for this warp's copies still in flight
-        if (!ok && lane == 0)
+        // before leaving, wait (bounded) for this warp's last copies: consumers
+        // that gave up no longer wait for them, and none may be in flight when
+        // the CTA ends (chunks [0, c) were issued; each stage's last phase is final)
+        if (lane == 0)
             for (int k = max(0, c - NSTAGE); k < c; k++)
-                mbar_wait(reinterpret_cast<uint64_t *>(&S.full[k % NSTAGE]), (k / NSTAGE) & 1, PIPE_WAIT_LIMIT);
+                mbar_wait(reinterpret_cast<uint64_t *>(&S.full[k % NSTAGE]), (k / NSTAGE) & 1, PIPE_WAIT_NS, PIPE_WAIT_POLLS);
         return;
     }
 
@@ -786,7 +792,7 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __gr
         for (int cs = ps; cs < pe; cs += CAP, c++) {
             const int st = c % NSTAGE, use = c / NSTAGE;
             // the decision to give up is made CTA-uniform through S.abort
-            if (!mbar_wait(reinterpret_cast<uint64_t *>(&S.full[st]), use & 1, PIPE_WAIT_LIMIT)) {
+            if (!mbar_wait(reinterpret_cast<uint64_t *>(&S.full[st]), use & 1, PIPE_WAIT_NS, PIPE_WAIT_POLLS)) {
                 *A.status = ICY_TIMEOUT_CODE;
                 S.abort = 1;
             }

@@ -49,11 +49,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return done != 0;
 }
 
-// Bounded wait for the phase with the given parity; false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long limit)
+__device__ __forceinline__ uint64_t global_ns()
 {
-    for (long it = 0; it < limit; it++)
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the phase with the given parity: false once limit_ns of
+// the global timer have passed, or after max_polls polls, whichever comes
+// first (the poll count bounds the wait even if the timer did not advance).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns, long max_polls)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (long it = 0; it < max_polls; it++) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
     return false;
 }
 

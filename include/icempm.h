@@ -249,6 +249,9 @@ int icy_mpm_status(icy_mpm *h);
  *                   point / node, unsorted (the reference's kernel structure)
  *   "pipe"          1 = the fused step kernel is fed by a producer warp with
  *                   bulk copies into a shared-memory ring (default 0)
+ *   "pipe_fault_test" 1 = (tests of the timeout path) the producer leaves the
+ *                   ring's first stage unfilled: every wait on it gives up
+ *                   after 1 s and the next download reports ICY_ERR_TIMEOUT
  */
 int icy_mpm_set_option(icy_mpm *h, const char *name, double value);
 

@@ -209,3 +209,35 @@ def test_out_of_grid_reports_reference_code(oracle):
         g.transfer_from_device()
     assert e.value.code in ICY_ERR_OUT_OF_GRID
     g.close()
+
+
+def test_pipe_wait_timeout_is_reported_and_recoverable(oracle):
+    """The bounded waits of the bulk-copy pipeline: with the first ring stage
+    left unfilled on purpose, every wait on it gives up after 1 s, the kernel
+    returns and the download reports ICY_ERR_TIMEOUT; the context stays usable
+    and the same instance then steps normally."""
+    import time
+    from icempm_multi_b200._lib import ICY_ERR_TIMEOUT
+    p, soa = standard(seed=41)
+    g = GPUImplementation(p, soa.clone())
+    g.set_option("pipe", 1)
+    g.set_option("pipe_fault_test", 1)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    t0 = time.time()
+    g.run_steps(0, 2, 0.0)
+    with pytest.raises(IcyError) as e:
+        g.transfer_from_device()
+    assert e.value.code == ICY_ERR_TIMEOUT
+    assert time.time() - t0 < 30
+    # recover: clear the status, upload the state again, step without the fault
+    g.set_option("pipe_fault_test", 0)
+    g.update_constants()
+    g.hssoa.copy_from(soa)
+    g.transfer_ponts_to_device()
+    g.run_steps(0, 40, 0.0)
+    g.transfer_from_device()
+    ref = soa.clone()
+    assert oracle.run(p, ref, 0, 40)[0] == 0
+    assert_close(field_errors(g.hssoa, ref))
+    g.close()
