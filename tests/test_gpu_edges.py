@@ -4,7 +4,8 @@ an empty instance, stencil bases exactly on the truncation boundary of
 a node with mass (normalize of a zero vector, kernels.cuh:270), points next
 to every wall, tiles holding more points than one staged chunk, and the full
 9.6 M-point instance through size-independent checks (FP32 against FP64,
-tiled FP64 against the one-thread-per-item kernels)."""
+tiled FP64 against the one-thread-per-item kernels), and an allocation the
+device refuses."""
 import numpy as np
 import pytest
 
@@ -152,3 +153,21 @@ def test_full_size_instance_consistency():
     assert e["pos"] <= TOL["pos"] and e["vel"] <= TOL["vel"] and e["status"] == 0.0, e
     e32 = field_errors(res["fp32"], res["tiled"])
     assert e32["pos"] <= 1e-6, e32
+
+
+@pytest.mark.parametrize("precision", [PRECISION_FP64, PRECISION_FP32_SPLIT])
+def test_allocation_refused_is_reported(precision):
+    """An instance larger than the device (4e9 points) is refused with
+    ICY_ERR_OUT_OF_MEMORY; the next instance is created normally."""
+    from icempm_multi_b200._lib import ICY_ERR_OUT_OF_MEMORY, IcyError
+    p, soa = standard()
+    huge = HostSideSOA(1)
+    with pytest.raises(IcyError) as e:
+        GPUImplementation(p, huge, precision=precision, capacity=4_000_000_000)
+    assert e.value.code == ICY_ERR_OUT_OF_MEMORY
+    g = GPUImplementation(p, soa.clone(), precision=precision)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.run_steps(0, 5, 0.0)
+    g.transfer_from_device()
+    g.close()

@@ -105,3 +105,12 @@ def test_serving_evict_resume_and_cancel():
     assert r0.sim_time == a.sim_time
     assert field_errors(r0.result, a.result)["pos"] <= MIX_TOL
     assert np.allclose(r0.bins, a.bins, rtol=1e-5, atol=1e-6 * (np.abs(a.bins).max() + 1))
+
+
+def test_request_larger_than_the_budget_is_refused():
+    sc = scenes()[:1]
+    one = device_bytes(sc[0][0], sc[0][1].capacity)
+    srv = Server(budget_bytes=0.5 * one, round_steps=20)
+    with pytest.raises(RuntimeError, match="budget"):
+        srv.run(requests(sc, [0.0], [40]))
+    srv.close()
