@@ -32,7 +32,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-from icempm_multi_b200.workloads import LARGE, MEDIUM  # noqa: E402
+from icempm_multi_b200.workloads import LARGE, MEDIUM, SMALL  # noqa: E402
 from icempm_multi_b200.workloads import make_workload as _make, workload_params  # noqa: E402
 
 METRIC = "particle-steps/s"
@@ -384,8 +384,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="time only the headline path (no other precision, batched or served legs)")
-    ap.add_argument("--workload", default="large", choices=["large", "medium"],
-                    help="large: the 9.6 M-point headline instance; medium: the 4.8 M-point profiling case")
+    ap.add_argument("--workload", default="large", choices=["large", "medium", "small"],
+                    help="large: the 9.6 M-point headline instance; medium: the 4.8 M-point profiling case; "
+                         "small: the 65,536-point CPU-runnable case (L2-resident, launch bound)")
     ap.add_argument("--precision", default="fp32", choices=["fp64", "fp32"],
                     help="path of the headline value: fp32 split precision (default) or fp64")
     ap.add_argument("--opt", action="append", default=[],
@@ -393,7 +394,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global WORKLOAD
-    WORKLOAD = LARGE if args.workload == "large" else MEDIUM
+    WORKLOAD = {"large": LARGE, "medium": MEDIUM, "small": SMALL}[args.workload]
     if args.impl == "reference":
         return run_reference_arm(args)
 

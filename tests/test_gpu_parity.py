@@ -241,3 +241,30 @@ def test_pipe_wait_timeout_is_reported_and_recoverable(oracle):
     assert oracle.run(p, ref, 0, 40)[0] == 0
     assert_close(field_errors(g.hssoa, ref))
     g.close()
+
+
+@pytest.mark.parametrize("precision", [PRECISION_FP64, 1])
+def test_matches_reference_cuda_build_directly(oracle, precision):
+    """Parity check (a): this library against the reference's own kernels
+    built for sm_100a (oracle/_ref/libref_cuda.so, one partition) on the same
+    seeded input, 300 steps of a 9,216-point block under the indenter.  Both
+    sum node contributions with float atomics in different orders, so the
+    FP64 comparison uses the FP64 tolerances (TOL); FP32 split uses POS_TOL."""
+    from oracle.oracle import RefCuda
+    from test_gpu_split import POS_TOL, run_split
+    p, soa = standard(n_cells_x=96, n_cells_y=24, grid=(192, 64), seed=44)
+    ref = soa.clone()
+    err, _, _ = oracle.run(p, ref, 0, 300)
+    assert err == 0
+    h = p.cellsize     # the reference kernels do not stop at out-of-grid points: stay well inside
+    assert ref.pos[0].min() > 4 * h and ref.pos[0].max() < (p.GridXTotal - 4) * h
+    assert ref.pos[1].min() > 2 * h and ref.pos[1].max() < (p.GridY - 4) * h
+    rc_out = soa.clone()
+    rc, _, _, _ = RefCuda().run(p, rc_out, 0, 300)
+    assert rc == 0
+    if precision == PRECISION_FP64:
+        out, _, _, _ = run_gpu(p, soa, 300)
+        assert_close(field_errors(out, rc_out))
+    else:
+        out, _, _ = run_split(p, soa, 300)
+        assert field_errors(out, rc_out)["pos"] <= POS_TOL
