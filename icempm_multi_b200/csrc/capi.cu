@@ -89,7 +89,7 @@ int icy_mpm_create(const icy_sim_params *p, int device, unsigned capacity, int p
     h->precision = precision;
     int rc = icy_instance_allocate(h, capacity);
     if (rc != ICY_OK) {
-        icy_instance_free(h);
+        icy_instance_free(h, rc == ICY_ERR_OUT_OF_MEMORY);
         delete h;
         return rc;
     }

@@ -190,7 +190,7 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     return ICY_OK;
 }
 
-void icy_instance_free(icy_mpm *h)
+void icy_instance_free(icy_mpm *h, bool trim)
 {
     icy_prof_free(h);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
@@ -202,6 +202,12 @@ void icy_instance_free(icy_mpm *h)
     cudaStream_t fs = h->stream ? h->stream : h->own_stream;
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, fs);   // back to the pool, after the stream's work
+    if (trim && fs) {
+        // a refused allocation: the blocks this instance did get (up to the
+        // whole device) go back to the driver now, not to the pool's cache
+        cudaStreamSynchronize(fs);
+        if (cudaMemPool_t pool = instance_pool(h->device)) cudaMemPoolTrimTo(pool, 0);
+    }
     h->d_st = h->d_st_alt = nullptr;
     h->d_stage = nullptr;
     h->d_gridf = nullptr;

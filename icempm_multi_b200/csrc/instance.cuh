@@ -90,7 +90,7 @@ void icy_set_error(const char *where, cudaError_t e);
 void icy_set_error_msg(const std::string &m);
 
 int icy_instance_allocate(icy_mpm *h, unsigned capacity);
-void icy_instance_free(icy_mpm *h);
+void icy_instance_free(icy_mpm *h, bool trim = false);   // trim: give unused pool memory back
 int icy_instance_upload(icy_mpm *h, const double *hssoa, unsigned cap, unsigned size);
 int icy_instance_download(icy_mpm *h, double *hssoa, unsigned cap);
 int icy_phase_reset_grid(icy_mpm *h);

@@ -3,10 +3,11 @@
 Mirror of ``HostSideSOA`` (simulation/hssoa/host_side_soa.h:52-74): one buffer
 of 16 lines x ``capacity`` doubles, ``size`` points in use, line 0 holding the
 64-bit utility word bit-cast into a double.  The buffer can be page-locked
-(through torch, which is used here only as the pinned-memory allocator) so
+(icy_host_alloc, released by icy_host_free when the object is collected) so
 that uploads and downloads run at full PCIe/C2C speed.
 """
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -20,10 +21,13 @@ class HostSideSOA:
         self.size = 0
         self._keep = None
         if pinned:
-            import torch
-            t = torch.zeros((N_PTS_ARRAYS, self.capacity), dtype=torch.float64).pin_memory()
-            self._keep = t
-            self.buf = t.numpy()
+            n = N_PTS_ARRAYS * self.capacity
+            ptr = C.c_void_p()
+            check(lib().icy_host_alloc(n * 8, C.byref(ptr)), "icy_host_alloc")
+            mem = (C.c_double * n).from_address(ptr.value)
+            # freed when the last numpy view of the buffer is gone
+            self._keep = weakref.finalize(mem, lib().icy_host_free, ptr)
+            self.buf = np.ctypeslib.as_array(mem).reshape(N_PTS_ARRAYS, self.capacity)
         else:
             self.buf = np.zeros((N_PTS_ARRAYS, self.capacity), dtype=np.float64)
 

@@ -135,11 +135,11 @@ def test_full_size_instance_consistency():
     one-thread-per-item FP64 kernels (same arithmetic, other summation order)
     and FP32 split against FP64."""
     from icempm_multi_b200.workloads import LARGE, make_workload
-    p, soa = make_workload(LARGE, pinned=True)
+    p, soa = make_workload(LARGE)      # pageable buffers: 4 x 1.2 GB pinned would stay cached in this process
     res = {}
     for name, prec, opts in (("tiled", PRECISION_FP64, {}), ("simple", PRECISION_FP64, {"tiled": 0}),
                              ("fp32", PRECISION_FP32_SPLIT, {})):
-        out = soa.clone(pinned=True)
+        out = soa.clone()
         g = GPUImplementation(p, out, precision=prec)
         for k, v in opts.items():
             g.set_option(k, v)
@@ -158,13 +158,19 @@ def test_full_size_instance_consistency():
 @pytest.mark.parametrize("precision", [PRECISION_FP64, PRECISION_FP32_SPLIT])
 def test_allocation_refused_is_reported(precision):
     """An instance larger than the device (4e9 points) is refused with
-    ICY_ERR_OUT_OF_MEMORY; the next instance is created normally."""
+    ICY_ERR_OUT_OF_MEMORY, the device memory the pool took for it goes back to
+    the driver (a refused FP32 request left the pool holding all but 23 MB of
+    the device, so a second process could not create its context), and the
+    next instance is created normally."""
+    import torch
     from icempm_multi_b200._lib import ICY_ERR_OUT_OF_MEMORY, IcyError
     p, soa = standard()
     huge = HostSideSOA(1)
+    free0 = torch.cuda.mem_get_info()[0]
     with pytest.raises(IcyError) as e:
         GPUImplementation(p, huge, precision=precision, capacity=4_000_000_000)
     assert e.value.code == ICY_ERR_OUT_OF_MEMORY
+    assert torch.cuda.mem_get_info()[0] >= free0 - (1 << 30)
     g = GPUImplementation(p, soa.clone(), precision=precision)
     g.update_constants()
     g.transfer_ponts_to_device()
