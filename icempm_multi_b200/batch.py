@@ -85,9 +85,10 @@ def device_bytes(params, capacity, precision=PRECISION_FP32_SPLIT):
 
 def main():
     """python -m icempm_multi_b200.batch [--instances 256] [--steps 10] [--seed 7] [--repeat 2]
+                                        [--workload large|medium|small]
 
-    Builds the batched workload (icempm_multi_b200.workloads.batch_scenarios)
-    and advances it `repeat` times by `steps` sub-steps (the first call
+    Builds the batched workload (icempm_multi_b200.workloads.batch_scenarios,
+    or copies of one single-instance workload) and advances it `repeat` times by `steps` sub-steps (the first call
     captures the CUDA graph), printing the device time of each call."""
     import argparse
     import time
@@ -98,10 +99,17 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--workload", choices=["large", "medium", "small"],
+                    help="every member a copy of this single-instance workload instead of the floe scenarios")
     a = ap.parse_args()
     b = Batch(a.instances)
     n = 0
-    for w in batch_scenarios(a.instances, seed=a.seed):
+    if a.workload:
+        from . import workloads
+        members = [getattr(workloads, a.workload.upper())] * a.instances
+    else:
+        members = batch_scenarios(a.instances, seed=a.seed)
+    for w in members:
         p, soa = make_workload(w)
         b.add(p, soa)
         n += soa.size
