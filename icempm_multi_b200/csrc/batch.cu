@@ -58,6 +58,8 @@ static SplitArgs member_args(icy_batch *b, icy_mpm *h, int slot)
     g.py = h->d_gridf + 2 * h->n_nodes;
     g.vx = h->d_gridf + 3 * h->n_nodes;
     g.vy = h->d_gridf + 4 * h->n_nodes;
+    g.mp = reinterpret_cast<float4 *>(h->d_gridf);               // 16-byte aligned (pool blocks: 256 B)
+    g.v = reinterpret_cast<float2 *>(h->d_gridf + 4 * h->n_nodes);
     g.ny = h->prm.GridY;
     g.halo = h->prm.GridHaloSize;
     A.g = g;
@@ -183,7 +185,7 @@ int64_t icy_mpm_device_bytes(const icy_sim_params *p, unsigned capacity, int pre
     const long nkeys = ntiles * TT + 1;
     int64_t b = 0;
     if (precision == ICY_PRECISION_FP32_SPLIT)
-        b += 2 * (int64_t)S_NLINES * 4 * pitch + 16 * 8 * (int64_t)std::min(pitch, 1L << 20) + 5 * 4 * (int64_t)n_nodes;
+        b += 2 * (int64_t)S_NLINES * 4 * pitch + 16 * 8 * (int64_t)std::min(pitch, 1L << 20) + 6 * 4 * (int64_t)n_nodes;
     else
         b += 2 * 16 * 8 * (int64_t)pitch + 5 * 8 * (int64_t)n_nodes;
     b += 4 * 4 * (int64_t)pitch + 4 * (2 * nkeys + 1) + 4 * 2 * ntiles + 2 * 8 * p->n_indenter_subdivisions + 65536;

@@ -121,13 +121,13 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
             icy_set_error("cudaMalloc(particles)", e);
             return ICY_ERR_OUT_OF_MEMORY;
         }
-        if ((e = dalloc(h, &h->d_gridf, 5 * h->n_nodes)) != cudaSuccess) {
+        if ((e = dalloc(h, &h->d_gridf, 6 * h->n_nodes)) != cudaSuccess) {   // either layout of GridViewF
             icy_set_error("cudaMalloc(grid)", e);
             return ICY_ERR_OUT_OF_MEMORY;
         }
         CK(dalloc(h, reinterpret_cast<GrainConstF **>(&h->d_grainf), GRAIN_TAB));
         CK(cudaMemsetAsync(h->d_st, 0, sizeof(unsigned) * S_NLINES * h->pitch, h->stream));
-        CK(cudaMemsetAsync(h->d_gridf, 0, sizeof(float) * 5 * h->n_nodes, h->stream));
+        CK(cudaMemsetAsync(h->d_gridf, 0, sizeof(float) * 6 * h->n_nodes, h->stream));
     } else {
         if ((e = dalloc(h, &h->d_pts, 16 * h->pitch)) != cudaSuccess ||
             (e = dalloc(h, &h->d_pts_alt, 16 * h->pitch)) != cudaSuccess) {
@@ -363,6 +363,8 @@ static GridViewF grid_view_f32(icy_mpm *h)
     g.py = h->d_gridf + 2 * h->n_nodes;
     g.vx = h->d_gridf + 3 * h->n_nodes;
     g.vy = h->d_gridf + 4 * h->n_nodes;
+    g.mp = reinterpret_cast<float4 *>(h->d_gridf);               // 16-byte aligned (pool blocks: 256 B)
+    g.v = reinterpret_cast<float2 *>(h->d_gridf + 4 * h->n_nodes);
     g.ny = h->prm.GridY;
     g.halo = h->prm.GridHaloSize;
     return g;

@@ -261,9 +261,35 @@ __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const Split
     M.m2[c] = make_float2(mass * s.B.a11 - Q.dtvd * tau.a11, __int_as_float(pack_base(bx, by)));
 }
 
+// FP32 grid of n nodes in one allocation of 6 n floats, in one of two layouts.
+// Alone: five arrays m, px, py, vx, vy (scalar atomics; the bases are
+// constant-bank operands).  In a batch (AOS): per node (m, px, py, -) as a
+// float4 taken by one vector atomic, then a float2 velocity array: two bases
+// to look up per member and fewer live addresses (the batched kernel spills
+// less and runs 10 % faster; alone the scalar layout is 2.5 % faster).
 struct GridViewF {
-    float *m, *px, *py, *vx, *vy;
+    float *m, *px, *py, *vx, *vy;   // alone
+    float4 *mp;                     // in a batch (same memory)
+    float2 *v;
     int ny, halo;
+    // node (m, px, py) += (dm, dpx, dpy)
+    template <bool AOS>
+    __device__ __forceinline__ void add(long k, float dm, float dpx, float dpy) const
+    {
+        if constexpr (AOS) {
+            atomicAdd(mp + k, make_float4(dm, dpx, dpy, 0.f));
+        } else {
+            atomicAdd(m + k, dm);
+            atomicAdd(px + k, dpx);
+            atomicAdd(py + k, dpy);
+        }
+    }
+    template <bool AOS>
+    __device__ __forceinline__ float2 vel(long k) const
+    {
+        if constexpr (AOS) return v[k];
+        else return make_float2(vx[k], vy[k]);
+    }
     __device__ __forceinline__ long idx(int gx, int gy) const { return (long)(gx + halo) * ny + gy; }
 };
 
@@ -313,6 +339,7 @@ __device__ __forceinline__ void point_contributions_f32(float h, float fx, float
     }
 }
 
+template <bool AOS>
 static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags, int2 *tlist, unsigned *tlist_n,
                                                    int inst, int ntx, int halo, float h, int bx, int by, float fx,
                                                    float fy, float mass, float mvx, float mvy, float s00, float s01,
@@ -320,10 +347,7 @@ static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags,
 {
     point_contributions_f32(h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
                             [&](int a, int b, float W, float dm, float tx, float ty) {
-                                const long k = g.idx(bx + a, by + b);
-                                atomicAdd(g.m + k, dm);
-                                atomicAdd(g.px + k, W * tx);
-                                atomicAdd(g.py + k, W * ty);
+                                g.add<AOS>(g.idx(bx + a, by + b), dm, W * tx, W * ty);
                             });
     const int t0x = (bx + halo) / TX, t1x = (bx + 2 + halo) / TX;
     const int t0y = by / TY, t1y = (by + 2) / TY;
@@ -336,7 +360,7 @@ static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags,
 }
 
 // phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32
-template <int NT, typename Sync>
+template <int NT, bool AOS, typename Sync>
 __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int tid, int tx, int ty, int cs, int ce,
                                                         const int *s_cs, float *mom, float (*s_odd)[RN],
                                                         unsigned &touch, unsigned &moved, Sync &&sync)
@@ -381,7 +405,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                                                 atomicAdd(&s_odd[2][k], W * ty);
                                             });
                 } else {
-                    p2g_global_f32(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01,
+                    p2g_global_f32<AOS>(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01,
                                    s10, s11);
                 }
             }
@@ -416,10 +440,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
         s_odd[0][k] = 0.f; s_odd[1][k] = 0.f; s_odd[2][k] = 0.f;
         if (m != 0.f || px != 0.f || py != 0.f) {
             const int gx = RX0 + i, gy = RY0 + jj;
-            const long q = A.g.idx(gx, gy);
-            atomicAdd(A.g.m + q, m);
-            atomicAdd(A.g.px + q, px);
-            atomicAdd(A.g.py + q, py);
+            A.g.add<AOS>(A.g.idx(gx, gy), m, px, py);
             const int dx = (gx + P.halo) / TX - tx + 1, dy = gy / TY - ty + 1;
             touch |= 1u << (dy * 3 + dx);
         }
@@ -492,13 +513,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
         if (DO_G2P) {
             for (int k = tid; k < RN; k += blockDim.x) {
                 const int gx = RX0 + k / RY, gy = RY0 + k % RY;
-                float vx = 0.f, vy = 0.f;
-                if (node_in_grid(P, gx, gy)) {
-                    const long q = A.g.idx(gx, gy);
-                    vx = A.g.vx[q];
-                    vy = A.g.vy[q];
-                }
-                s_v[k] = make_float2(vx, vy);
+                s_v[k] = node_in_grid(P, gx, gy) ? A.g.vel<BATCH>(A.g.idx(gx, gy)) : make_float2(0.f, 0.f);
             }
         }
         __syncthreads();
@@ -517,10 +532,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
 #pragma unroll
                 for (int a = 0; a < 3; a++)
 #pragma unroll
-                    for (int b = 0; b < 3; b++) {
-                        const long k = A.g.idx(bx + a, by + b);
-                        nv[a * 3 + b] = make_float2(A.g.vx[k], A.g.vy[k]);
-                    }
+                    for (int b = 0; b < 3; b++) nv[a * 3 + b] = A.g.vel<BATCH>(A.g.idx(bx + a, by + b));
             }
         };
         unsigned touch = 0;
@@ -556,7 +568,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             if (DO_P2G && cs == ps && tid >= PF0 && tid < PF0 + S_JP + 2)
                 prefetch_next_item<BATCH>(A1, Aarr, work, ti + gridDim.x, na, tid - PF0);
             if (DO_P2G)
-                p2g_cells_and_flush_f32<TILE_THREADS_F32>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
+                p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
                                                       [] { __syncthreads(); });
         }
         if (DO_P2G) {
@@ -818,9 +830,16 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
             gy[u] = ty * TY + (l & (TY - 1));
             if (gx[u] >= A.P.gridx + A.P.halo || gy[u] >= A.P.gridy) continue;   // past the grid edge
             q[u] = A.g.idx(gx[u], gy[u]);
-            m[u] = A.g.m[q[u]];
-            px[u] = A.g.px[q[u]];
-            py[u] = A.g.py[q[u]];
+            if constexpr (BATCH) {
+                const float4 a = A.g.mp[q[u]];
+                m[u] = a.x;
+                px[u] = a.y;
+                py[u] = a.z;
+            } else {
+                m[u] = A.g.m[q[u]];
+                px[u] = A.g.px[q[u]];
+                py[u] = A.g.py[q[u]];
+            }
         }
 #pragma unroll
         for (int u = 0; u < UPD_TILES; u++) {
@@ -831,11 +850,16 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
             const int bin = node_velocity_f32(A.P, A.Q, gx[u], gy[u], m[u], px[u], py[u],
                                               BATCH ? clk[inst[u]].ind_x : ind_x, BATCH ? clk[inst[u]].y0 : ind_y,
                                               vx, vy, fx, fy);
-            A.g.vx[q[u]] = vx;
-            A.g.vy[q[u]] = vy;
-            A.g.m[q[u]] = 0.f;
-            A.g.px[q[u]] = 0.f;
-            A.g.py[q[u]] = 0.f;
+            if constexpr (BATCH) {
+                A.g.v[q[u]] = make_float2(vx, vy);
+                A.g.mp[q[u]] = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                A.g.vx[q[u]] = vx;
+                A.g.vy[q[u]] = vy;
+                A.g.m[q[u]] = 0.f;
+                A.g.px[q[u]] = 0.f;
+                A.g.py[q[u]] = 0.f;
+            }
             if (bin >= 0) {
                 if (BATCH) {
                     atomicAdd(A.acc + 2 * bin, fx);
