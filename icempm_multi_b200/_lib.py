@@ -85,7 +85,8 @@ EXPORTED = [
     "icy_mpm_receive_halos", "icy_mpm_update_nodes", "icy_mpm_g2p", "icy_mpm_receive_points", "icy_mpm_step",
     "icy_mpm_synchronize", "icy_mpm_status", "icy_mpm_kernel_launches", "icy_version", "icy_last_error",
     "icy_mpm_profile", "icy_mpm_profile_read", "icy_mpm_set_option", "icy_step_noalloc",
-    "icy_batch_create", "icy_batch_destroy", "icy_batch_add", "icy_batch_remove", "icy_batch_step",
+    "icy_batch_create", "icy_batch_destroy", "icy_batch_add", "icy_batch_add_async", "icy_batch_retire",
+    "icy_batch_collect", "icy_batch_wait_steps", "icy_batch_remove", "icy_batch_step",
     "icy_batch_download", "icy_batch_synchronize", "icy_batch_set_option", "icy_batch_info",
     "icy_batch_device_bytes", "icy_mpm_device_bytes", "icy_scene_place", "icy_host_alloc", "icy_host_free",
     "icy_batch_set_clock",
@@ -142,6 +143,11 @@ def lib():
         "icy_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(vp)]),
         "icy_batch_destroy": (C.c_int, [vp]),
         "icy_batch_add": (C.c_int, [vp, P, vp, C.c_uint, C.c_uint, C.POINTER(C.c_int)]),
+        "icy_batch_add_async": (C.c_int, [vp, P, vp, C.c_uint, C.c_uint, C.POINTER(C.c_int)]),
+        "icy_batch_retire": (C.c_int, [vp, C.c_int, vp, C.c_uint, vp]),
+        "icy_batch_collect": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_uint),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+        "icy_batch_wait_steps": (C.c_int, [vp, C.c_int]),
         "icy_batch_remove": (C.c_int, [vp, C.c_int]),
         "icy_batch_step": (C.c_int, [vp, C.c_int]),
         "icy_batch_download": (C.c_int, [vp, C.c_int, vp, C.c_uint, up, vp, dp, C.POINTER(C.c_int64)]),

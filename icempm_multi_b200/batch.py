@@ -17,6 +17,8 @@ class Batch:
         self._b = C.c_void_p()
         check(lib().icy_batch_create(device, int(max_instances), C.byref(self._b)), "icy_batch_create")
         self.params = {}
+        self._keep = {}         # host buffers of asynchronous admissions
+        self._retiring = {}     # slot -> (state buffer, bins) of retirements in flight
 
     def close(self):
         if self._b:
@@ -37,9 +39,53 @@ class Batch:
         self.params[slot.value] = params
         return slot.value
 
+    def add_async(self, params, soa):
+        """Admit a scenario without waiting for its upload (icy_batch_add_async):
+        soa must stay unchanged until a round queued after this call has run;
+        returns its slot."""
+        slot = C.c_int(-1)
+        check(lib().icy_batch_add_async(self._b, C.byref(params), soa.ptr, soa.capacity, soa.size, C.byref(slot)),
+              "icy_batch_add_async")
+        self.params[slot.value] = params
+        self._keep[slot.value] = soa
+        return slot.value
+
+    def retire(self, slot, soa=None, bins=True):
+        """Take a member out after the queued work; its state goes into soa (if
+        given) and its force bins into a new array while later rounds run.
+        Finish with collect(slot)."""
+        p = self.params[slot]
+        b = np.zeros(2 * p.n_indenter_subdivisions) if bins else None
+        check(lib().icy_batch_retire(self._b, int(slot), soa.ptr if soa is not None else None,
+                                     soa.capacity if soa is not None else 0,
+                                     b.ctypes.data_as(C.c_void_p) if b is not None else None), "icy_batch_retire")
+        self._keep.pop(slot, None)
+        self._retiring[slot] = (soa, b)
+
+    def collect(self, slot, wait=True):
+        """None while a retirement's copy runs (wait=False); else frees the slot
+        and returns (sim_time, next_step, bins)."""
+        done, n, t, st = C.c_int(0), C.c_uint(0), C.c_double(0), C.c_int64(0)
+        rc = lib().icy_batch_collect(self._b, int(slot), 1 if wait else 0, C.byref(done), C.byref(n), C.byref(t),
+                                     C.byref(st))
+        if not done.value:
+            check(rc, "icy_batch_collect")
+            return None
+        soa, b = self._retiring.pop(slot)
+        self.params.pop(slot, None)
+        if soa is not None:
+            soa.size = n.value
+        check(rc, "icy_batch_collect")
+        return t.value, st.value, b
+
+    def wait_steps(self, in_flight):
+        """Block until at most in_flight of the step() calls so far are unfinished."""
+        check(lib().icy_batch_wait_steps(self._b, int(in_flight)), "icy_batch_wait_steps")
+
     def remove(self, slot):
         check(lib().icy_batch_remove(self._b, int(slot)), "icy_batch_remove")
         self.params.pop(slot, None)
+        self._keep.pop(slot, None)
 
     def step(self, nsteps):
         check(lib().icy_batch_step(self._b, int(nsteps)), "icy_batch_step")

@@ -25,11 +25,25 @@ using namespace icy_dev;
         if (e_ != cudaSuccess) { icy_set_error(#call, e_); return ICY_ERR_CUDA; } \
     } while (0)
 
+// A retired member: its download is in flight on the side stream.
+struct Retiring {
+    icy_mpm *h = nullptr;
+    cudaEvent_t done = nullptr;
+    const double *hssoa = nullptr;   // destination of the download (NULL: none)
+    double *bins = nullptr;          // caller's force bins, filled at collection (NULL: none)
+    double *h_bins = nullptr;        // page-locked staging of the bins (a pageable target would block)
+    int nbins = 0, bins_cap = 0;
+};
+
 struct icy_batch {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;   // rounds, re-binning, work-list rebuilds
+    cudaStream_t side = nullptr;     // admissions (upload, binning) and retirements (download)
+    cudaEvent_t ev_join = nullptr, ev_round = nullptr;
     int nslots = 0;
     std::vector<icy_mpm *> members;
+    std::vector<Retiring> retiring;
+    BatchClock *h_clk = nullptr;     // page-locked: the clocks of retired members
     SplitArgs *d_args = nullptr;
     BatchClock *d_clk = nullptr;
     int *d_rec = nullptr;
@@ -40,6 +54,9 @@ struct icy_batch {
     int *d_woff = nullptr, *d_nwork = nullptr;
     bool dirty = true;
     int steps_since_bin = 0, resort_every = 256;
+    static constexpr int NEV = 8;
+    cudaEvent_t ev_steps[NEV] = {};   // ring: recorded after each icy_batch_step
+    int64_t steps_queued = 0;
     std::map<int, cudaGraphExec_t> graphs;
     std::map<int, int> graph_launches;   // kernels per replay
     int tile_grid = 0, update_grid = 0;
@@ -115,7 +132,8 @@ static int rebuild(icy_batch *b)
     k_batch_work_fill<<<dim3(8, b->nslots), 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_woff, b->d_work);
     CKB(cudaGetLastError());
     b->launches += 2;
-    CKB(cudaStreamSynchronize(b->stream));   // host vectors above go out of scope
+    // no synchronisation: a copy from pageable memory is staged before
+    // cudaMemcpyAsync returns, so `args` may go out of scope
     b->dirty = false;
     return ICY_OK;
 }
@@ -207,7 +225,17 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
     };
     cudaError_t e;
     if ((e = cudaSetDevice(device)) != cudaSuccess) return fail(e, "cudaSetDevice");
-    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    b->retiring.assign(max_instances, Retiring{});
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(e, "stream");
+    if ((e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&b->ev_round, cudaEventDisableTiming)) != cudaSuccess)
+        return fail(e, "event");
+    for (cudaEvent_t &ev : b->ev_steps)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    if ((e = cudaMallocHost(&b->h_clk, sizeof(BatchClock) * max_instances)) != cudaSuccess)
+        return fail(e, "cudaMallocHost(batch clocks)");
     if ((e = cudaMalloc(&b->d_args, sizeof(SplitArgs) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_clk, sizeof(BatchClock) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_rec, sizeof(int) * max_instances)) != cudaSuccess ||
@@ -239,9 +267,21 @@ int icy_batch_destroy(icy_batch *b)
     if (!b) return ICY_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->side) cudaStreamSynchronize(b->side);
     drop_graphs(b);
     for (icy_mpm *h : b->members)
-        if (h) icy_mpm_destroy(h);
+        if (h) {
+            h->stream = h->own_stream;
+            icy_mpm_destroy(h);
+        }
+    for (Retiring &r : b->retiring) {
+        if (r.h) {
+            r.h->stream = r.h->own_stream;
+            icy_mpm_destroy(r.h);
+        }
+        if (r.done) cudaEventDestroy(r.done);
+        if (r.h_bins) cudaFreeHost(r.h_bins);
+    }
     cudaFree(b->d_args);
     cudaFree(b->d_clk);
     cudaFree(b->d_rec);
@@ -250,26 +290,37 @@ int icy_batch_destroy(icy_batch *b)
     cudaFree(b->d_work);
     cudaFree(b->d_woff);
     cudaFree(b->d_nwork);
+    if (b->h_clk) cudaFreeHost(b->h_clk);
+    for (cudaEvent_t ev : b->ev_steps)
+        if (ev) cudaEventDestroy(ev);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->ev_round) cudaEventDestroy(b->ev_round);
+    if (b->side) cudaStreamDestroy(b->side);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return ICY_OK;
 }
 
-int icy_batch_add(icy_batch *b, const icy_sim_params *p, const double *hssoa, unsigned capacity, unsigned size,
-                  int *slot)
+// Admission on the side stream (upload, HSSOA conversion, binning), joined
+// into the batch stream by an event: the rounds already queued run on
+// meanwhile, the next one waits for it.
+static int add_member(icy_batch *b, const icy_sim_params *p, const double *hssoa, unsigned capacity, unsigned size,
+                      int *slot)
 {
     if (!b || !p || !hssoa || !slot || size > capacity || p->UpdateEveryNthStep <= 0) return ICY_ERR_INVALID_ARGUMENT;
     int s = -1;
     for (int k = 0; k < b->nslots; k++)
-        if (!b->members[k]) { s = k; break; }
+        if (!b->members[k] && !b->retiring[k].h) { s = k; break; }
     if (s < 0) return ICY_ERR_NO_SPACE;
     CKB(cudaSetDevice(b->device));
     icy_mpm *h = nullptr;
     int rc = icy_mpm_create(p, b->device, std::max(size, 1u), ICY_PRECISION_FP32_SPLIT, &h);
     if (rc) return rc;
-    h->stream = b->stream;
+    h->stream = b->side;
     if ((rc = icy_mpm_update_constants(h, p)) || (rc = icy_mpm_transfer_points_to_device(h, hssoa, capacity, size)) ||
         (rc = icy_mpm_reset_indenter_force_accumulator(h)) || (rc = icy_instance_bin(h))) {
+        cudaStreamSynchronize(b->side);
+        h->stream = h->own_stream;
         icy_mpm_destroy(h);
         return rc;
     }
@@ -283,11 +334,116 @@ int icy_batch_add(icy_batch *b, const icy_sim_params *p, const double *hssoa, un
     c.step = 0;
     c.every = p->UpdateEveryNthStep;
     c.live = 1;
+    CKB(cudaEventRecord(b->ev_join, b->side));
+    CKB(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
+    // the clock on the batch stream, after the queued rounds (whose clock
+    // kernels advance every live slot); from pageable memory, so staged
+    // before the call returns
     CKB(cudaMemcpyAsync(b->d_clk + s, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
-    CKB(cudaStreamSynchronize(b->stream));
+    h->stream = b->stream;   // the member's later work (re-binning, downloads) in the batch's order
     b->members[s] = h;
     b->dirty = true;
     *slot = s;
+    return ICY_OK;
+}
+
+int icy_batch_add(icy_batch *b, const icy_sim_params *p, const double *hssoa, unsigned capacity, unsigned size,
+                  int *slot)
+{
+    int rc = add_member(b, p, hssoa, capacity, size, slot);
+    if (rc) return rc;
+    CKB(cudaStreamSynchronize(b->side));
+    return ICY_OK;
+}
+
+int icy_batch_add_async(icy_batch *b, const icy_sim_params *p, const double *hssoa, unsigned capacity,
+                        unsigned size, int *slot)
+{
+    return add_member(b, p, hssoa, capacity, size, slot);
+}
+
+static __global__ void k_batch_leave(BatchClock *clk, int slot) { clk[slot].live = 0; }
+
+int icy_batch_retire(icy_batch *b, int slot, double *hssoa, unsigned capacity, double *bins)
+{
+    if (!b || slot < 0 || slot >= b->nslots || !b->members[slot]) return ICY_ERR_INVALID_ARGUMENT;
+    icy_mpm *h = b->members[slot];
+    if (hssoa && h->n > capacity) return ICY_ERR_CAPACITY;
+    CKB(cudaSetDevice(b->device));
+    Retiring &r = b->retiring[slot];
+    if (!r.done) CKB(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming));
+    // leaves the batch after the work already queued; its clock stays for the readback
+    k_batch_leave<<<1, 1, 0, b->stream>>>(b->d_clk, slot);
+    CKB(cudaGetLastError());
+    b->launches++;
+    CKB(cudaEventRecord(b->ev_round, b->stream));
+    CKB(cudaStreamWaitEvent(b->side, b->ev_round, 0));
+    h->stream = b->side;
+    if (hssoa)
+        if (int rc = icy_instance_download(h, hssoa, capacity)) return rc;
+    r.bins = bins;
+    r.nbins = 2 * h->prm.n_indenter_subdivisions;
+    if (bins) {
+        if (r.bins_cap < r.nbins) {
+            if (r.h_bins) CKB(cudaFreeHost(r.h_bins));
+            r.h_bins = nullptr;
+            r.bins_cap = 0;
+            CKB(cudaMallocHost(&r.h_bins, sizeof(double) * r.nbins));
+            r.bins_cap = r.nbins;
+        }
+        CKB(cudaMemcpyAsync(r.h_bins, h->d_acc, sizeof(double) * r.nbins, cudaMemcpyDeviceToHost, b->side));
+    }
+    CKB(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->side));
+    CKB(cudaMemcpyAsync(b->h_clk + slot, b->d_clk + slot, sizeof(BatchClock), cudaMemcpyDeviceToHost, b->side));
+    CKB(cudaEventRecord(r.done, b->side));
+    r.h = h;
+    r.hssoa = hssoa;
+    b->members[slot] = nullptr;
+    b->dirty = true;
+    return ICY_OK;
+}
+
+int icy_batch_collect(icy_batch *b, int slot, int wait, int *done, unsigned *size, double *sim_time, int64_t *step)
+{
+    if (!b || slot < 0 || slot >= b->nslots || !b->retiring[slot].h || !done) return ICY_ERR_INVALID_ARGUMENT;
+    CKB(cudaSetDevice(b->device));
+    Retiring &r = b->retiring[slot];
+    if (wait) {
+        CKB(cudaEventSynchronize(r.done));
+    } else {
+        const cudaError_t q = cudaEventQuery(r.done);
+        if (q == cudaErrorNotReady) {
+            *done = 0;
+            return ICY_OK;
+        }
+        CKB(q);
+    }
+    *done = 1;
+    icy_mpm *h = r.h;
+    const int code = *h->h_status;
+    if (r.bins) std::memcpy(r.bins, r.h_bins, sizeof(double) * r.nbins);
+    if (size) *size = h->n;
+    if (sim_time) *sim_time = b->h_clk[slot].t;
+    if (step) *step = b->h_clk[slot].step;
+    // active point count of the downloaded state (simulation/gpu_implementation5.cpp:399-433)
+    long active = 0;
+    if (r.hssoa)
+        for (unsigned i = 0; i < h->n; i++) {
+            long long u;
+            std::memcpy(&u, r.hssoa + i, 8);
+            if (!(u & ICY_STATUS_DISABLED)) active++;
+        }
+    const bool count_ok = !r.hssoa || active == h->prm.nPtsTotal;
+    h->stream = h->own_stream;
+    icy_mpm_destroy(h);
+    r.h = nullptr;
+    r.hssoa = nullptr;
+    r.bins = nullptr;
+    if (code) return code;
+    if (!count_ok) {
+        icy_set_error_msg("icy_batch_collect(): active point count mismatch");
+        return ICY_ERR_POINT_COUNT;
+    }
     return ICY_OK;
 }
 
@@ -296,6 +452,7 @@ int icy_batch_remove(icy_batch *b, int slot)
     if (!b || slot < 0 || slot >= b->nslots || !b->members[slot]) return ICY_ERR_INVALID_ARGUMENT;
     CKB(cudaSetDevice(b->device));
     CKB(cudaStreamSynchronize(b->stream));
+    CKB(cudaStreamSynchronize(b->side));
     BatchClock c{};
     CKB(cudaMemcpy(b->d_clk + slot, &c, sizeof(c), cudaMemcpyHostToDevice));
     icy_mpm *h = b->members[slot];
@@ -326,6 +483,23 @@ int icy_batch_step(icy_batch *b, int nsteps)
     b->steps_since_bin += nsteps;
     if (b->resort_every > 0 && b->steps_since_bin >= b->resort_every)
         if (int rc = rebin_members(b)) return rc;
+    CKB(cudaEventRecord(b->ev_steps[b->steps_queued % icy_batch::NEV], b->stream));
+    b->steps_queued++;
+    return ICY_OK;
+}
+
+int icy_batch_wait_steps(icy_batch *b, int in_flight)
+{
+    if (!b || in_flight < 0) return ICY_ERR_INVALID_ARGUMENT;
+    CKB(cudaSetDevice(b->device));
+    if (in_flight == 0) {
+        CKB(cudaStreamSynchronize(b->stream));
+        return ICY_OK;
+    }
+    // the newest call that must have finished (the ring holds the last NEV calls:
+    // a larger in_flight waits as for NEV - 1)
+    const int64_t k = b->steps_queued - 1 - std::min(in_flight, icy_batch::NEV - 1);
+    if (k >= 0) CKB(cudaEventSynchronize(b->ev_steps[k % icy_batch::NEV]));
     return ICY_OK;
 }
 
@@ -362,6 +536,7 @@ int icy_batch_synchronize(icy_batch *b)
     if (!b) return ICY_ERR_INVALID_ARGUMENT;
     CKB(cudaSetDevice(b->device));
     CKB(cudaStreamSynchronize(b->stream));
+    CKB(cudaStreamSynchronize(b->side));
     return ICY_OK;
 }
 

@@ -5,12 +5,16 @@ Requests arrive over time (e.g. a Poisson process); each asks for a scenario
 server keeps every admitted scenario's state resident on the device as a
 member of one Batch, advances all members together in rounds of
 `round_steps` sub-steps, and between rounds:
-  * downloads and releases the members that have done their steps,
+  * takes out the members that have done their steps (their results are
+    copied to the host on a side stream while the next round runs),
   * admits waiting requests, first come first served, while their device
-    memory fits the budget and a slot is free.
-So requests that arrive while others run join the running batch as memory
-frees up, and their work overlaps on the device.  Completion latency is
-measured from arrival to the end of the result download.
+    memory fits the budget and a slot is free (their upload and binning run
+    on the side stream too, and the next round waits for them).
+The host queues round k + 1 while round k runs and waits only for round k - 1,
+so the device does not idle between rounds.  Requests that arrive while
+others run join the running batch as memory frees up, and their work
+overlaps on the device.  Completion latency is measured from arrival to the
+moment the host holds the result.
 
 A request can be cancelled (dropped from the queue or the batch) or evicted:
 its state, simulation time, step index and force bins are downloaded, its
@@ -71,7 +75,7 @@ class Server:
         self.rounds = 0
         self.peak_live = 0
         self.peak_bytes = 0.0
-        self._scratch = {}      # page-locked download buffers by capacity, when results are not kept
+        self._scratch = {}      # free page-locked download buffers by capacity, when results are not kept
 
     def close(self):
         self.batch.close()
@@ -80,12 +84,12 @@ class Server:
         while self.queue and len(self.running) < self.max_instances:
             r = self.queue[0]
             need = device_bytes(r.params, r.soa.capacity)
+            if need > self.budget:   # larger than the whole budget: refuse instead of waiting forever
+                raise RuntimeError(f"request {r.rid} needs {need} bytes, budget {self.budget}")
             if self.used + need > self.budget:
-                if not self.running:   # larger than the whole budget: refuse instead of waiting forever
-                    raise RuntimeError(f"request {r.rid} needs {need} bytes, budget {self.budget}")
                 break
             self.queue.popleft()
-            r.slot = self.batch.add(r.params, r.soa)
+            r.slot = self.batch.add_async(r.params, r.soa)
             if r.evictions:
                 self.batch.set_clock(r.slot, r.resume_time, r.resume_step)
             r.bytes = need
@@ -97,29 +101,42 @@ class Server:
         self.peak_bytes = max(self.peak_bytes, self.used)
 
     def _out_buffer(self, capacity):
-        """Result buffer: a new one when results are kept, else a reused page-locked one."""
+        """Result buffer: a new one when results are kept, else a page-locked one
+        from the free list (returned by _release)."""
         if self.keep_results:
             return HostSideSOA(capacity)
         cap = 1 << max(int(capacity) - 1, 1).bit_length()
-        buf = self._scratch.get(cap)
-        if buf is None:
-            buf = self._scratch[cap] = HostSideSOA(cap, pinned=True)
-        return buf
+        free = self._scratch.setdefault(cap, [])
+        return free.pop() if free else HostSideSOA(cap, pinned=True)
 
-    def _complete(self, t0):
+    def _release(self, buf):
+        if not self.keep_results:
+            self._scratch.setdefault(buf.capacity, []).append(buf)
+
+    def _retire_finished(self):
+        """Members whose steps are all queued leave the batch; their results
+        are copied after the queued rounds.  Returns [(slot, request, buffer)]."""
+        out = []
         for slot, r in list(self.running.items()):
             if r.steps_done >= r.steps:
-                out = self._out_buffer(r.soa.capacity)
-                r.sim_time, _, r.bins = self.batch.download(slot, out)
-                if r.bins_before is not None:
-                    r.bins = r.bins + r.bins_before
-                self.batch.remove(slot)
-                r.done = time.perf_counter() - t0
-                if self.keep_results:
-                    r.result = out
-                self.used -= r.bytes
+                buf = self._out_buffer(r.soa.capacity)
+                self.batch.retire(slot, buf)
                 del self.running[slot]
-                self.completed.append(r)
+                out.append((slot, r, buf))
+        return out
+
+    def _collect(self, retired, t0):
+        for slot, r, buf in retired:
+            r.sim_time, _, r.bins = self.batch.collect(slot, wait=True)
+            if r.bins_before is not None:
+                r.bins = r.bins + r.bins_before
+            r.done = time.perf_counter() - t0
+            if self.keep_results:
+                r.result = buf
+            else:
+                self._release(buf)
+            self.used -= r.bytes
+            self.completed.append(r)
 
     def _running(self, rid):
         for slot, r in self.running.items():
@@ -164,30 +181,36 @@ class Server:
 
     def run(self, requests, on_round=None):
         """Serve `requests` (arrival times relative to now); returns stats.
-        on_round(server, round_index) is called after every round."""
+        on_round(server, round_index) is called after every round is queued."""
         pending = sorted(requests, key=lambda r: r.arrival)
         pi = 0
         work = 0.0
+        retired = []            # taken out after the previous round; results being copied
         t0 = time.perf_counter()
-        while pi < len(pending) or self.queue or self.running:
+        while pi < len(pending) or self.queue or self.running or retired:
             now = time.perf_counter() - t0
             while pi < len(pending) and pending[pi].arrival <= now:
                 self.queue.append(pending[pi])
                 pi += 1
             self._admit(now)
-            if not self.running:
-                if pi < len(pending):
-                    time.sleep(max(0.0, min(0.01, pending[pi].arrival - now)))
-                continue
-            self.batch.step(self.round_steps)
-            self.batch.synchronize()
-            self.rounds += 1
-            for r in self.running.values():
-                r.steps_done += self.round_steps
-                work += r.points * self.round_steps
-            self._complete(t0)
-            if on_round is not None:
+            stepped = False
+            if self.running:
+                self.batch.step(self.round_steps)
+                stepped = True
+                self.rounds += 1
+                for r in self.running.values():
+                    r.steps_done += self.round_steps
+                    work += r.points * self.round_steps
+            finished = self._retire_finished()
+            # at most this round in flight; the previous round's results are copied by now
+            self.batch.wait_steps(1)
+            self._collect(retired, t0)
+            retired = finished
+            if stepped and on_round is not None:
                 on_round(self, self.rounds)
+            if not self.running and not retired and not self.queue and pi < len(pending):
+                time.sleep(max(0.0, min(0.01, pending[pi].arrival - (time.perf_counter() - t0))))
+        self.batch.wait_steps(0)
         makespan = time.perf_counter() - t0
         lat = np.array([r.done - r.arrival for r in self.completed]) if self.completed else np.zeros(1)
         return {

@@ -292,6 +292,28 @@ int icy_batch_destroy(icy_batch *b);
    *slot receives its member index.  ICY_ERR_NO_SPACE if all slots are taken. */
 int icy_batch_add(icy_batch *b, const icy_sim_params *p, const double *hssoa,
                   unsigned capacity, unsigned size, int *slot);
+/* Admission without waiting: the upload, conversion and binning run on the
+   batch's side stream while the rounds already queued go on; the next round
+   waits for them.  The HSSOA buffer must stay valid and unchanged until
+   icy_batch_synchronize returns or a round queued after this call has
+   finished.  No counterpart in the reference (one scenario per process). */
+int icy_batch_add_async(icy_batch *b, const icy_sim_params *p, const double *hssoa,
+                        unsigned capacity, unsigned size, int *slot);
+/* Take a member out of the batch after the work already queued: its state
+   (HSSOA in upload order, when hssoa is not NULL), indenter bins (when bins
+   is not NULL), simulation time and step index are copied to the host on the
+   side stream while later rounds run without it (a page-locked hssoa lets
+   the call return at once; a pageable one makes it wait for the queued
+   rounds).  The slot stays reserved until icy_batch_collect reports the copy
+   done, and fills `bins` then; the buffers must stay valid until then.  No
+   counterpart in the reference. */
+int icy_batch_retire(icy_batch *b, int slot, double *hssoa, unsigned capacity, double *bins);
+/* Finish a retirement: *done = 0 if the copy is still running (wait = 0),
+   else *done = 1, the member's size, time and step, its device status code
+   as the return value (or ICY_ERR_POINT_COUNT as for
+   icy_mpm_transfer_from_device), and its slot and device memory are freed. */
+int icy_batch_collect(icy_batch *b, int slot, int wait, int *done, unsigned *size,
+                      double *sim_time, int64_t *step);
 /* Free a member's slot and device memory. */
 int icy_batch_remove(icy_batch *b, int slot);
 /* Advance every member by nsteps sub-steps of icy::Model::Step (asynchronous). */
@@ -301,6 +323,11 @@ int icy_batch_step(icy_batch *b, int nsteps);
 int icy_batch_download(icy_batch *b, int slot, double *hssoa, unsigned capacity,
                        unsigned *size, double *bins, double *sim_time, int64_t *step);
 int icy_batch_synchronize(icy_batch *b);
+/* Block until at most `in_flight` of the icy_batch_step calls made so far are
+   unfinished on the device (0: all finished), so that a host loop can queue
+   the next round while the current one runs.  The last 8 calls are tracked:
+   a larger in_flight waits as for 7. */
+int icy_batch_wait_steps(icy_batch *b, int in_flight);
 /* Set a member's simulation time and next step index (and its indenter
    position x0 + t V), e.g. to resume a member evicted with
    icy_batch_download at that time and step. */

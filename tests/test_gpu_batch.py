@@ -7,6 +7,7 @@ import pytest
 from icempm_multi_b200 import GPUImplementation
 from icempm_multi_b200._lib import PRECISION_FP32_SPLIT
 from icempm_multi_b200.batch import Batch
+from icempm_multi_b200.hssoa import HostSideSOA
 from scenarios import standard, stress
 from test_gpu_parity import field_errors
 from test_gpu_split import POS_TOL
@@ -92,4 +93,38 @@ def test_batch_members_keep_their_own_clock(oracle):
     od = sa.clone()
     _, step_d, _ = b.download(d, od)
     assert step_d == 10
+    b.close()
+
+
+def test_async_admission_and_retirement(oracle):
+    """icy_batch_add_async while a round is queued, icy_batch_retire /
+    icy_batch_collect behind the next one: the same clocks and states as the
+    synchronous calls, and the slot is reused only after its collection."""
+    (pa, sa), (pb, sb) = standard(seed=41), standard(n_cells_x=16, n_cells_y=6, grid=(64, 32), seed=42)
+    b = Batch(4)
+    a = b.add(pa, sa)
+    b.step(30)
+    c = b.add_async(pb, sb)          # joins behind the queued round
+    b.step(30)
+    oa = HostSideSOA(sa.capacity, pinned=True)
+    oc = HostSideSOA(sb.capacity, pinned=True)
+    b.retire(a, oa)
+    b.retire(c, oc)
+    d = b.add_async(pa, sa)          # a and c are still reserved
+    assert d not in (a, c)
+    b.step(10)
+    ta, step_a, bins_a = b.collect(a)
+    tc, step_c, _ = b.collect(c)
+    assert (step_a, step_c) == (60, 30)
+    assert ta == pytest.approx(60 * pa.InitialTimeStep) and tc == pytest.approx(30 * pb.InitialTimeStep)
+    assert oa.size == sa.size and np.all(np.isfinite(bins_a))
+    ra, rb = sa.clone(), sb.clone()
+    oracle.run(pa, ra, 0, 60)
+    oracle.run(pb, rb, 0, 30)
+    assert field_errors(oa, ra)["pos"] <= POS_TOL
+    assert field_errors(oc, rb)["pos"] <= POS_TOL
+    e = b.add(pb, sb)                # a freed slot is taken again
+    assert e in (a, c)
+    b.wait_steps(0)
+    assert b.info()["live"] == 2
     b.close()
