@@ -57,17 +57,34 @@ def test_split_roundtrip(built):
     assert np.allclose(out.vel[:, m], soa.vel[:, m], rtol=1e-7, atol=1e-7)
 
 
+def conservation_errors(p, a, b):
+    """max |x_a - x_b| / h over the points, total mass of a and b (the same set
+    of enabled points and materials: equal), and the total momentum
+    difference |sum m (v_a - v_b)| / sum m |v_b|."""
+    m = ~b.disabled()
+    mass_a = np.where(a.liquid()[~a.disabled()], p.WaterParticleMass, p.ParticleMass).sum()
+    mass = np.where(b.liquid()[m], p.WaterParticleMass, p.ParticleMass)
+    dmom = np.abs((mass * (a.vel[:, m] - b.vel[:, m])).sum(axis=1)).max()
+    scale = (mass * np.hypot(b.vel[0, m], b.vel[1, m])).sum()
+    return {"max_dx_h": float(np.abs(a.pos[:, m] - b.pos[:, m]).max() / p.cellsize),
+            "mass_a": float(mass_a), "mass_b": float(mass.sum()),
+            "momentum": float(dmom / scale if scale > 0 else dmom)}
+
+
 def test_split_1000_steps_within_target(oracle):
     p, soa = standard(n_cells_x=48, n_cells_y=12, grid=(128, 48), seed=21)
     ref = soa.clone()
     assert oracle.run(p, ref, 0, 1000)[0] == 0
     out, t, bins = run_split(p, soa, 1000, chunk=250)
     errs = field_errors(out, ref)
-    print("split 1000 steps", soa.size, errs)
+    cons = conservation_errors(p, out, ref)
+    print("split 1000 steps", soa.size, errs, cons)
     assert errs["pos"] <= POS_TOL
     for k, v in TOL32.items():
         assert errs[k] <= v, (k, errs)
     assert errs["status"] <= STATUS_MAX
+    assert cons["mass_a"] == cons["mass_b"]
+    assert cons["max_dx_h"] <= 1e-2 and cons["momentum"] <= 1e-3, cons
 
 
 def test_split_stress_branches(oracle):
@@ -100,3 +117,24 @@ def test_split_phase_api(oracle):
     ref = soa.clone()
     oracle.run(p, ref, 0, 60)
     assert field_errors(a, ref)["pos"] <= POS_TOL
+
+
+def test_split_small_workload_1000_steps(oracle):
+    """The 65,536-point CPU-runnable workload (grid 512 x 256 at h = 0.25 m,
+    64 m x 16 m block, dt 1e-4 s) for 1000 steps: FP32 split against the
+    FP64 oracle within the accuracy target, mass identical, momentum and the
+    largest position difference stated."""
+    from icempm_multi_b200.workloads import SMALL, make_workload
+    p, soa = make_workload(SMALL)
+    ref = soa.clone()
+    assert oracle.run(p, ref, 0, 1000)[0] == 0
+    out, _, _ = run_split(p, soa, 1000, chunk=250)
+    errs = field_errors(out, ref)
+    cons = conservation_errors(p, out, ref)
+    print("split small 1000 steps", soa.size, errs, cons)
+    assert errs["pos"] <= POS_TOL
+    for k, v in TOL32.items():
+        assert errs[k] <= v, (k, errs)
+    assert errs["status"] <= STATUS_MAX
+    assert cons["mass_a"] == cons["mass_b"]
+    assert cons["max_dx_h"] <= 1e-2 and cons["momentum"] <= 1e-3, cons
