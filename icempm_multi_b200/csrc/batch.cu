@@ -52,6 +52,7 @@ struct icy_batch {
     BatchItem *d_work = nullptr;
     long work_cap = 0;
     int *d_woff = nullptr, *d_nwork = nullptr;
+    int *d_claim = nullptr;          // work-item counters of the tile kernel
     bool dirty = true;
     int steps_since_bin = 0, resort_every = 256;
     static constexpr int NEV = 8;
@@ -155,6 +156,7 @@ static int rebin_members(icy_batch *b)
 static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
 {
     SplitArgs none{};
+    none.claim = b->d_claim;
     cudaGraph_t g = nullptr;
     int n = 0;
     CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -241,11 +243,13 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
         (e = cudaMalloc(&b->d_rec, sizeof(int) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_tlist_n, sizeof(unsigned) * 2)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_woff, sizeof(int) * max_instances)) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_nwork, sizeof(int))) != cudaSuccess)
+        (e = cudaMalloc(&b->d_nwork, sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_claim, sizeof(int) * 2)) != cudaSuccess)
         return fail(e, "cudaMalloc(batch)");
     cudaMemsetAsync(b->d_clk, 0, sizeof(BatchClock) * max_instances, b->stream);
     cudaMemsetAsync(b->d_rec, 0, sizeof(int) * max_instances, b->stream);
     cudaMemsetAsync(b->d_nwork, 0, sizeof(int), b->stream);
+    cudaMemsetAsync(b->d_claim, 0, sizeof(int) * 2, b->stream);
     cudaMemsetAsync(b->d_tlist_n, 0, sizeof(unsigned) * 2, b->stream);
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
@@ -290,6 +294,7 @@ int icy_batch_destroy(icy_batch *b)
     cudaFree(b->d_work);
     cudaFree(b->d_woff);
     cudaFree(b->d_nwork);
+    cudaFree(b->d_claim);
     if (b->h_clk) cudaFreeHost(b->h_clk);
     for (cudaEvent_t ev : b->ev_steps)
         if (ev) cudaEventDestroy(ev);

@@ -388,6 +388,7 @@ static SplitArgs split_args(icy_mpm *h, bool record)
     A.inst = 0;
     A.status = h->d_status;
     A.moved = h->d_moved;
+    A.claim = nullptr;   // batches only
     A.grain_tab = static_cast<const GrainConstF *>(h->d_grainf);
     A.record_pq = record ? 1 : 0;
     A.acc = h->d_acc;

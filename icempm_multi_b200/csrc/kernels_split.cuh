@@ -307,6 +307,7 @@ struct SplitArgs {
     int inst;           // this instance's slot in a batch (0 alone)
     int *status;
     unsigned long long *moved;
+    int *claim;         // batch: [0] next work item to hand out, [1] CTAs finished (zero between launches)
     const GrainConstF *grain_tab;
     int record_pq;
     double *acc;        // indenter force bins
@@ -493,13 +494,23 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     __shared__ float s_odd[3][RN];
     __shared__ int s_cs[TT + 1];
     __shared__ unsigned s_touch;
+    __shared__ int s_claim;
     extern __shared__ float4 s_momf4[];
     float *const s_momf = reinterpret_cast<float *>(s_momf4);
     const int na = BATCH ? *nwork : *A1.n_active;
     const int tid = threadIdx.x;
+    // Alone, CTA c takes the tiles c, c + gridDim.x, ... (equal tiles, and no
+    // claim to wait for: 5 % faster).  In a batch, where the items differ in
+    // size, they are handed out one at a time (A1.claim[0]), each CTA claiming
+    // its next item when it starts one, so that the CTAs finish together (4 %).
+    if (BATCH && tid == 0) s_claim = atomicAdd(A1.claim, 1);
     for (int k = tid; k < RN; k += blockDim.x) { s_odd[0][k] = 0.f; s_odd[1][k] = 0.f; s_odd[2][k] = 0.f; }
-    for (int ti = blockIdx.x; ti < na; ti += gridDim.x) {
+    __syncthreads();
+    int ti = BATCH ? s_claim : (int)blockIdx.x;
+    __syncthreads();   // everybody has read s_claim; later reads of it come before the item's last barrier
+    while (ti < na) {
         const BatchItem w = BATCH ? work[ti] : BatchItem{0, A1.active[ti]};
+        if (BATCH && tid == 0) s_claim = atomicAdd(A1.claim, 1);
         const SplitArgs &A = BATCH ? Aarr[w.inst] : A1;
         const StepParams &P = A.P;
         const bool record = BATCH ? rec[w.inst] != 0 : A.record_pq != 0;
@@ -517,6 +528,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             }
         }
         __syncthreads();
+        const int next = BATCH ? s_claim : ti + (int)gridDim.x;
         const int ps = s_cs[0], pe = s_cs[TT];
         // the 3 x 3 node velocities of a stencil: from the staged region (one check
         // per point), else from the grid
@@ -566,7 +578,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             // next item's loads
             constexpr int PF0 = TT < TILE_THREADS_F32 ? TT : TILE_THREADS_F32 - (S_JP + 2);
             if (DO_P2G && cs == ps && tid >= PF0 && tid < PF0 + S_JP + 2)
-                prefetch_next_item<BATCH>(A1, Aarr, work, ti + gridDim.x, na, tid - PF0);
+                prefetch_next_item<BATCH>(A1, Aarr, work, next, na, tid - PF0);
             if (DO_P2G)
                 p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
                                                       [] { __syncthreads(); });
@@ -583,6 +595,17 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
         }
         __syncthreads();
+        ti = next;
+    }
+    // the last CTA to finish resets the counters for the next launch: every
+    // CTA's last claim came before its count
+    if (BATCH && tid == 0) {
+        __threadfence();
+        if (atomicAdd(A1.claim + 1, 1) == (int)gridDim.x - 1) {
+            A1.claim[0] = 0;
+            A1.claim[1] = 0;
+            __threadfence();
+        }
     }
 }
 
