@@ -310,10 +310,12 @@ def measure_e2e(g, stream, soa, steps, frame, local, pg):
     return max(e0.elapsed_time(e1), wall * 1e3), downloads
 
 
-def measure_batch(n_instances=256, steps=100, seed=7):
+def measure_batch(n_instances=256, steps=256, seed=7):
     """The batched workload: n_instances floe scenarios (points log-uniform
     10k-500k, E 5e8-2e9 Pa, friction angle 45-70 deg, indenter 0.5-3 m/s,
-    CFL time steps) advanced together, one graph replay per call."""
+    CFL time steps) advanced together, one graph replay per call.  The timed
+    call is one re-binning interval (256 steps), so it holds exactly one
+    re-binning of all members."""
     import torch
     from icempm_multi_b200.batch import Batch
     from icempm_multi_b200.workloads import batch_scenarios, make_workload as mk
@@ -325,7 +327,7 @@ def measure_batch(n_instances=256, steps=100, seed=7):
         b.add(p, soa)
         npts += soa.size
     from icempm_multi_b200.autotune import tune_batch
-    # launch shape by timing this batch (120 steps; the re-binning interval stays 256)
+    # launch shape by timing this batch (6 candidates x 30 steps; the re-binning interval stays 256)
     tuned = tune_batch(b, steps=10, resort=False)
     b.step(steps)            # captures the graph for this step count, warms up
     b.synchronize()
@@ -342,6 +344,7 @@ def measure_batch(n_instances=256, steps=100, seed=7):
     return {"value": npts * steps / (ms / 1e3), "unit": METRIC, "instances": n_instances, "points": npts,
             "steps": steps, "ms_per_step": ms / steps, "gpu_launches": int(launches),
             "autotuned": tuned["settings"],
+            "timing": "one call of 256 steps (the re-binning interval): one re-binning of all members included",
             "workload": "floe scenarios: points log-uniform 10k-500k, grids 128x128..1024x512 (h=0.1 m), "
                         "E U(5e8,2e9), phi U(45,70), indenter U(0.5,3) m/s, CFL dt, FP32 split, CUDA graph"}
 
