@@ -385,7 +385,10 @@ int icy_batch_retire(icy_batch *b, int slot, double *hssoa, unsigned capacity, d
     CKB(cudaStreamWaitEvent(b->side, b->ev_round, 0));
     h->stream = b->side;
     if (hssoa)
-        if (int rc = icy_instance_download(h, hssoa, capacity)) return rc;
+        if (int rc = icy_instance_download(h, hssoa, capacity)) {
+            h->stream = b->stream;
+            return rc;
+        }
     r.bins = bins;
     r.nbins = 2 * h->prm.n_indenter_subdivisions;
     if (bins) {
