@@ -4,8 +4,9 @@ an empty instance, stencil bases exactly on the truncation boundary of
 a node with mass (normalize of a zero vector, kernels.cuh:270), points next
 to every wall, tiles holding more points than one staged chunk, and the full
 9.6 M-point instance through size-independent checks (FP32 against FP64,
-tiled FP64 against the one-thread-per-item kernels), and an allocation the
-device refuses."""
+tiled FP64 against the one-thread-per-item kernels), the largest grid
+dimensions the packed cell indices take, and an allocation the device
+refuses."""
 import numpy as np
 import pytest
 
@@ -177,3 +178,40 @@ def test_allocation_refused_is_reported(precision):
     g.run_steps(0, 5, 0.0)
     g.transfer_from_device()
     g.close()
+
+
+@pytest.mark.parametrize("precision", [PRECISION_FP64, PRECISION_FP32_SPLIT])
+def test_grid_beyond_the_packed_indices_is_refused(precision):
+    """Node columns (GridX + 2 halo) and rows are packed into 16 bits: 32,768
+    columns are refused with ICY_ERR_INVALID_ARGUMENT."""
+    from icempm_multi_b200._lib import ICY_ERR_INVALID_ARGUMENT, IcyError
+    p = params_for(32768 - 16, 16, 0.25, 1e-4)
+    with pytest.raises(IcyError) as e:
+        GPUImplementation(p, HostSideSOA(16), precision=precision)
+    assert e.value.code == ICY_ERR_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("shape", ["widest", "tallest"])
+def test_largest_grid_dimensions(oracle, shape):
+    """32,767 node columns (or rows), the largest the packed indices take, with
+    a block of points at the far end: cell indices near the 16-bit limit, the
+    far wall conditions, 20 steps against the oracle."""
+    h = 0.25
+    if shape == "widest":
+        p = params_for(32767 - 16, 16, h, 1e-4, IndVelocity=0.0, IndDepth=0.0)
+    else:
+        p = params_for(16, 32767, h, 1e-4, IndVelocity=0.0, IndDepth=0.0)
+    soa = make_block(p, 8 * h, 4 * h, ppc=4, seed=36, n_grains=4)
+    if shape == "widest":
+        soa.pos[0] += (p.GridXTotal - 4.5) * h - soa.pos[0].max()   # against the right wall
+        soa.vel[0] = 1.0
+    else:
+        soa.pos[1] += (p.GridY - 6.5) * h - soa.pos[1].max()        # at the top, falling
+        soa.vel[0] = 2.0 * (soa.pos[1] - soa.pos[1].mean())          # and sheared (Fe - I, Bp not zero)
+    p.indenter_x = p.indenter_x_initial = -100.0
+    ref = soa.clone()
+    assert oracle.run(p, ref, 0, 20)[0] == 0
+    out, _, _, _ = run_gpu(p, soa, 20)
+    assert_close(field_errors(out, ref))
+    out32, _, _ = run_split(p, soa, 20)
+    assert field_errors(out32, ref)["pos"] <= POS_TOL
