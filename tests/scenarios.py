@@ -61,3 +61,27 @@ def comparable_bits(soa):
     liq = soa.liquid()
     b[1:3, liq] = 0
     return b
+
+
+def randomized(seed):
+    """A seeded random floe-indentation scene: grid, cell size, block, points
+    per cell, material (E, nu, friction angle, cohesion, strengths, grain
+    variability), indenter (speed, depth, diameter) and time step drawn from
+    ranges that keep every point inside the grid for the steps the tests run."""
+    rng = np.random.default_rng(1000 + seed)
+    h = float(rng.choice([0.1, 0.2, 0.25, 0.5]))
+    gx, gy = int(rng.integers(48, 160)), int(rng.integers(32, 80))
+    bw, bh = int(rng.integers(8, max(9, gx // 2))), int(rng.integers(4, max(5, gy // 3)))
+    E = float(rng.uniform(5e8, 3e9))
+    rho = 980.0
+    c = np.sqrt(E / rho)
+    dt = float(0.3 * h / c)                     # CFL number 0.3
+    p = params_for(gx, gy, h, dt, YoungsModulus=E, PoissonsRatio=float(rng.uniform(0.2, 0.4)),
+                   DP_phi=float(rng.uniform(30, 70)), DP_threshold_p=float(rng.choice([0.0, 50.0, 500.0])),
+                   GrainVariability=float(rng.uniform(0.0, 0.8)), IndVelocity=float(rng.uniform(0.5, 8.0)),
+                   IndDepth=float(rng.uniform(0.1, 0.6)) * bh * h, IndDiameter=float(rng.uniform(0.5, 3.0)),
+                   IceCompressiveStrength=float(rng.uniform(2e6, 1e8)),
+                   IceTensileStrength=float(rng.uniform(2e5, 5e6)), IceShearStrength=float(rng.uniform(1e5, 3e6)))
+    soa = make_block(p, bw * h, bh * h, ppc=int(rng.choice([2, 4, 6, 9])), seed=seed,
+                     n_grains=int(rng.integers(0, 40)))
+    return p, soa

@@ -1,0 +1,48 @@
+"""Seeded randomized scenes (grid, cell size, block, points per cell, material,
+cohesion, strengths, grain variability, indenter, CFL time step; see
+scenarios.randomized) for 200 steps through the C-ABI against the FP64
+oracle: the tiled FP64 path and the one-thread-per-item FP64 kernels within
+the parity tolerances, the FP32 split path within its position target."""
+import pytest
+
+from scenarios import randomized
+from test_gpu_parity import TOL, assert_close, field_errors, run_gpu
+from test_gpu_split import POS_TOL, TOL32, run_split
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 200
+
+
+@pytest.fixture(scope="module")
+def oracle(built):
+    from oracle.oracle import Oracle
+    return Oracle()
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_randomized_scene_matches_oracle(oracle, seed):
+    p, soa = randomized(seed)
+    ref = soa.clone()
+    assert oracle.run(p, ref, 0, STEPS)[0] == 0
+    out, _, _, _ = run_gpu(p, soa, STEPS)
+    e64 = field_errors(out, ref)
+    simple = soa.clone()
+    from icempm_multi_b200 import GPUImplementation
+    g = GPUImplementation(p, simple)
+    g.set_option("tiled", 0)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.reset_indenter_force_accumulator()
+    g.run_steps(0, STEPS, 0.0)
+    g.transfer_from_device()
+    g.close()
+    es = field_errors(simple, ref)
+    out32, _, _ = run_split(p, soa, STEPS)
+    e32 = field_errors(out32, ref)
+    print("randomized", seed, soa.size, "fp64", e64, "simple", es, "fp32", e32)
+    assert_close(e64)
+    assert_close(es)
+    assert e32["pos"] <= POS_TOL
+    for k, v in TOL32.items():
+        assert e32[k] <= v, (k, e32)
