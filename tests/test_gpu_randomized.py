@@ -46,3 +46,32 @@ def test_randomized_scene_matches_oracle(oracle, seed):
     assert e32["pos"] <= POS_TOL
     for k, v in TOL32.items():
         assert e32[k] <= v, (k, e32)
+
+
+def test_randomized_scenes_as_one_batch(oracle):
+    """The twelve scenes as members of one batch (each with its own time step,
+    material and grid), half of them admitted while the first round is
+    queued, all retired together: every member against the oracle for its own
+    step count."""
+    from icempm_multi_b200.batch import Batch
+    from icempm_multi_b200.hssoa import HostSideSOA
+    scenes = [randomized(s) for s in range(12)]
+    b = Batch(16)
+    slots = [b.add(p, soa) for p, soa in scenes[:6]]
+    b.step(100)
+    slots += [b.add_async(p, soa) for p, soa in scenes[6:]]
+    b.step(100)
+    outs = []
+    for (p, soa), slot in zip(scenes, slots):
+        out = HostSideSOA(soa.capacity, pinned=True)
+        b.retire(slot, out)
+        outs.append(out)
+    for k, ((p, soa), slot, out) in enumerate(zip(scenes, slots, outs)):
+        _, step, _ = b.collect(slot)
+        n = 200 if k < 6 else 100
+        assert step == n
+        ref = soa.clone()
+        assert oracle.run(p, ref, 0, n)[0] == 0
+        e = field_errors(out, ref)
+        assert e["pos"] <= POS_TOL, (k, e)
+    b.close()
