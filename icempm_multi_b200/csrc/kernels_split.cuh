@@ -455,14 +455,6 @@ constexpr int TILE_THREADS_F32 = 256, TILE_CTAS_F32 = 3;
 // Work items of a batch: (instance, tile) pairs over all instances.
 struct BatchItem { int inst, tile; };
 
-// L2 prefetch of [p, p + bytes) rounded inward to 16-byte boundaries (never
-// past either end): cp.async.bulk.prefetch.L2 from this GPU's global memory.
-__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes)
-{
-    const uintptr_t a = ((uintptr_t)p + 15) & ~uintptr_t(15), e = ((uintptr_t)p + bytes) & ~uintptr_t(15);
-    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
-}
-
 // Starts moving the next work item's point lines (line `which` < S_JP + 1) or
 // cell ranges (which == S_JP + 1) into L2 while this CTA is in its cell phase.
 template <bool BATCH>

@@ -561,6 +561,31 @@ __device__ __forceinline__ void mark_node_tiles(const TileArgs &A, int tx, int t
     }
 }
 
+// L2 prefetch of [p, p + bytes) rounded inward to 16-byte boundaries (never
+// past either end): cp.async.bulk.prefetch.L2 from this GPU's global memory.
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes)
+{
+    const uintptr_t a = ((uintptr_t)p + 15) & ~uintptr_t(15), e = ((uintptr_t)p + bytes) & ~uintptr_t(15);
+    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
+// Starts moving the next tile's point lines that G2P reads (which < 8: utility,
+// Jp, x, y, Fe00..Fe11) or its cell ranges (which == 8) into L2 while this CTA
+// is in its cell phase.
+constexpr int TILE_PREFETCHES = 9;
+__device__ __forceinline__ void prefetch_next_tile(const TileArgs &A, int next, int na, int which)
+{
+    if (next >= na) return;
+    const int *cs = A.cell_start + (long)A.active[next] * TT;
+    if (which == 8) {
+        prefetch_l2(cs, (TT + 1) * sizeof(int));
+        return;
+    }
+    const int line = which < 1 ? 0 : which < 4 ? which + 2 : which + 4;   // 0, 3, 4, 5, 8, 9, 10, 11
+    const int ps = cs[0], pe = cs[TT];
+    if (pe > ps) prefetch_l2(A.pts + A.pitch * line + ps, (size_t)(pe - ps) * sizeof(double));
+}
+
 // ---------------------------------------------------------------- plain tile kernel
 // One persistent CTA loop over the non-empty tiles, points read straight from
 // global memory.  Used for the first step of a run (<false, true, false>: P2G
@@ -652,6 +677,9 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_co
                 if (DO_P2G) p2g_moments(P, s, s_mom, j, A.status);
             }
             __syncthreads();
+            // the last threads start the next tile's loads during the cell phase
+            if (DO_P2G && cs == ps && tid >= TILE_THREADS - TILE_PREFETCHES)
+                prefetch_next_tile(A, ti + gridDim.x, na, tid - (TILE_THREADS - TILE_PREFETCHES));
             if (DO_P2G)
                 p2g_cells_and_flush<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_mom, s_odd, touch, moved,
                                                   [] { __syncthreads(); });
