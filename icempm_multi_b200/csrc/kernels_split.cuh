@@ -571,6 +571,18 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             constexpr int PF0 = TT < TILE_THREADS_F32 ? TT : TILE_THREADS_F32 - (S_JP + 2);
             if (DO_P2G && cs == ps && tid >= PF0 && tid < PF0 + S_JP + 2)
                 prefetch_next_item<BATCH>(A1, Aarr, work, next, na, tid - PF0);
+            // and the first threads its staged node velocities (columns of vx and vy,
+            // or of the float2 velocities of a batch member)
+            if (DO_G2P && DO_P2G && cs == ps && tid < (BATCH ? 1 : 2) * RX && next < na) {
+                const BatchItem wn = BATCH ? work[next] : BatchItem{0, A1.active[next]};
+                const SplitArgs &An = BATCH ? Aarr[wn.inst] : A1;
+                const int nx0 = (wn.tile % An.G.ntx) * TX - An.P.halo - RM, ny0 = (wn.tile / An.G.ntx) * TY - RM;
+                if (BATCH)
+                    prefetch_region_column(An.g.v, An.P.gridx, An.P.gridy, An.P.halo, An.g.ny, nx0, ny0, tid);
+                else
+                    prefetch_region_column(tid < RX ? An.g.vx : An.g.vy, An.P.gridx, An.P.gridy, An.P.halo, An.g.ny,
+                                           nx0, ny0, tid % RX);
+            }
             if (DO_P2G)
                 p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
                                                       [] { __syncthreads(); });

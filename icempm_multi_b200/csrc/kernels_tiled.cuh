@@ -569,6 +569,22 @@ __device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes)
     if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
 }
 
+// Prefetches into L2 one column of the node region a tile stages (RY nodes of
+// column RX0 + col from row RY0, clipped to the grid) of one node array:
+// the first and the last node's lines (a column spans at most two lines).
+template <typename T>
+__device__ __forceinline__ void prefetch_region_column(const T *arr, int gridx, int gridy, int halo, int ny, int RX0,
+                                                       int RY0, int col)
+{
+    const int gx = RX0 + col;
+    if (gx < -halo || gx >= gridx + halo) return;
+    const int y0 = max(RY0, 0), y1 = min(RY0 + RY, gridy);
+    if (y1 <= y0) return;
+    const T *c = arr + (long)(gx + halo) * ny;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c + y0));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(c + y1 - 1));
+}
+
 // Starts moving the next tile's point lines that G2P reads (which < 8: utility,
 // Jp, x, y, Fe00..Fe11) or its cell ranges (which == 8) into L2 while this CTA
 // is in its cell phase.
