@@ -407,6 +407,8 @@ def main():
     torch.cuda.set_device(local)
     p, soa = make_workload(pinned=True)
     n = soa.size
+    # the other-precision leg starts from the same state (the end-to-end leg downloads into soa)
+    soa0 = soa.clone() if not args.no_extra else None
 
     # ---- headline path, device-resident timed region ----------------------------------
     g, stream, r = measure_instance(p, soa, args.precision, args.steps, args.warmup, local, pg, args.opt)
@@ -465,7 +467,7 @@ def main():
     if not args.no_extra:
         other = "fp64" if args.precision == "fp32" else "fp32"
         k2 = min(args.steps, 100)
-        g2, _, r2 = measure_instance(p, soa, other, k2, args.warmup, local, pg, profile=True, clocks=False)
+        g2, _, r2 = measure_instance(p, soa0, other, k2, args.warmup, local, pg, profile=True, clocks=False)
         g2.close()
         ms2 = max_over_ranks(pg, r2["ms"], local)
         out[other] = {"value": n * k2 * world / (ms2 / 1e3), "unit": METRIC, "ms_per_step": ms2 / k2,
