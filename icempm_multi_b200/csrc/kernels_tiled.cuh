@@ -29,7 +29,7 @@ constexpr int TX = 32, TY = 8, TT = TX * TY;   // stencil bases (cells) per tile
 constexpr int RM = 1;                          // drift margin (cells) of the staged region
 constexpr int RX = TX + 2 + 2 * RM, RY = TY + 2 + 2 * RM, RN = RX * RY;
 constexpr int TILE_THREADS = 256;
-constexpr int CAP = 704;                       // points staged per chunk
+constexpr int CAP = 1056;                      // points staged per chunk (a tile holds 1,024 at 4 per cell)
 constexpr int BASE_NONE = 0x7fffffff;
 constexpr int ICY_TIMEOUT_CODE = 108;          // ICY_ERR_TIMEOUT
 
@@ -415,8 +415,14 @@ __device__ __forceinline__ void store_point(double *__restrict__ pts, long pitch
 // with one padding column after every 4 points (cell threads read points about
 // 4 apart).  After the cell phase the same buffer holds the cell partials
 // (27 x TT doubles).
+// Moments of a point, four double2 vectors and a 64-bit word per slot, one
+// padding slot after every 4 points (the cell phase reads points about 4
+// apart per lane): (fx, fy), (m vx, m vy), (S00, S01), (S10, S11) with
+// S = m Bp - dt vol Dp_inv tau, and the packed stencil base (low 32 bits)
+// with the liquid flag (bit 32) that selects the point's mass.
 constexpr int MOM_N = CAP + CAP / 4;
-constexpr size_t MOM_BYTES = sizeof(double2) * 5 * MOM_N;
+constexpr size_t MOM_BYTES = (sizeof(double2) * 4 + sizeof(unsigned long long)) * MOM_N;
+constexpr unsigned long long MOM_LIQUID = 1ull << 32;
 static_assert(27 * TT * sizeof(double) <= MOM_BYTES, "cell partials alias the moment buffer");
 __device__ __forceinline__ int mom_col(int j) { return j + (j >> 2); }
 constexpr size_t TILE_DYN_SMEM = MOM_BYTES;
@@ -426,6 +432,7 @@ __device__ __forceinline__ void p2g_moments(const StepParams &P, const PointStat
                                             int *status)
 {
     double2 *m = reinterpret_cast<double2 *>(mom);
+    unsigned long long *mb = reinterpret_cast<unsigned long long *>(m + 4 * MOM_N);
     const int c = mom_col(j);
     const bool liquid = (s.util & kLiquid) != 0;
     const double mass = liquid ? P.mass_water : P.mass_ice;
@@ -433,21 +440,20 @@ __device__ __forceinline__ void p2g_moments(const StepParams &P, const PointStat
     const int e = base_error(P, bx, by);
     if (e) {
         *status = e;
-        m[4 * MOM_N + c].y = __longlong_as_double((long long)BASE_NONE);
+        mb[c] = (unsigned)BASE_NONE;
         return;
     }
     const M2<double> tau = liquid ? water_stress(s.Jp, P.kappa) : kirchhoff(s.F, P.mu, P.kappa);
     m[c] = make_double2(s.x * P.hinv - (double)bx, s.y * P.hinv - (double)by);
-    m[MOM_N + c] = make_double2(mass, s.vx * mass);
-    m[2 * MOM_N + c] = make_double2(s.vy * mass, mass * s.B.a00 - P.dt_vol_Dpinv * tau.a00);
-    m[3 * MOM_N + c] = make_double2(mass * s.B.a01 - P.dt_vol_Dpinv * tau.a01, mass * s.B.a10 - P.dt_vol_Dpinv * tau.a10);
-    m[4 * MOM_N + c] = make_double2(mass * s.B.a11 - P.dt_vol_Dpinv * tau.a11,
-                                    __longlong_as_double((long long)pack_base(bx, by)));
+    m[MOM_N + c] = make_double2(s.vx * mass, s.vy * mass);
+    m[2 * MOM_N + c] = make_double2(mass * s.B.a00 - P.dt_vol_Dpinv * tau.a00, mass * s.B.a01 - P.dt_vol_Dpinv * tau.a01);
+    m[3 * MOM_N + c] = make_double2(mass * s.B.a10 - P.dt_vol_Dpinv * tau.a10, mass * s.B.a11 - P.dt_vol_Dpinv * tau.a11);
+    mb[c] = (unsigned long long)(unsigned)pack_base(bx, by) | (liquid ? MOM_LIQUID : 0ull);
 }
 
 __device__ __forceinline__ void mom_none(double *mom, int j)
 {
-    reinterpret_cast<double2 *>(mom)[4 * MOM_N + mom_col(j)].y = __longlong_as_double((long long)BASE_NONE);
+    reinterpret_cast<unsigned long long *>(reinterpret_cast<double2 *>(mom) + 4 * MOM_N)[mom_col(j)] = (unsigned)BASE_NONE;
 }
 
 // Phases 2 and 3 for one chunk of points [cs, ce) of tile (tx, ty): cell
@@ -473,14 +479,15 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
         for (int j = r0; j < r1; j++) {
             const double2 *mv = reinterpret_cast<const double2 *>(mom);
             const int c = mom_col(j);
-            const double2 q4 = mv[4 * MOM_N + c];
-            const int pb = (int)__double_as_longlong(q4.y);
+            const unsigned long long bw = reinterpret_cast<const unsigned long long *>(mv + 4 * MOM_N)[c];
+            const int pb = (int)(unsigned)bw;
             if (pb == BASE_NONE) continue;
             int bx, by;
             unpack_base(pb, bx, by);
             const double2 q0 = mv[c], q1 = mv[MOM_N + c], q2 = mv[2 * MOM_N + c], q3 = mv[3 * MOM_N + c];
-            const double fx = q0.x, fy = q0.y, mass = q1.x, mvx = q1.y, mvy = q2.x;
-            const double s00 = q2.y, s01 = q3.x, s10 = q3.y, s11 = q4.x;
+            const double mass = (bw & MOM_LIQUID) ? P.mass_water : P.mass_ice;
+            const double fx = q0.x, fy = q0.y, mvx = q1.x, mvy = q1.y;
+            const double s00 = q2.x, s01 = q2.y, s10 = q3.x, s11 = q3.y;
             if (bx == bxc && by == byc) {
                 point_contributions(P.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
                                     [&](int a, int b, double W, double dm, double tx, double ty) {
@@ -723,7 +730,8 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_co
 // global memory.  One CTA per SM.
 constexpr int PIPE_CONS = 256, PIPE_THREADS = PIPE_CONS + 32, NSTAGE = 2;
 constexpr int NLINE = 8;                          // utility, Jp, x, y, Fe00..Fe11
-constexpr int LINE_CAP = CAP + 2;                 // slack for 16-byte alignment of the copy
+constexpr int PIPE_CAP = 704;                     // points per staged chunk of the pipelined kernel
+constexpr int LINE_CAP = PIPE_CAP + 2;            // slack for 16-byte alignment of the copy
 static_assert((LINE_CAP * sizeof(double)) % 16 == 0, "16-byte aligned staged lines");
 static __device__ __constant__ const int kPipeLines[NLINE] = {0, 3, 4, 5, 8, 9, 10, 11};
 constexpr uint64_t PIPE_WAIT_NS = 1000000000ull;  // a wait gives up after 1 s ...
@@ -771,7 +779,7 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __gr
             const int ps = A.cell_start[(long)t * TT], pe = A.cell_start[(long)(t + 1) * TT];
             const int tx = t % A.G.ntx, ty = t / A.G.ntx;
             const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
-            for (int cs = ps; cs < pe; cs += CAP, c++) {
+            for (int cs = ps; cs < pe; cs += PIPE_CAP, c++) {
                 const int st = c % NSTAGE, use = c / NSTAGE;
                 if (use > 0 && !mbar_wait(reinterpret_cast<uint64_t *>(&S.empty[st]), (use - 1) & 1,
                                           PIPE_WAIT_NS, PIPE_WAIT_POLLS)) {
@@ -780,7 +788,7 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __gr
                     break;
                 }
                 fence_proxy_async_smem();
-                const int ce = min(cs + CAP, pe);
+                const int ce = min(cs + PIPE_CAP, pe);
                 const int a0 = cs & ~1, a1 = (ce + 1) & ~1;
                 for (int k = lane; k < RN; k += 32) {
                     const int gx = RX0 + k / RY, gy = RY0 + k % RY;
@@ -833,7 +841,7 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __gr
         const int tx = t % A.G.ntx, ty = t / A.G.ntx;
         const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
         touch = 0;
-        for (int cs = ps; cs < pe; cs += CAP, c++) {
+        for (int cs = ps; cs < pe; cs += PIPE_CAP, c++) {
             const int st = c % NSTAGE, use = c / NSTAGE;
             // the decision to give up is made CTA-uniform through S.abort
             if (!mbar_wait(reinterpret_cast<uint64_t *>(&S.full[st]), use & 1, PIPE_WAIT_NS, PIPE_WAIT_POLLS)) {
