@@ -119,7 +119,7 @@ def test_points_at_every_wall(oracle):
 
 def test_tiles_with_more_points_than_a_chunk(oracle):
     """16 points per cell: a 32 x 8-cell tile holds up to 4,096 points, more
-    than one staged chunk (704 FP64 / 1,280 FP32), so the chunk loop runs."""
+    than one staged chunk (1,056 FP64 / 1,280 FP32), so the chunk loop runs."""
     p = params_for(96, 48, 0.25, 5e-5)
     soa = make_block(p, 40 * 0.25, 10 * 0.25, ppc=16, seed=34, n_grains=8)
     assert soa.size == 40 * 10 * 16
