@@ -260,6 +260,9 @@ int icy_mpm_set_option(icy_mpm *h, const char *name, double value)
     if (k == "resort_every") {
         if (value < 0) return ICY_ERR_INVALID_ARGUMENT;
         h->resort_every = (int)value;
+    } else if (k == "profile_every") {
+        if (value < 1 || value > (1 << 20)) return ICY_ERR_INVALID_ARGUMENT;
+        h->prof_every = (int)value;
     } else if (k == "pipe") {
         h->pipe = value != 0;
     } else if (k == "pipe_fault_test") {
@@ -295,17 +298,22 @@ static cudaEvent_t pool_get(icy_mpm *h)
 
 void icy_prof_begin(icy_mpm *h, int kernel)
 {
+    h->prof_cur = false;
     if (!h->profiling) return;
+    if (h->prof_seen.size() != K_N_KERNELS) h->prof_seen.assign(K_N_KERNELS, 0);
+    if (h->prof_seen[kernel]++ % h->prof_every != 0) return;   // not a sampled launch
     icy_mpm::ProfRec r{kernel, pool_get(h), pool_get(h)};
     if (!r.a || !r.b) return;
     cudaEventRecord(r.a, h->stream);
     h->prof_recs.push_back(r);
+    h->prof_cur = true;
 }
 
 void icy_prof_end(icy_mpm *h)
 {
-    if (!h->profiling || h->prof_recs.empty()) return;
+    if (!h->profiling || !h->prof_cur || h->prof_recs.empty()) return;
     cudaEventRecord(h->prof_recs.back().b, h->stream);
+    h->prof_cur = false;
 }
 
 int icy_prof_resolve(icy_mpm *h)
@@ -345,6 +353,7 @@ int icy_mpm_profile(icy_mpm *h, int enable)
         if (rc) return rc;
         h->prof_ms.assign(K_N_KERNELS, 0.0);
         h->prof_n.assign(K_N_KERNELS, 0);
+        h->prof_seen.assign(K_N_KERNELS, 0);
     }
     h->profiling = enable != 0;
     return ICY_OK;

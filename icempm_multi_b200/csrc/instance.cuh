@@ -67,6 +67,9 @@ struct icy_mpm {
     // per-kernel event profiling (icy_mpm_profile)
     struct ProfRec { int kernel; cudaEvent_t a, b; };
     bool profiling = false;
+    int prof_every = 1;                // time every prof_every-th launch of each kernel
+    bool prof_cur = false;             // the open launch is timed
+    std::vector<int64_t> prof_seen;    // launches of each kernel since profiling started
     std::vector<ProfRec> prof_recs;
     std::vector<cudaEvent_t> event_pool;
     std::vector<double> prof_ms;

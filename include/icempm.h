@@ -252,6 +252,10 @@ int icy_mpm_status(icy_mpm *h);
  *   "pipe_fault_test" 1 = (tests of the timeout path) the producer leaves the
  *                   ring's first stage unfilled: every wait on it gives up
  *                   after 1 s and the next download reports ICY_ERR_TIMEOUT
+ *   "profile_every" n = icy_mpm_profile times every n-th launch of each kernel
+ *                   (default 1); an event pair on the stream costs the step
+ *                   loop a few microseconds, so sampling keeps a profiled run
+ *                   close to an unprofiled one
  */
 int icy_mpm_set_option(icy_mpm *h, const char *name, double value);
 
@@ -259,15 +263,16 @@ int icy_mpm_set_option(icy_mpm *h, const char *name, double value);
 int64_t icy_mpm_kernel_launches(icy_mpm *h);
 /*
  * Per-kernel timing with CUDA events recorded on the instance stream around
- * every kernel launch (the event pairs of GPU_Partition::record_timings,
+ * every kernel launch, or every n-th launch of each kernel with the option
+ * "profile_every" (the event pairs of GPU_Partition::record_timings,
  * simulation/gpu_partition.cu:344-401, but per kernel and read only on
  * request).  enable=1 clears and starts recording, enable=0 stops.
  */
 int icy_mpm_profile(icy_mpm *h, int enable);
 /*
  * Synchronises and returns up to `max` kernel entries: names (max x 48 chars,
- * NUL-terminated), total milliseconds and launch counts; *count receives the
- * number of distinct kernels recorded.
+ * NUL-terminated), total milliseconds and counts of the timed launches;
+ * *count receives the number of distinct kernels recorded.
  */
 int icy_mpm_profile_read(icy_mpm *h, int max, char *names, double *ms_total,
                          int64_t *launches, int *count);
