@@ -114,7 +114,8 @@ class GPUImplementation:
         check(lib().icy_mpm_profile(self._h, int(bool(enable))), "icy_mpm_profile")
 
     def profile_read(self):
-        """{kernel name: (total ms, launches)} recorded since profiling was enabled."""
+        """{kernel name: (total ms, timed launches)} recorded since profiling was
+        enabled (every launch, or every n-th with the option "profile_every")."""
         mx = 32
         names = C.create_string_buffer(48 * mx)
         ms = np.zeros(mx)

@@ -215,3 +215,30 @@ def test_largest_grid_dimensions(oracle, shape):
     assert_close(field_errors(out, ref))
     out32, _, _ = run_split(p, soa, 20)
     assert field_errors(out32, ref)["pos"] <= POS_TOL
+
+
+@pytest.mark.parametrize("precision", [PRECISION_FP64, PRECISION_FP32_SPLIT])
+def test_kernel_timing_samples_every_nth_launch(precision):
+    """With the option profile_every = 4, 16 sub-steps time launches 0, 4, 8
+    and 12 of the grid update (16 launches) and of the fused step kernel (15),
+    with positive durations; profile_every = 1 times every launch."""
+    p, soa = standard(seed=8)
+    g = GPUImplementation(p, soa.clone(), precision=precision)
+    g.update_constants()
+    g.transfer_ponts_to_device()
+    g.set_option("resort_every", 0)
+    for every, expect in ((4, 4), (1, None)):
+        g.set_option("profile_every", every)
+        g.profile(True)
+        g.run_steps(0, 16, 0.0)
+        prof = g.profile_read()
+        g.profile(False)
+        ms_u, n_u = prof["k_update_nodes"]
+        ms_t, n_t = prof["k_tile_g2p2g"]
+        assert ms_u > 0 and ms_t > 0
+        assert (n_u, n_t) == ((4, 4) if expect else (16, 15))
+    from icempm_multi_b200._lib import ICY_ERR_INVALID_ARGUMENT, IcyError
+    with pytest.raises(IcyError) as e:
+        g.set_option("profile_every", 0)
+    assert e.value.code == ICY_ERR_INVALID_ARGUMENT
+    g.close()
