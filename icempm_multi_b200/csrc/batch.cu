@@ -19,6 +19,14 @@
 
 using namespace icy_dev;
 
+namespace icy_dev {   // batch_cargs.cu
+int batch_const_slots();
+cudaError_t batch_const_upload(const SplitArgs *args, int n, cudaStream_t s);
+cudaError_t batch_const_setup();
+void batch_const_launch_tile(int kind, int grid, cudaStream_t s, const SplitArgs &none, const SplitArgs *args,
+                             const BatchItem *work, const int *nwork, const int *rec);
+}
+
 #define CKB(call)                                                                 \
     do {                                                                          \
         cudaError_t e_ = (call);                                                  \
@@ -129,6 +137,7 @@ static int rebuild(icy_batch *b)
     for (int s = 0; s < b->nslots; s++)
         if (b->members[s]) args[s] = member_args(b, b->members[s], s);
     CKB(cudaMemcpyAsync(b->d_args, args.data(), sizeof(SplitArgs) * b->nslots, cudaMemcpyHostToDevice, b->stream));
+    if (b->nslots <= batch_const_slots()) CKB(batch_const_upload(args.data(), b->nslots, b->stream));
     k_batch_work_offsets<<<1, 1024, 0, b->stream>>>(b->d_args, b->d_clk, b->nslots, b->d_woff, b->d_nwork);
     k_batch_work_fill<<<dim3(8, b->nslots), 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_woff, b->d_work);
     CKB(cudaGetLastError());
@@ -152,6 +161,18 @@ static int rebin_members(icy_batch *b)
     return ICY_OK;
 }
 
+// The batched tile kernel (kind 0: first P2G, 1: fused, 2: last G2P): the
+// constant-bank variant for batches of at most batch_const_slots() slots.
+template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
+static void launch_tile_batch(icy_batch *b, const SplitArgs &none, size_t smem, int kind)
+{
+    if (b->nslots <= batch_const_slots())
+        batch_const_launch_tile(kind, b->tile_grid, b->stream, none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+    else
+        k_tile_f32<DO_G2P, DO_P2G, WRITE_VB, true><<<b->tile_grid, TILE_THREADS_F32, smem, b->stream>>>(
+            none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+}
+
 // Capture [P2G] + nsteps x [advance, update, G2P(+P2G)] as a graph.
 static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
 {
@@ -160,19 +181,16 @@ static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
     cudaGraph_t g = nullptr;
     int n = 0;
     CKB(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    k_tile_f32<false, true, false, true><<<b->tile_grid, TILE_THREADS_F32, MOMF_BYTES, b->stream>>>(
-        none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+    launch_tile_batch<false, true, false>(b, none, MOMF_BYTES, 0);
     n++;
     for (int k = 0; k < nsteps; k++) {
         k_batch_advance<<<(b->nslots + 127) / 128, 128, 0, b->stream>>>(b->d_clk, b->d_rec, b->nslots);
         k_update_list_f32<true><<<b->update_grid, 256, 0, b->stream>>>(SplitArgs{}, b->d_args, b->d_clk, b->d_tlist,
                                                                           b->d_tlist_n, 0.0, 0.0);
         if (k + 1 < nsteps)
-            k_tile_f32<true, true, false, true><<<b->tile_grid, TILE_THREADS_F32, MOMF_BYTES, b->stream>>>(
-                none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+            launch_tile_batch<true, true, false>(b, none, MOMF_BYTES, 1);
         else
-            k_tile_f32<true, false, true, true><<<b->tile_grid, TILE_THREADS_F32, 0, b->stream>>>(
-                none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+            launch_tile_batch<true, false, true>(b, none, 0, 2);
         n += 3;
     }
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
@@ -257,6 +275,7 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
                          (int)MOMF_BYTES);
     cudaFuncSetAttribute(k_tile_f32<false, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)MOMF_BYTES);
+    if ((e = batch_const_setup()) != cudaSuccess) return fail(e, "cudaFuncSetAttribute");
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false, true>, TILE_THREADS_F32,
                                                   MOMF_BYTES);
     b->tile_grid = std::max(1, sms * std::max(per_sm, 1));

@@ -1,0 +1,47 @@
+// batch_cargs.cu -- the batched tile kernel for batches of at most 128 slots,
+// reading its members' arguments from a constant-bank copy of the batch's
+// argument table (ICY_BATCH_CONST_ARGS in kernels_split.cuh).  The batched
+// step is 5-6 % faster at 120 members than with the global table, which the
+// kernels of batch.cu read for larger batches.
+#include <cuda_runtime.h>
+
+#include "../../include/icempm.h"
+#define ICY_BATCH_CONST_ARGS
+#include "kernels_split.cuh"
+
+using namespace icy_dev;
+
+namespace icy_dev {
+
+int batch_const_slots() { return BATCH_CONST_SLOTS; }
+
+// args[0 .. n) into the constant bank of this module, on stream s (n <= 128)
+cudaError_t batch_const_upload(const SplitArgs *args, int n, cudaStream_t s)
+{
+    if (n > BATCH_CONST_SLOTS) return cudaErrorInvalidValue;
+    return cudaMemcpyToSymbolAsync(c_batch_args, args, sizeof(SplitArgs) * n, 0, cudaMemcpyHostToDevice, s);
+}
+
+cudaError_t batch_const_setup()
+{
+    cudaError_t e = cudaFuncSetAttribute(k_tile_f32<true, true, false, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MOMF_BYTES);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_f32<false, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)MOMF_BYTES);
+    return e;
+}
+
+// kind 0: first P2G, 1: fused G2P + P2G, 2: last G2P (as in batch.cu)
+void batch_const_launch_tile(int kind, int grid, cudaStream_t s, const SplitArgs &none, const SplitArgs *args,
+                             const BatchItem *work, const int *nwork, const int *rec)
+{
+    if (kind == 0)
+        k_tile_f32<false, true, false, true><<<grid, TILE_THREADS_F32, MOMF_BYTES, s>>>(none, args, work, nwork, rec);
+    else if (kind == 1)
+        k_tile_f32<true, true, false, true><<<grid, TILE_THREADS_F32, MOMF_BYTES, s>>>(none, args, work, nwork, rec);
+    else
+        k_tile_f32<true, false, true, true><<<grid, TILE_THREADS_F32, 0, s>>>(none, args, work, nwork, rec);
+}
+
+}  // namespace icy_dev

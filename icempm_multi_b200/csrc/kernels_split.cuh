@@ -314,6 +314,16 @@ struct SplitArgs {
     long n_nodes;       // nodes of the grid
 };
 
+#ifdef ICY_BATCH_CONST_ARGS
+// Only in batch_cargs.cu: the member arguments of a batch of at most
+// BATCH_CONST_SLOTS slots, copied to the constant bank, where the batched
+// tile kernel reads them as the single-instance kernel reads its own (no
+// global loads and fewer spills in the point loop).  In its own translation
+// unit so that the kernels reading the global table compile as before.
+constexpr int BATCH_CONST_SLOTS = 128;
+static __constant__ SplitArgs c_batch_args[BATCH_CONST_SLOTS];
+#endif
+
 // P2G contributions of one point to its 3 x 3 nodes (simulation/kernels.cuh:
 // 100-120): node (a, b) gets W m and W (m v + S d) with W = wx[a] wy[b] and
 // d = ((a - fx) h, (b - fy) h).  S d is affine in (a, b), so it is evaluated
@@ -503,7 +513,11 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     while (ti < na) {
         const BatchItem w = BATCH ? work[ti] : BatchItem{0, A1.active[ti]};
         if (BATCH && tid == 0) s_claim = atomicAdd(A1.claim, 1);
+#ifdef ICY_BATCH_CONST_ARGS
+        const SplitArgs &A = BATCH ? c_batch_args[w.inst] : A1;
+#else
         const SplitArgs &A = BATCH ? Aarr[w.inst] : A1;
+#endif
         const StepParams &P = A.P;
         const bool record = BATCH ? rec[w.inst] != 0 : A.record_pq != 0;
         const float *fst = reinterpret_cast<const float *>(A.st);

@@ -61,7 +61,7 @@ class Request:
 
 
 class Server:
-    def __init__(self, budget_bytes=150e9, max_instances=1024, round_steps=50, device=0, keep_results=True):
+    def __init__(self, budget_bytes=150e9, max_instances=128, round_steps=50, device=0, keep_results=True):
         self.batch = Batch(max_instances, device=device)
         self.budget = float(budget_bytes)
         self.round_steps = int(round_steps)
