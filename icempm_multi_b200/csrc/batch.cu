@@ -21,6 +21,8 @@ using namespace icy_dev;
 
 namespace icy_dev {   // batch_cargs.cu
 int batch_const_slots();
+bool batch_const_acquire(int device, const void *batch);
+void batch_const_release(int device, const void *batch);
 cudaError_t batch_const_upload(const SplitArgs *args, int n, cudaStream_t s);
 cudaError_t batch_const_setup();
 void batch_const_launch_tile(int kind, int grid, cudaStream_t s, const SplitArgs &none, const SplitArgs *args,
@@ -69,6 +71,7 @@ struct icy_batch {
     std::map<int, cudaGraphExec_t> graphs;
     std::map<int, int> graph_launches;   // kernels per replay
     int tile_grid = 0, update_grid = 0;
+    bool cargs = false;              // owns the device's constant-bank argument table (batch_cargs.cu)
     int64_t launches = 0;
 };
 
@@ -137,7 +140,7 @@ static int rebuild(icy_batch *b)
     for (int s = 0; s < b->nslots; s++)
         if (b->members[s]) args[s] = member_args(b, b->members[s], s);
     CKB(cudaMemcpyAsync(b->d_args, args.data(), sizeof(SplitArgs) * b->nslots, cudaMemcpyHostToDevice, b->stream));
-    if (b->nslots <= batch_const_slots()) CKB(batch_const_upload(args.data(), b->nslots, b->stream));
+    if (b->cargs) CKB(batch_const_upload(args.data(), b->nslots, b->stream));
     k_batch_work_offsets<<<1, 1024, 0, b->stream>>>(b->d_args, b->d_clk, b->nslots, b->d_woff, b->d_nwork);
     k_batch_work_fill<<<dim3(8, b->nslots), 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_woff, b->d_work);
     CKB(cudaGetLastError());
@@ -162,11 +165,11 @@ static int rebin_members(icy_batch *b)
 }
 
 // The batched tile kernel (kind 0: first P2G, 1: fused, 2: last G2P): the
-// constant-bank variant for batches of at most batch_const_slots() slots.
+// constant-bank variant when this batch owns the device's table.
 template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
 static void launch_tile_batch(icy_batch *b, const SplitArgs &none, size_t smem, int kind)
 {
-    if (b->nslots <= batch_const_slots())
+    if (b->cargs)
         batch_const_launch_tile(kind, b->tile_grid, b->stream, none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
     else
         k_tile_f32<DO_G2P, DO_P2G, WRITE_VB, true><<<b->tile_grid, TILE_THREADS_F32, smem, b->stream>>>(
@@ -276,6 +279,7 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
     cudaFuncSetAttribute(k_tile_f32<false, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)MOMF_BYTES);
     if ((e = batch_const_setup()) != cudaSuccess) return fail(e, "cudaFuncSetAttribute");
+    b->cargs = max_instances <= batch_const_slots() && batch_const_acquire(device, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false, true>, TILE_THREADS_F32,
                                                   MOMF_BYTES);
     b->tile_grid = std::max(1, sms * std::max(per_sm, 1));
@@ -314,6 +318,7 @@ int icy_batch_destroy(icy_batch *b)
     cudaFree(b->d_woff);
     cudaFree(b->d_nwork);
     cudaFree(b->d_claim);
+    if (b->cargs) batch_const_release(b->device, b);
     if (b->h_clk) cudaFreeHost(b->h_clk);
     for (cudaEvent_t ev : b->ev_steps)
         if (ev) cudaEventDestroy(ev);

@@ -5,6 +5,9 @@
 // kernels of batch.cu read for larger batches.
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+
 #include "../../include/icempm.h"
 #define ICY_BATCH_CONST_ARGS
 #include "kernels_split.cuh"
@@ -14,6 +17,28 @@ using namespace icy_dev;
 namespace icy_dev {
 
 int batch_const_slots() { return BATCH_CONST_SLOTS; }
+
+// The table is one per device for the whole process: one batch at a time
+// owns it (the first small batch created on the device); the others read
+// their global tables.
+static std::mutex g_owner_mutex;
+static std::map<int, const void *> g_owner;
+
+bool batch_const_acquire(int device, const void *batch)
+{
+    std::lock_guard<std::mutex> g(g_owner_mutex);
+    auto it = g_owner.find(device);
+    if (it != g_owner.end() && it->second) return it->second == batch;
+    g_owner[device] = batch;
+    return true;
+}
+
+void batch_const_release(int device, const void *batch)
+{
+    std::lock_guard<std::mutex> g(g_owner_mutex);
+    auto it = g_owner.find(device);
+    if (it != g_owner.end() && it->second == batch) it->second = nullptr;
+}
 
 // args[0 .. n) into the constant bank of this module, on stream s (n <= 128)
 cudaError_t batch_const_upload(const SplitArgs *args, int n, cudaStream_t s)

@@ -128,3 +128,31 @@ def test_async_admission_and_retirement(oracle):
     b.wait_steps(0)
     assert b.info()["live"] == 2
     b.close()
+
+
+def test_two_small_batches_at_once(oracle):
+    """Two batches alive together, stepped in turns: the first owns the device's
+    constant-bank copy of its member arguments, the second reads its own global
+    table; each member matches the oracle, and after both are closed a new
+    batch takes the table over."""
+    (pa, sa), (pb, sb) = standard(seed=43), standard(n_cells_x=16, n_cells_y=6, grid=(64, 32), seed=44)
+    b1, b2 = Batch(4), Batch(4)
+    s1, s2 = b1.add(pa, sa), b2.add(pb, sb)
+    for _ in range(3):
+        b1.step(20)
+        b2.step(20)
+    o1, o2 = sa.clone(), sb.clone()
+    assert b1.download(s1, o1)[1] == 60 and b2.download(s2, o2)[1] == 60
+    ra, rb = sa.clone(), sb.clone()
+    assert oracle.run(pa, ra, 0, 60)[0] == 0 and oracle.run(pb, rb, 0, 60)[0] == 0
+    assert field_errors(o1, ra)["pos"] <= POS_TOL
+    assert field_errors(o2, rb)["pos"] <= POS_TOL
+    b1.close()
+    b2.close()
+    b3 = Batch(4)
+    s3 = b3.add(pb, sb)
+    b3.step(60)
+    o3 = sb.clone()
+    b3.download(s3, o3)
+    assert field_errors(o3, rb)["pos"] <= POS_TOL
+    b3.close()
