@@ -61,6 +61,12 @@ class Request:
 
 
 class Server:
+    """Continuous batching of requests on one device under a memory budget.
+
+    max_instances bounds the requests resident at once; a batch of at most
+    128 slots keeps its members' kernel arguments in the constant bank
+    (faster steps), so the default stays there."""
+
     def __init__(self, budget_bytes=150e9, max_instances=128, round_steps=50, device=0, keep_results=True):
         self.batch = Batch(max_instances, device=device)
         self.budget = float(budget_bytes)
