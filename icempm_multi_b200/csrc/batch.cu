@@ -391,7 +391,7 @@ int icy_batch_add_async(icy_batch *b, const icy_sim_params *p, const double *hss
     return add_member(b, p, hssoa, capacity, size, slot);
 }
 
-static __global__ void k_batch_leave(BatchClock *clk, int slot) { clk[slot].live = 0; }
+static __global__ void k_batch_leave(BatchClock *clk, int slot, int live) { clk[slot].live = live; }
 
 int icy_batch_retire(icy_batch *b, int slot, double *hssoa, unsigned capacity, double *bins)
 {
@@ -400,34 +400,51 @@ int icy_batch_retire(icy_batch *b, int slot, double *hssoa, unsigned capacity, d
     if (hssoa && h->n > capacity) return ICY_ERR_CAPACITY;
     CKB(cudaSetDevice(b->device));
     Retiring &r = b->retiring[slot];
+    // host-side preparation that can fail comes before the member leaves the
+    // device work list, so that a failure here leaves it a member on both sides
     if (!r.done) CKB(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming));
+    const int nbins = 2 * h->prm.n_indenter_subdivisions;
+    if (bins && r.bins_cap < nbins) {
+        if (r.h_bins) CKB(cudaFreeHost(r.h_bins));
+        r.h_bins = nullptr;
+        r.bins_cap = 0;
+        CKB(cudaMallocHost(&r.h_bins, sizeof(double) * nbins));
+        r.bins_cap = nbins;
+    }
     // leaves the batch after the work already queued; its clock stays for the readback
-    k_batch_leave<<<1, 1, 0, b->stream>>>(b->d_clk, slot);
+    k_batch_leave<<<1, 1, 0, b->stream>>>(b->d_clk, slot, 0);
     CKB(cudaGetLastError());
     b->launches++;
-    CKB(cudaEventRecord(b->ev_round, b->stream));
-    CKB(cudaStreamWaitEvent(b->side, b->ev_round, 0));
+    // a failure from here on puts the member back into the batch on the device
+    // (no round can have been queued in between) and leaves it a member
+    auto undo = [&](int rc) {
+        h->stream = b->stream;
+        k_batch_leave<<<1, 1, 0, b->stream>>>(b->d_clk, slot, 1);
+        if (cudaGetLastError() == cudaSuccess) b->launches++;
+        return rc;
+    };
+    cudaError_t e;
+    if ((e = cudaEventRecord(b->ev_round, b->stream)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(b->side, b->ev_round, 0)) != cudaSuccess) {
+        icy_set_error("icy_batch_retire(event)", e);
+        return undo(ICY_ERR_CUDA);
+    }
     h->stream = b->side;
     if (hssoa)
-        if (int rc = icy_instance_download(h, hssoa, capacity)) {
-            h->stream = b->stream;
-            return rc;
-        }
+        if (int rc = icy_instance_download(h, hssoa, capacity)) return undo(rc);
     r.bins = bins;
-    r.nbins = 2 * h->prm.n_indenter_subdivisions;
-    if (bins) {
-        if (r.bins_cap < r.nbins) {
-            if (r.h_bins) CKB(cudaFreeHost(r.h_bins));
-            r.h_bins = nullptr;
-            r.bins_cap = 0;
-            CKB(cudaMallocHost(&r.h_bins, sizeof(double) * r.nbins));
-            r.bins_cap = r.nbins;
-        }
-        CKB(cudaMemcpyAsync(r.h_bins, h->d_acc, sizeof(double) * r.nbins, cudaMemcpyDeviceToHost, b->side));
+    r.nbins = nbins;
+    if ((bins && (e = cudaMemcpyAsync(r.h_bins, h->d_acc, sizeof(double) * nbins, cudaMemcpyDeviceToHost,
+                                      b->side)) != cudaSuccess) ||
+        (e = cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->side)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(b->h_clk + slot, b->d_clk + slot, sizeof(BatchClock), cudaMemcpyDeviceToHost,
+                             b->side)) != cudaSuccess ||
+        (e = cudaEventRecord(r.done, b->side)) != cudaSuccess) {
+        icy_set_error("icy_batch_retire(readback)", e);
+        r.bins = nullptr;
+        return undo(ICY_ERR_CUDA);
     }
-    CKB(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->side));
-    CKB(cudaMemcpyAsync(b->h_clk + slot, b->d_clk + slot, sizeof(BatchClock), cudaMemcpyDeviceToHost, b->side));
-    CKB(cudaEventRecord(r.done, b->side));
     r.h = h;
     r.hssoa = hssoa;
     b->members[slot] = nullptr;

@@ -16,6 +16,7 @@
 // GPU (on different streams, or from different host threads) race on it.
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -47,24 +48,48 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
-void *g_scratch_addr[kMaxDevices] = {};
+struct Resolved { void *ctx; void *addr; };
+Resolved g_scratch[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device, resolved once
-// per device (with that device current).
+// The driver's cuCtxGetCurrent, through the runtime's entry-point query (the
+// library does not link the driver library itself).
+typedef int (*CtxGetCurrentFn)(void **);
+CtxGetCurrentFn ctx_get_current()
+{
+    static CtxGetCurrentFn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    return fn;
+}
+
+// Device address of the scratch array on the current device, resolved with
+// that device current at the first call, and again whenever the device's
+// context has changed since (after cudaDeviceReset the module, and with it
+// the array, is loaded anew and may sit at another address).
 int scratch_address(int device, unsigned char **out)
 {
     if (device < 0 || device >= kMaxDevices) return ICY_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_addr[device]) {
+    void *ctx = nullptr;
+    if (CtxGetCurrentFn f = ctx_get_current()) f(&ctx);
+    Resolved &r = g_scratch[device];
+    if (!r.addr || r.ctx != ctx) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) {
             icy_set_error("cudaGetSymbolAddress(g_noalloc_scratch)", e);
             return ICY_ERR_CUDA;
         }
-        g_scratch_addr[device] = p;
+        if (!ctx && ctx_get_current()) ctx_get_current()(&ctx);   // the call above made the context current
+        r.addr = p;
+        r.ctx = ctx;
     }
-    *out = static_cast<unsigned char *>(g_scratch_addr[device]);
+    *out = static_cast<unsigned char *>(r.addr);
     return ICY_OK;
 }
 
@@ -79,7 +104,8 @@ int scratch_address(int device, unsigned char **out)
 extern "C" int icy_step_noalloc(const icy_sim_params *p, double *d_hssoa, unsigned pitch, unsigned n, int step0,
                                 int nsteps, double *sim_time, double *d_indenter_bins, void *stream)
 {
-    if (!p || !sim_time || nsteps < 0 || (n > 0 && !d_hssoa) || pitch < n) return ICY_ERR_INVALID_ARGUMENT;
+    if (!p || !sim_time || nsteps < 0 || (n > 0 && !d_hssoa) || pitch < n || n > (unsigned)INT_MAX)
+        return ICY_ERR_INVALID_ARGUMENT;
     if (p->UpdateEveryNthStep <= 0 || p->GridXTotal < 4 || p->GridY < 4 || p->GridHaloSize < 0 ||
         p->n_indenter_subdivisions < 1)
         return ICY_ERR_INVALID_ARGUMENT;
@@ -115,15 +141,32 @@ extern "C" int icy_step_noalloc(const icy_sim_params *p, double *d_hssoa, unsign
 
     const StepParams P = icy_step_params(*p);
     double t = *sim_time;
+    double t_done = t;   // time of the last sub-step whose G2P was queued
+    cudaError_t e = cudaSuccess;
+    const char *where = nullptr;
     for (int k = 0; k < nsteps; k++) {
         // icy::Model::Step sub-step (simulation/model.cpp:40-49)
         t += p->InitialTimeStep;
         const double ind_x = p->indenter_x_initial + t * p->IndVelocity;
-        CKN(cudaMemsetAsync(grid, 0, sizeof(double) * 3 * n_nodes, s));
-        CKN(icy_launch_p2g_simple(s, P, d_hssoa, (long)pitch, (int)n, grid, n_nodes, status));
-        CKN(icy_launch_update_simple(s, P, grid, n_nodes, ind_x, p->indenter_y, bins));
         const int rec = ((step0 + k) % p->UpdateEveryNthStep) == 0;
-        CKN(icy_launch_g2p_simple(s, P, d_hssoa, (long)pitch, (int)n, grid, n_nodes, rec, status));
+        if ((e = cudaMemsetAsync(grid, 0, sizeof(double) * 3 * n_nodes, s)) != cudaSuccess) where = "cudaMemsetAsync(grid)";
+        else if ((e = icy_launch_p2g_simple(s, P, d_hssoa, (long)pitch, (int)n, grid, n_nodes, status)) != cudaSuccess)
+            where = "icy_launch_p2g_simple";
+        else if ((e = icy_launch_update_simple(s, P, grid, n_nodes, ind_x, p->indenter_y, bins)) != cudaSuccess)
+            where = "icy_launch_update_simple";
+        else if ((e = icy_launch_g2p_simple(s, P, d_hssoa, (long)pitch, (int)n, grid, n_nodes, rec, status)) !=
+                 cudaSuccess)
+            where = "icy_launch_g2p_simple";
+        if (where) break;
+        t_done = t;
+    }
+    if (where) {
+        // the sub-steps queued before the failure still run: wait for them, so
+        // that d_hssoa is no longer changing, and report how far it advanced
+        icy_set_error(where, e);
+        cudaStreamSynchronize(s);
+        *sim_time = t_done;
+        return ICY_ERR_CUDA;
     }
     int code = 0;
     CKN(cudaMemcpyAsync(&code, status, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -36,6 +36,10 @@ def workload_params(w, halo=8):
         "IndDiameter": 2 * w["ind_radius"], "IndVelocity": w["ind_velocity"], "IndDepth": w["ind_depth"],
         "SetupType": 0,
     }
+    if "strengths" in w:   # ice strengths (Pa): compressive, tensile, shear, second tensile
+        c, t, sh, t2 = w["strengths"]
+        cfg.update({"IceCompressiveStrength": c, "IceTensileStrength": t, "IceShearStrength": sh,
+                    "IceTensileStrength2": t2})
     p, _ = parse_json(json.dumps(cfg))
     return p
 

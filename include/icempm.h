@@ -365,7 +365,15 @@ int64_t icy_mpm_device_bytes(const icy_sim_params *p, unsigned capacity, int pre
  * d_indenter_bins (2*n_indenter_subdivisions doubles in device memory, or
  * NULL) accumulates the indenter force.  Work is queued on `stream` (NULL =
  * the default stream); the call then synchronises that stream and returns
- * the device error code (0, or the reference's 70..73).
+ * the device error code (0, or the reference's 70..73).  n may be at most
+ * INT_MAX.  If a CUDA call fails part way, the call waits for the sub-steps
+ * already queued, leaves *sim_time at the end of the last of them (so the
+ * caller knows how far d_hssoa advanced) and returns ICY_ERR_CUDA.
+ *
+ * It runs the one-thread-per-item FP64 kernels (the reference's own kernel
+ * structure: global FP64 atomics, no binning, which would need a second
+ * particle buffer), about half the speed of the binned, tile-staged path of
+ * icy_mpm_step on the same instance.
  *
  * It allocates nothing: the grid (5 arrays of GridY*(GridX+2*halo) doubles)
  * and the status word live in one file-scope device array of

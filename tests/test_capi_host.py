@@ -16,12 +16,12 @@ import pytest
 from icempm_multi_b200 import default_params, make_block, parse_file, parse_json
 from icempm_multi_b200._lib import (EXPORTED, ICY_ERR_CONFIG_MISSING, ICY_ERR_FILE, ICY_ERR_JSON, LIB_PATH,
                                     IcyError, SimParams, lib)
+from refpaths import INPUTS as REF_INPUTS
 from scenarios import params_for
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "icempm.h")
 REF_PARAMS = os.path.join(ROOT, "oracle", "_ref", "libref_params.so")
-REF_INPUTS = "/root/reference/input_"
 
 
 def header_symbols():
@@ -101,6 +101,27 @@ def test_reference_input_files_parse_identically(built):
         rc, raw_ref, _ = _ref_params().parse_file(ref, path)
         assert rc == 0 and raw == raw_ref, name
         assert bytes(ours) == bytes(ref), name
+
+
+GOLDEN_PARAMS = os.path.join(ROOT, "tests", "golden", "params_ref.json")
+
+
+def test_reset_and_parse_match_reference_golden(built, tmp_path):
+    """SimParams::Reset and ParseFile against the reference's own parser as
+    recorded in tests/golden/params_ref.json (written by
+    tests/golden/make_params_golden.py from oracle/_ref/libref_params.so):
+    the reference's parameter files and the configurations above, byte for
+    byte, where neither the reference tree nor rapidjson is present."""
+    g = json.load(open(GOLDEN_PARAMS))
+    assert bytes(default_params()) == bytes.fromhex(g["reset"])
+    assert len(g["cases"]) >= len(CONFIGS) + 5
+    for case in g["cases"]:
+        f = tmp_path / "cfg.json"
+        f.write_text(case["text"])
+        assert case["rc"] == 0, case["name"]
+        ours, raw = parse_file(str(f))
+        assert raw == case["raw"], case["name"]
+        assert bytes(ours) == bytes.fromhex(case["params"]), case["name"]
 
 
 def test_parse_errors(built, tmp_path):

@@ -7,11 +7,15 @@ import pytest
 
 from scenarios import randomized
 from test_gpu_parity import TOL, assert_close, field_errors, run_gpu
-from test_gpu_split import POS_TOL, TOL32, run_split
+from test_gpu_split import POS_TOL, run_split
 
 pytestmark = pytest.mark.gpu
 
 STEPS = 200
+# FP32 field bounds of these scenes (up to 74 % of the points crushed, the
+# return mapping taken at every step by most of them): about ten times the
+# largest errors measured over the twelve scenes (4.1e-4, 3.6e-4, 8.8e-4, 3.5e-4)
+TOL32_SCENES = {"vel": 4e-3, "Fe": 4e-3, "Bp": 1e-2, "Jp": 4e-3}
 
 
 @pytest.fixture(scope="module")
@@ -44,7 +48,7 @@ def test_randomized_scene_matches_oracle(oracle, seed):
     assert_close(e64)
     assert_close(es)
     assert e32["pos"] <= POS_TOL
-    for k, v in TOL32.items():
+    for k, v in TOL32_SCENES.items():
         assert e32[k] <= v, (k, e32)
 
 

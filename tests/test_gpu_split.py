@@ -2,22 +2,26 @@
 positions, FP32 Fe - I, FP32 grid; FP64 return mapping and force bins).
 
 Accuracy gate: relative L2 position error ||X - X_ref|| / ||X_ref|| <= 1e-4
-against the FP64 CPU oracle after 1000 steps.  Other fields are reported and
-held to the looser FP32 bounds written below.
+against the FP64 CPU oracle after 1000 steps.  Because positions are about
+75 m from the origin on the large grids, that figure dilutes local error, so
+the tests also bound the error relative to the displacement,
+||(X - X0) - (X_ref - X0)|| / ||X_ref - X0||, and the largest position
+difference in cells, max |X - X_ref| / h.  Other fields are held to the FP32
+bounds written below (about ten times the errors measured on these cases).
 """
 import numpy as np
 import pytest
 
 from icempm_multi_b200 import GPUImplementation
-from icempm_multi_b200._lib import PRECISION_FP32_SPLIT
+from icempm_multi_b200._lib import PRECISION_FP32_SPLIT, PRECISION_FP64
 from scenarios import standard, stress
 from test_gpu_parity import field_errors
 
 pytestmark = pytest.mark.gpu
 
 POS_TOL = 1e-4                       # the split-precision accuracy target
-TOL32 = {"vel": 5e-2, "Fe": 5e-2, "Jp": 5e-2}
-STATUS_MAX = 0.05
+TOL32 = {"vel": 1e-4, "Fe": 2e-4, "Bp": 2e-3, "Jp": 4e-4}   # measured at most 3.1e-6, 1.8e-5, 1.6e-4, 3.1e-5
+STATUS_MAX = 1e-3
 
 
 @pytest.fixture(scope="module")
@@ -57,6 +61,16 @@ def test_split_roundtrip(built):
     assert np.allclose(out.vel[:, m], soa.vel[:, m], rtol=1e-7, atol=1e-7)
 
 
+def displacement_errors(p, x0, a, b):
+    """Error of run a against run b relative to b's displacement from the
+    common start x0, and the largest position difference in cells."""
+    m = ~b.disabled()
+    d = np.linalg.norm(b.pos[:, m] - x0.pos[:, m])
+    return {"disp_rel": float(np.linalg.norm(a.pos[:, m] - b.pos[:, m]) / (d if d > 0 else 1.0)),
+            "max_dx_h": float(np.abs(a.pos[:, m] - b.pos[:, m]).max() / p.cellsize),
+            "disp_max_h": float(np.abs(b.pos[:, m] - x0.pos[:, m]).max() / p.cellsize)}
+
+
 def conservation_errors(p, a, b):
     """max |x_a - x_b| / h over the points, total mass of a and b (the same set
     of enabled points and materials: equal), and the total momentum
@@ -78,7 +92,9 @@ def test_split_1000_steps_within_target(oracle):
     out, t, bins = run_split(p, soa, 1000, chunk=250)
     errs = field_errors(out, ref)
     cons = conservation_errors(p, out, ref)
-    print("split 1000 steps", soa.size, errs, cons)
+    disp = displacement_errors(p, soa, out, ref)
+    print("split 1000 steps", soa.size, errs, cons, disp)
+    assert disp["disp_rel"] <= 2e-2, disp          # measured 2.2e-3 (displacements of 0.008 h)
     assert errs["pos"] <= POS_TOL
     for k, v in TOL32.items():
         assert errs[k] <= v, (k, errs)
@@ -131,10 +147,47 @@ def test_split_small_workload_1000_steps(oracle):
     out, _, _ = run_split(p, soa, 1000, chunk=250)
     errs = field_errors(out, ref)
     cons = conservation_errors(p, out, ref)
-    print("split small 1000 steps", soa.size, errs, cons)
+    disp = displacement_errors(p, soa, out, ref)
+    print("split small 1000 steps", soa.size, errs, cons, disp)
+    assert disp["disp_rel"] <= 2e-3, disp          # measured 1.9e-4
     assert errs["pos"] <= POS_TOL
     for k, v in TOL32.items():
         assert errs[k] <= v, (k, errs)
     assert errs["status"] <= STATUS_MAX
     assert cons["mass_a"] == cons["mass_b"]
     assert cons["max_dx_h"] <= 1e-2 and cons["momentum"] <= 1e-3, cons
+
+
+def test_large_instance_1000_steps_fp32_vs_fp64(built):
+    """The single large instance (grid 4096 x 2048 at h = 0.05 m, 150 m x
+    40 m block at 4 points per cell: 9.6 M points, dt 2e-5 s) for 1000 steps
+    on the FP32 split path against the tiled FP64 path on the same GPU (the
+    FP64 path is held to the FP64 oracle at 1e-12 by the parity tests): the
+    1e-4 accuracy gate at the benchmark's own size and length, with the
+    displacement-relative error, the largest position difference, the other
+    fields, mass and momentum."""
+    from icempm_multi_b200.workloads import LARGE, make_workload
+    p, soa = make_workload(LARGE)
+    assert soa.size == 9_600_000
+    runs = {}
+    for name, prec in (("fp64", PRECISION_FP64), ("fp32", PRECISION_FP32_SPLIT)):
+        out = soa.clone()
+        g = GPUImplementation(p, out, precision=prec)
+        g.update_constants()
+        g.transfer_ponts_to_device()
+        t = g.run_steps(0, 1000, 0.0)
+        g.transfer_from_device()
+        g.close()
+        runs[name] = (out, t)
+    assert runs["fp32"][1] == runs["fp64"][1]
+    a, b = runs["fp32"][0], runs["fp64"][0]
+    errs = field_errors(a, b)
+    cons = conservation_errors(p, a, b)
+    disp = displacement_errors(p, soa, a, b)
+    print("large 9.6M 1000 steps", errs, cons, disp)
+    assert errs["pos"] <= POS_TOL
+    assert disp["disp_rel"] <= 2e-3 and disp["max_dx_h"] <= 3e-4, disp   # measured 1.2e-4, 2.7e-5
+    for k, v in TOL32.items():
+        assert errs[k] <= v, (k, errs)
+    assert errs["status"] <= STATUS_MAX
+    assert cons["mass_a"] == cons["mass_b"] and cons["momentum"] <= 1e-3, cons

@@ -19,8 +19,7 @@ from scenarios import comparable_bits
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "icempm_host.h")
-REF = "/root/reference"
-GEOM = os.path.join(REF, "build", "geometries_2d")
+from refpaths import GEOM, REF
 have_geom = pytest.mark.skipif(not os.path.exists(os.path.join(GEOM, "2d_70k.h5")),
                                reason="reference point clouds absent")
 
