@@ -125,7 +125,7 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
             icy_set_error("cudaMalloc(grid)", e);
             return ICY_ERR_OUT_OF_MEMORY;
         }
-        CK(dalloc(h, reinterpret_cast<GrainConstF **>(&h->d_grainf), GRAIN_TAB));
+        CK(dalloc(h, reinterpret_cast<GrainConstF **>(&h->d_grainf), GRAIN_TAB_F32));
         CK(cudaMemsetAsync(h->d_st, 0, sizeof(unsigned) * S_NLINES * h->pitch, h->stream));
         CK(cudaMemsetAsync(h->d_gridf, 0, sizeof(float) * 6 * h->n_nodes, h->stream));
     } else {
@@ -301,8 +301,8 @@ int icy_instance_bin(icy_mpm *h)
     icy_prof_begin(h, K_BIN);
     CK(cudaMemsetAsync(h->d_counts, 0, sizeof(int) * nkeys, h->stream));
     if (is_split(h))
-        k_bin_count_f32<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_st, h->pitch, (int)h->n, h->d_keys,
-                                                   h->d_ranks, h->d_counts, h->d_status);
+        k_bin_count_f32<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_st, (int)h->n, h->d_keys, h->d_ranks,
+                                                   h->d_counts, h->d_status);
     else
         k_bin_count<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_pts, h->pitch, (int)h->n, h->d_keys,
                                                h->d_ranks, h->d_counts, h->d_status);
@@ -469,7 +469,7 @@ int icy_instance_constants(icy_mpm *h)
     k_grain_table<<<(GRAIN_TAB + 255) / 256, 256, 0, h->stream>>>(icy_step_params(h->prm), h->d_grain);
     CK_LAUNCH("k_grain_table");
     if (is_split(h)) {
-        k_grain_table_f32<<<(GRAIN_TAB + 255) / 256, 256, 0, h->stream>>>(h->d_grain,
+        k_grain_table_f32<<<(GRAIN_TAB_F32 + 255) / 256, 256, 0, h->stream>>>(h->d_grain,
                                                                         static_cast<GrainConstF *>(h->d_grainf));
         CK_LAUNCH("k_grain_table_f32");
     }

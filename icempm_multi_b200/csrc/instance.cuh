@@ -33,8 +33,8 @@ struct icy_mpm {
     int *d_block_sums = nullptr;
 
     // FP32 split-precision state (precision == ICY_PRECISION_FP32_SPLIT):
-    // 17 lines of 4-byte words per point, an FP32 grid, FP64 staging for the
-    // HSSOA conversion
+    // 17 words per point in 32-point blocks (kernels_split.cuh), an FP32 grid,
+    // FP64 staging for the HSSOA conversion
     unsigned *d_st = nullptr, *d_st_alt = nullptr;
     double *d_stage = nullptr;
     long stage_n = 0;

@@ -1,28 +1,46 @@
 // kernels_split.cuh -- FP32 "split precision" variant of the tiled step.
 //
-// Device state per point (17 lines of 4 bytes, `pitch` entries each):
-//   utility (low 32 bits of the reference's 64-bit word), packed integer cell
-//   (cx + 32768) << 16 | cy, FP32 offset inside the cell (ox, oy in [0,1)),
-//   FP32 De = Fe - I, Jp, then vx, vy, Bp (4), P, Q.
-// Positions as integer cell + FP32 offset keep ~1e-8 cells of resolution on
-// any grid; holding Fe - I instead of Fe keeps full FP32 precision of the
-// small elastic strain, and det(Fe) - 1 and dev(Fe Fe^T) are formed from De
-// without cancellation.  Grid mass and momentum are FP32.  FP64 is kept for
-// the return mapping of crushed points (the projected Fe is formed in FP64
-// and stored back as Fe - I, so nearly equal singular values lose nothing)
-// and for the indenter force bins.  The tiling, sorting and the three phases
-// are those of the FP64 kernels in kernels_tiled.cuh.
+// Device state, in blocks of 32 points (point i: block i / 32, lane i % 32),
+// `pitch` points of capacity (a multiple of 32), 17 words per point:
+//   hot part, read and written at every step, 288 words per block:
+//     words [0, 128)    one 16-byte vector per point: (base word, gx, gy, utility)
+//     words [128, 256)  one 16-byte vector per point: De = Fe - I (d00, d01, d10, d11)
+//     words [256, 288)  Jp_inv per point
+//   cold part (from word 9 * pitch on), written on the last step of a call
+//   and on record steps only, 256 words per block:
+//     words [0, 128)    (vx, vy, P, Q) per point
+//     words [128, 256)  Bp (b00, b01, b10, b11) per point
+// so that a thread reads and writes a point's step state with two 128-bit
+// and one 32-bit access, a warp's accesses are contiguous, and a tile's
+// points (consecutive after binning) are one contiguous range of the hot part.
+//
+// Position: the reference's stencil base b = (int)(x/h - 0.5) (truncation,
+// simulation/kernels.cuh:90), packed with 16 bits per axis in the base word,
+// and g = x/h - b - 1 in FP32: g lies in [-0.5, 0.5) wherever x/h >= 0.5
+// (elsewhere the truncation puts it in (-1.5, -0.5]).  The quadratic
+// B-spline weights are 0.5 (0.5 - g)^2, 0.75 - g^2, 0.5 (0.5 + g)^2, the node
+// offsets (i - fx) are (i - 1 - g), nothing is re-based between G2P and P2G,
+// and moving a point to the next base (g -= 1 or g += 1 from [0.5, 1) or
+// [-1, -0.5)) is exact.  g keeps ~3e-8 cells of resolution on any grid.
+// Holding Fe - I instead of Fe keeps full FP32 precision of the small elastic
+// strain, and det(Fe) - 1 and dev(Fe Fe^T) are formed from De without
+// cancellation.  Grid mass and momentum are FP32.  FP64 is kept for the
+// return mapping of crushed points (the projected Fe is formed in FP64 and
+// stored back as Fe - I, so nearly equal singular values lose nothing) and
+// for the indenter force bins.  The tiling, sorting and the three phases are
+// those of the FP64 kernels in kernels_tiled.cuh.
 #pragma once
 #include "kernels_tiled.cuh"
 
 namespace icy_dev {
 
-enum SplitLine {
-    S_UTIL = 0, S_CELL, S_OX, S_OY, S_D00, S_D01, S_D10, S_D11, S_JP,
-    S_VX, S_VY, S_B00, S_B01, S_B10, S_B11, S_P, S_Q, S_NLINES
-};
+constexpr int SB = 32;                   // points per block of the state
+constexpr int HOT_WORDS = 9 * SB;        // words of a block's hot part
+constexpr int COLD_WORDS = 8 * SB;       // words of a block's cold part
+constexpr int S_NLINES = 17;             // words per point, hot + cold
+constexpr int S_HOT = 9;                 // the cold part starts at word S_HOT * pitch
 
-struct GrainConstF { float pmin2, k, msq; };
+struct GrainConstF { float pmin2, k, msq, pad; };
 
 // FP32 copies of the per-step constants
 struct SplitConsts {
@@ -40,33 +58,60 @@ __host__ __device__ inline SplitConsts split_consts(const StepParams &P)
     return c;
 }
 
+// Failure-surface constants in FP32: [0, GRAIN_TAB) by grain slot as the FP64
+// table, then [GRAIN_TAB, GRAIN_TAB + 330) by grain id modulo 330.  The
+// reference varies the constants with (grain + 3) % 30 and (grain + 4) % 11
+// of the grain id as a short (simulation/kernels.cuh:341,560-576): for a
+// non-negative id that is periodic in 330, so one remainder finds the entry;
+// a negative id (C remainders are negative) takes the slot table.
+constexpr int GRAIN_PERIOD = 330, GRAIN_TAB_F32 = GRAIN_TAB + GRAIN_PERIOD;
 static __global__ void k_grain_table_f32(const GrainConst *tab, GrainConstF *out)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < GRAIN_TAB) out[s] = GrainConstF{(float)tab[s].pmin2, (float)tab[s].k, (float)tab[s].msq};
+    if (s >= GRAIN_TAB_F32) return;
+    const GrainConst c = tab[s < GRAIN_TAB ? s : grain_slot(s - GRAIN_TAB)];
+    out[s] = GrainConstF{(float)c.pmin2, (float)c.k, (float)c.msq, 0.f};
+}
+__device__ __forceinline__ int grain_entry_f32(unsigned util)
+{
+    const short g = (short)util;
+    return g >= 0 ? GRAIN_TAB + (int)((unsigned)g % GRAIN_PERIOD) : grain_slot(g);
 }
 
-__device__ __forceinline__ unsigned pack_cell(int cx, int cy) { return ((unsigned)(cx + 32768) << 16) | (unsigned)cy; }
-__device__ __forceinline__ void unpack_cell(unsigned k, int &cx, int &cy)
+// base word: 16 bits per axis, each offset by 32768
+__host__ __device__ __forceinline__ unsigned split_pack(int bx, int by)
 {
-    cx = (int)(k >> 16) - 32768;
-    cy = (int)(k & 0xffffu);
+    return ((unsigned)(bx + 32768) << 16) | ((unsigned)(by + 32768) & 0xffffu);
+}
+__host__ __device__ __forceinline__ void split_unpack(unsigned w, int &bx, int &by)
+{
+    bx = (int)(w >> 16) - 32768;
+    by = (int)(w & 0xffffu) - 32768;
 }
 
-// Stencil base with the reference's truncation, (int)(x/h - 0.5) (kernels.cuh:90),
-// from cell c and offset o (x/h = c + o), and the offset f = x/h - base.
-__device__ __forceinline__ void split_base(int c, float o, int &base, float &f)
+// Moves (b, g) to the base of the new position after g changed by at most a
+// cell or so: the reference's truncating base (int)(b + g + 0.5)
+// (simulation/kernels.cuh:90) and g = x/h - b - 1.  Returns false on the
+// common path (g still in [-0.5, 0.5): the base is unchanged).
+__device__ __forceinline__ bool split_rebase(int &b, float &g)
 {
-    const bool nonneg = c >= 1 || (c == 0 && o >= 0.5f);   // c + o - 0.5 >= 0
-    base = nonneg ? (o >= 0.5f ? c : c - 1) : (o > 0.5f ? c + 1 : c);
-    f = (float)(c - base) + o;
+    if (g >= -0.5f && g < 0.5f) return false;
+    // floor semantics first (bounded: a step moves a point by at most half a cell)
+    for (int k = 0; k < 4 && g >= 0.5f; k++) { b += 1; g -= 1.0f; }
+    for (int k = 0; k < 4 && g < -0.5f; k++) { b -= 1; g += 1.0f; }
+    // truncation toward zero where x/h - 0.5 = b + (g + 0.5) is negative and not whole
+    if (b < 0 && g > -0.5f) { b += 1; g -= 1.0f; }
+    return true;
 }
 
-__device__ __forceinline__ void split_renorm(int &c, float &o)
+// quadratic B-spline weights of the stencil columns 0, 1, 2 (simulation/kernels.cuh:100-103)
+// with fx = 1 + g
+__device__ __forceinline__ void weights_g(float g, float w[3])
 {
-    if (o >= 1.0f) { c += 1; o -= 1.0f; }
-    else if (o < 0.0f) { c -= 1; o += 1.0f; }
-    if (o >= 1.0f) o = 0.99999994f;   // o = 1 - ulp after rounding
+    const float a0 = 0.5f - g, a2 = 0.5f + g;
+    w[0] = (0.5f * a0) * a0;
+    w[1] = 0.75f - g * g;
+    w[2] = (0.5f * a2) * a2;
 }
 
 // dev(Fe Fe^T) and J = det Fe from De = Fe - I, without cancellation:
@@ -81,11 +126,20 @@ __device__ __forceinline__ void split_dev(const M2<float> &D, float &jm1, float 
 }
 
 struct PointF {
-    unsigned util;
-    int cx, cy;
-    float ox, oy, Jp, vx, vy, ptr, qtr;
+    unsigned util, bw;   // utility (low 32 bits), base word
+    int bx, by;
+    float gx, gy, Jp, vx, vy, ptr, qtr;
     M2<float> D, B;
 };
+
+// addresses of point i's vectors in the blocked state
+__device__ __forceinline__ unsigned *hot_vec(unsigned *st, long i) { return st + (i >> 5) * HOT_WORDS + (i & 31) * 4; }
+__device__ __forceinline__ const unsigned *hot_vec(const unsigned *st, long i)
+{
+    return st + (i >> 5) * HOT_WORDS + (i & 31) * 4;
+}
+__device__ __forceinline__ long hot_jp(long i) { return (i >> 5) * HOT_WORDS + 256 + (i & 31); }
+__device__ __forceinline__ long cold_vec(long pitch, long i) { return S_HOT * pitch + (i >> 5) * COLD_WORDS + (i & 31) * 4; }
 
 // The return mapping of a crushed point in FP64 (kernels.cuh:540-545, 623-674)
 // from its FP32 state, out of line: few points take it, and keeping its FP64
@@ -108,40 +162,38 @@ template <typename VSrc>
 __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitConsts &Q, const GrainConstF *tab,
                                                PointF &s, int *status, VSrc &&vsrc)
 {
-    int bx, by;
-    float fx, fy;
-    split_base(s.cx, s.ox, bx, fx);
-    split_base(s.cy, s.oy, by, fy);
-    const int e = base_error(P, bx, by);
+    const int e = base_error(P, s.bx, s.by);
     if (e) { *status = e; return false; }
     float wx[3], wy[3];
-    bspline_weights(fx, wx);
-    bspline_weights(fy, wy);
+    weights_g(s.gx, wx);
+    weights_g(s.gy, wy);
     // v = sum W v_i and Bp = 4/h sum W v_i (i - f)^T (kernels.cuh:357-372),
     // separably: sums over b with wy per column a, then over a with wx;
-    // sum W v_i (i - f) = sum W v_i i - f v
+    // sum W v_i (i - f) = sum W v_i (i - 1) - g v
     float2 nv[9];
-    vsrc(bx, by, nv);
+    vsrc(s.bx, s.by, nv);
     float cvx[3], cvy[3], cbx[3], cby[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         const float2 n0 = nv[a * 3], n1 = nv[a * 3 + 1], n2 = nv[a * 3 + 2];
         cvx[a] = wy[0] * n0.x + wy[1] * n1.x + wy[2] * n2.x;
         cvy[a] = wy[0] * n0.y + wy[1] * n1.y + wy[2] * n2.y;
-        cbx[a] = wy[1] * n1.x + 2.f * (wy[2] * n2.x);
-        cby[a] = wy[1] * n1.y + 2.f * (wy[2] * n2.y);
+        cbx[a] = wy[2] * n2.x - wy[0] * n0.x;
+        cby[a] = wy[2] * n2.y - wy[0] * n0.y;
     }
     const float vx = wx[0] * cvx[0] + wx[1] * cvx[1] + wx[2] * cvx[2];
     const float vy = wx[0] * cvy[0] + wx[1] * cvy[1] + wx[2] * cvy[2];
-    const float sax = wx[1] * cvx[1] + 2.f * (wx[2] * cvx[2]), say = wx[1] * cvy[1] + 2.f * (wx[2] * cvy[2]);
+    const float sax = wx[2] * cvx[2] - wx[0] * cvx[0], say = wx[2] * cvy[2] - wx[0] * cvy[0];
     const float sbx = wx[0] * cbx[0] + wx[1] * cbx[1] + wx[2] * cbx[2];
     const float sby = wx[0] * cby[0] + wx[1] * cby[1] + wx[2] * cby[2];
-    const M2<float> B{Q.s4 * (sax - fx * vx), Q.s4 * (sbx - fy * vx), Q.s4 * (say - fx * vy), Q.s4 * (sby - fy * vy)};
+    const M2<float> B{Q.s4 * (sax - s.gx * vx), Q.s4 * (sbx - s.gy * vx), Q.s4 * (say - s.gx * vy),
+                      Q.s4 * (sby - s.gy * vy)};
     // advection in cell units, x += v dt (kernels.cuh:375)
-    s.ox += vx * Q.dt_hinv;
-    s.oy += vy * Q.dt_hinv;
-    split_renorm(s.cx, s.ox);
-    split_renorm(s.cy, s.oy);
+    s.gx += vx * Q.dt_hinv;
+    s.gy += vy * Q.dt_hinv;
+    const bool mx = split_rebase(s.bx, s.gx);
+    const bool my = split_rebase(s.by, s.gy);
+    if (mx || my) s.bw = split_pack(s.bx, s.by);
     // Fe <- (I + dt Bp) Fe  as  De <- De + T + T De,  T = dt Bp (kernels.cuh:376)
     const M2<float> T{Q.dt * B.a00, Q.dt * B.a01, Q.dt * B.a10, Q.dt * B.a11};
     const M2<float> D = s.D;
@@ -159,8 +211,8 @@ __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitC
         s.ptr = -(Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
         s.qtr = __fdividef(2.f * Q.mu, Je) * sqrtf(d00 * d00 + d01 * d01);   // sqrt(2) mu/J |dev|, |dev| = sqrt(2(d00^2+d01^2))
         if (!(s.util & (unsigned)kCrushed)) {
-            const GrainConstF *gc = tab + grain_slot((short)s.util);
-            const float pmin2 = __ldg(&gc->pmin2), k = __ldg(&gc->k), msq = __ldg(&gc->msq);
+            const float4 gc = __ldg(reinterpret_cast<const float4 *>(tab) + grain_entry_f32(s.util));
+            const float pmin2 = gc.x, k = gc.y, msq = gc.z;
             bool crushed;
             if (s.ptr < 0.f) crushed = s.ptr < pmin2 || s.qtr > k * (s.ptr - pmin2);
             else crushed = (1.f + 2.f * Q.beta) * s.qtr * s.qtr + msq * (s.ptr + Q.beta * Q.pmax) * (s.ptr - Q.pmax) > 0.f;
@@ -181,36 +233,40 @@ __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitC
 __device__ __forceinline__ void store_point_f32(unsigned *__restrict__ st, long pitch, long i, const PointF &s,
                                                 bool write_vb, bool record_pq)
 {
-    float *f = reinterpret_cast<float *>(st);
-    st[i] = s.util;
-    st[i + pitch * S_CELL] = pack_cell(s.cx, s.cy);
-    f[i + pitch * S_OX] = s.ox;
-    f[i + pitch * S_OY] = s.oy;
-    f[i + pitch * S_D00] = s.D.a00; f[i + pitch * S_D01] = s.D.a01;
-    f[i + pitch * S_D10] = s.D.a10; f[i + pitch * S_D11] = s.D.a11;
-    f[i + pitch * S_JP] = s.Jp;
-    if (write_vb) {
-        f[i + pitch * S_VX] = s.vx; f[i + pitch * S_VY] = s.vy;
-        f[i + pitch * S_B00] = s.B.a00; f[i + pitch * S_B01] = s.B.a01;
-        f[i + pitch * S_B10] = s.B.a10; f[i + pitch * S_B11] = s.B.a11;
+    unsigned *v = hot_vec(st, i);
+    *reinterpret_cast<uint4 *>(v) = make_uint4(s.bw, __float_as_uint(s.gx), __float_as_uint(s.gy), s.util);
+    *reinterpret_cast<float4 *>(v + 128) = make_float4(s.D.a00, s.D.a01, s.D.a10, s.D.a11);
+    reinterpret_cast<float *>(st)[hot_jp(i)] = s.Jp;
+    if (write_vb || record_pq) {
+        float *c = reinterpret_cast<float *>(st) + cold_vec(pitch, i);
+        if (write_vb) {
+            *reinterpret_cast<float2 *>(c) = make_float2(s.vx, s.vy);
+            *reinterpret_cast<float4 *>(c + 128) = make_float4(s.B.a00, s.B.a01, s.B.a10, s.B.a11);
+        }
+        if (record_pq) *reinterpret_cast<float2 *>(c + 2) = make_float2(s.ptr, s.qtr);
     }
-    if (record_pq) { f[i + pitch * S_P] = s.ptr; f[i + pitch * S_Q] = s.qtr; }
 }
 
-__device__ __forceinline__ void load_point_f32(const unsigned *__restrict__ st, long pitch, long i, PointF &s)
+// Loads point i's step state; returns false for a disabled point.
+__device__ __forceinline__ bool load_point_f32(const unsigned *__restrict__ st, long i, PointF &s)
 {
-    const float *f = reinterpret_cast<const float *>(st);
-    unpack_cell(st[i + pitch * S_CELL], s.cx, s.cy);
-    s.ox = f[i + pitch * S_OX];
-    s.oy = f[i + pitch * S_OY];
-    s.D = {f[i + pitch * S_D00], f[i + pitch * S_D01], f[i + pitch * S_D10], f[i + pitch * S_D11]};
-    s.Jp = f[i + pitch * S_JP];
+    const unsigned *v = hot_vec(st, i);
+    const uint4 a = *reinterpret_cast<const uint4 *>(v);
+    const float4 d = *reinterpret_cast<const float4 *>(v + 128);
+    s.Jp = reinterpret_cast<const float *>(st)[hot_jp(i)];
+    s.bw = a.x;
+    s.gx = __uint_as_float(a.y);
+    s.gy = __uint_as_float(a.z);
+    s.util = a.w;
+    s.D = {d.x, d.y, d.z, d.w};
+    split_unpack(s.bw, s.bx, s.by);
+    return !(s.util & (unsigned)kDisabled);
 }
 
 // ---------------------------------------------------------------- P2G (FP32)
 // Moments of a point as three vectors in shared memory, one padding column
 // after every 4 points (the cell phase reads points about 4 apart per lane):
-//   m0 = (fx, fy, mass, m vx),  m1 = (m vy, S00, S01, S10),  m2 = (S11, base)
+//   m0 = (gx, gy, mass, m vx),  m1 = (m vy, S00, S01, S10),  m2 = (S11, base word)
 // with S = m Bp - dt vol Dp_inv tau (simulation/kernels.cuh:57-92).
 constexpr int CAPF = 1280;                // points per chunk of the FP32 tile kernel
 constexpr int MOMF_N = CAPF + CAPF / 4;
@@ -232,11 +288,7 @@ __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const Split
     const MomF M(mom);
     const bool liquid = (s.util & (unsigned)kLiquid) != 0;
     const float mass = liquid ? Q.mass_water : Q.mass_ice;
-    int bx, by;
-    float fx, fy;
-    split_base(s.cx, s.ox, bx, fx);
-    split_base(s.cy, s.oy, by, fy);
-    const int e = base_error(P, bx, by);
+    const int e = base_error(P, s.bx, s.by);
     if (e) {
         *status = e;
         M.none(j);
@@ -255,10 +307,10 @@ __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const Split
         tau = {s1 * d00 + s2, s1 * d01, s1 * d01, -s1 * d00 + s2};
     }
     const int c = momf_col(j);
-    M.m0[c] = make_float4(fx, fy, mass, s.vx * mass);
+    M.m0[c] = make_float4(s.gx, s.gy, mass, s.vx * mass);
     M.m1[c] = make_float4(s.vy * mass, mass * s.B.a00 - Q.dtvd * tau.a00, mass * s.B.a01 - Q.dtvd * tau.a01,
                           mass * s.B.a10 - Q.dtvd * tau.a10);
-    M.m2[c] = make_float2(mass * s.B.a11 - Q.dtvd * tau.a11, __int_as_float(pack_base(bx, by)));
+    M.m2[c] = make_float2(mass * s.B.a11 - Q.dtvd * tau.a11, __uint_as_float(s.bw));
 }
 
 // FP32 grid of n nodes in one allocation of 6 n floats, in one of two layouts.
@@ -298,7 +350,7 @@ struct SplitArgs {
     SplitConsts Q;
     TileGeom G;
     GridViewF g;
-    unsigned *st;
+    unsigned *st;       // blocked state: hot part, then the cold part from word S_HOT * pitch
     long pitch;
     const int *cell_start, *active, *n_active;
     unsigned *flags;
@@ -308,7 +360,7 @@ struct SplitArgs {
     int *status;
     unsigned long long *moved;
     int *claim;         // batch: [0] next work item to hand out, [1] CTAs finished (zero between launches)
-    const GrainConstF *grain_tab;
+    const GrainConstF *grain_tab;   // GRAIN_TAB_F32 entries
     int record_pq;
     double *acc;        // indenter force bins
     long n_nodes;       // nodes of the grid
@@ -326,37 +378,40 @@ static __constant__ SplitArgs c_batch_args[BATCH_CONST_SLOTS];
 
 // P2G contributions of one point to its 3 x 3 nodes (simulation/kernels.cuh:
 // 100-120): node (a, b) gets W m and W (m v + S d) with W = wx[a] wy[b] and
-// d = ((a - fx) h, (b - fy) h).  S d is affine in (a, b), so it is evaluated
-// as c0 + a S(:,0) h + b S(:,1) h: per node one product for W and one
-// multiply-add per component.
+// d = ((a - fx) h, (b - fy) h) = ((a - 1 - gx) h, (b - 1 - gy) h).  S d is
+// affine in (a, b), so it is evaluated as c + (a - 1) S(:,0) h + (b - 1) S(:,1) h:
+// per node one product for W and one addition per component.
 template <typename Sink>
-__device__ __forceinline__ void point_contributions_f32(float h, float fx, float fy, float mass, float mvx,
+__device__ __forceinline__ void point_contributions_f32(float h, float gx, float gy, float mass, float mvx,
                                                         float mvy, float s00, float s01, float s10, float s11,
                                                         Sink &&sink)
 {
     float wx[3], wy[3];
-    bspline_weights(fx, wx);
-    bspline_weights(fy, wy);
+    weights_g(gx, wx);
+    weights_g(gy, wy);
     const float s00h = s00 * h, s01h = s01 * h, s10h = s10 * h, s11h = s11 * h;
-    const float c0x = mvx - (s00h * fx + s01h * fy), c0y = mvy - (s10h * fx + s11h * fy);
+    const float cx = mvx - (s00h * gx + s01h * gy), cy = mvy - (s10h * gx + s11h * gy);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        const float ax = c0x + (float)a * s00h, ay = c0y + (float)a * s10h;
+        const float ax = a == 0 ? cx - s00h : a == 1 ? cx : cx + s00h;
+        const float ay = a == 0 ? cy - s10h : a == 1 ? cy : cy + s10h;
 #pragma unroll
         for (int b = 0; b < 3; b++) {
             const float W = wx[a] * wy[b];
-            sink(a, b, W, W * mass, ax + (float)b * s01h, ay + (float)b * s11h);
+            const float tx = b == 0 ? ax - s01h : b == 1 ? ax : ax + s01h;
+            const float ty = b == 0 ? ay - s11h : b == 1 ? ay : ay + s11h;
+            sink(a, b, W, W * mass, tx, ty);
         }
     }
 }
 
 template <bool AOS>
 static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags, int2 *tlist, unsigned *tlist_n,
-                                                   int inst, int ntx, int halo, float h, int bx, int by, float fx,
-                                                   float fy, float mass, float mvx, float mvy, float s00, float s01,
+                                                   int inst, int ntx, int halo, float h, int bx, int by, float gx,
+                                                   float gy, float mass, float mvx, float mvy, float s00, float s01,
                                                    float s10, float s11)
 {
-    point_contributions_f32(h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
+    point_contributions_f32(h, gx, gy, mass, mvx, mvy, s00, s01, s10, s11,
                             [&](int a, int b, float W, float dm, float tx, float ty) {
                                 g.add<AOS>(g.idx(bx + a, by + b), dm, W * tx, W * ty);
                             });
@@ -370,11 +425,47 @@ static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags,
     }
 }
 
+// Cells of a tile in the order the cell phase takes them: by point count,
+// largest first, so that the 32 cells of a warp hold about the same number of
+// points (the warp's loop runs as long as its fullest cell; in input order a
+// warp's fullest cell holds about twice the mean).  rank[c] = (count bucket
+// << 16) | rank of cell c within its bucket, from shared atomics on hist; the
+// first warp then turns the buckets into perm (position -> cell).  Any order
+// gives the same sums: each cell's partials have a fixed place.
+constexpr int CNT_BUCKETS = 16;
+// every thread of the tile (tid < TT): its cell's count
+__device__ __forceinline__ void cell_order_count(int (&hist)[CNT_BUCKETS], int (&rank)[TT], int tid, int cnt)
+{
+    const int b = CNT_BUCKETS - 1 - min(cnt, CNT_BUCKETS - 1);   // largest first
+    rank[tid] = (b << 16) | atomicAdd(hist + b, 1);
+}
+// the first warp, after a barrier that follows every count
+__device__ __forceinline__ void cell_order_build(int (&hist)[CNT_BUCKETS], const int (&rank)[TT], int (&perm)[TT],
+                                                 int lane)
+{
+    const int h = lane < CNT_BUCKETS ? hist[lane] : 0;
+    int x = h;
+#pragma unroll
+    for (int o = 1; o < CNT_BUCKETS; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    const int off = x - h;   // exclusive prefix of the bucket
+    __syncwarp();
+    if (lane < CNT_BUCKETS) hist[lane] = 0;   // ready for the next tile
+#pragma unroll
+    for (int c = lane; c < TT; c += 32) {
+        const int r = rank[c];
+        perm[__shfl_sync(0xffffffffu, off, r >> 16) + (r & 0xffff)] = c;
+    }
+}
+
 // phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32
 template <int NT, bool AOS, typename Sync>
 __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int tid, int tx, int ty, int cs, int ce,
-                                                        const int *s_cs, float *mom, float (*s_odd)[RN],
-                                                        unsigned &touch, unsigned &moved, Sync &&sync)
+                                                        const int *s_cs, const int *s_perm, float *mom,
+                                                        float (*s_odd)[RN], unsigned &touch, unsigned &moved,
+                                                        Sync &&sync)
 {
     const StepParams &P = A.P;
     const int X0 = tx * TX - P.halo, Y0 = ty * TY;
@@ -383,21 +474,20 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
 #pragma unroll
     for (int q = 0; q < 27; q++) acc[q] = 0.f;
     if (tid < TT) {
-        const int bxc = X0 + tid / TY, byc = Y0 + tid % TY;
-        const int r0 = max(s_cs[tid], cs) - cs, r1 = min(s_cs[tid + 1], ce) - cs;
+        const int cell = s_perm[tid];
+        const unsigned pbc = split_pack(X0 + cell / TY, Y0 + cell % TY);
+        const int r0 = max(s_cs[cell], cs) - cs, r1 = min(s_cs[cell + 1], ce) - cs;
         const MomF M(mom);
         for (int j = r0; j < r1; j++) {
             const int c = momf_col(j);
             const float2 q2 = M.m2[c];
-            const int pb = __float_as_int(q2.y);
-            if (pb == BASE_NONE) continue;
-            int bx, by;
-            unpack_base(pb, bx, by);
+            const unsigned pb = __float_as_uint(q2.y);
+            if (pb == (unsigned)BASE_NONE) continue;
             const float4 q0 = M.m0[c], q1 = M.m1[c];
-            const float fx = q0.x, fy = q0.y, mass = q0.z, mvx = q0.w, mvy = q1.x;
+            const float gx = q0.x, gy = q0.y, mass = q0.z, mvx = q0.w, mvy = q1.x;
             const float s00 = q1.y, s01 = q1.z, s10 = q1.w, s11 = q2.x;
-            if (bx == bxc && by == byc) {
-                point_contributions_f32(A.Q.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
+            if (pb == pbc) {
+                point_contributions_f32(A.Q.h, gx, gy, mass, mvx, mvy, s00, s01, s10, s11,
                                         [&](int a, int b, float W, float dm, float tx, float ty) {
                                             const int q = (a * 3 + b) * 3;
                                             acc[q] += dm;
@@ -406,9 +496,11 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                                         });
             } else {
                 moved++;
+                int bx, by;
+                split_unpack(pb, bx, by);
                 const int lx = bx - RX0, ly = by - RY0;
                 if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
-                    point_contributions_f32(A.Q.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
+                    point_contributions_f32(A.Q.h, gx, gy, mass, mvx, mvy, s00, s01, s10, s11,
                                             [&](int a, int b, float W, float dm, float tx, float ty) {
                                                 const int k = (lx + a) * RY + (ly + b);
                                                 atomicAdd(&s_odd[0][k], dm);
@@ -416,8 +508,8 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                                                 atomicAdd(&s_odd[2][k], W * ty);
                                             });
                 } else {
-                    p2g_global_f32<AOS>(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by, fx, fy, mass, mvx, mvy, s00, s01,
-                                   s10, s11);
+                    p2g_global_f32<AOS>(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by,
+                                        gx, gy, mass, mvx, mvy, s00, s01, s10, s11);
                 }
             }
         }
@@ -425,8 +517,9 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
     sync();
     float4 *part = reinterpret_cast<float4 *>(mom);   // [9 node offsets][TT cells], aliasing the moments
     if (tid < TT) {
+        const int cell = s_perm[tid];
 #pragma unroll
-        for (int q = 0; q < 9; q++) part[q * TT + tid] = make_float4(acc[3 * q], acc[3 * q + 1], acc[3 * q + 2], 0.f);
+        for (int q = 0; q < 9; q++) part[q * TT + cell] = make_float4(acc[3 * q], acc[3 * q + 1], acc[3 * q + 2], 0.f);
     }
     sync();
     for (int k = tid; k < RN; k += NT) {
@@ -461,12 +554,15 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
 
 // Threads and resident CTAs per SM of the FP32 tile kernel.
 constexpr int TILE_THREADS_F32 = 256, TILE_CTAS_F32 = 3;
+static_assert(TILE_THREADS_F32 == TT, "one thread per cell of a tile in the cell phase");
 
 // Work items of a batch: (instance, tile) pairs over all instances.
 struct BatchItem { int inst, tile; };
 
-// Starts moving the next work item's point lines (line `which` < S_JP + 1) or
-// cell ranges (which == S_JP + 1) into L2 while this CTA is in its cell phase.
+// Starts moving the next work item's hot state (pieces which < 8 of its
+// contiguous block range) or cell ranges (which == 8) into L2 while this CTA
+// is in its cell phase.
+constexpr int PF_PIECES = 8;
 template <bool BATCH>
 __device__ __forceinline__ void prefetch_next_item(const SplitArgs &A1, const SplitArgs *Aarr, const BatchItem *work,
                                                    int next, int na, int which)
@@ -475,12 +571,15 @@ __device__ __forceinline__ void prefetch_next_item(const SplitArgs &A1, const Sp
     const BatchItem w = BATCH ? work[next] : BatchItem{0, A1.active[next]};
     const SplitArgs &A = BATCH ? Aarr[w.inst] : A1;
     const int *cs = A.cell_start + (long)w.tile * TT;
-    if (which == S_JP + 1) {
+    if (which == PF_PIECES) {
         prefetch_l2(cs, (TT + 1) * sizeof(int));
         return;
     }
     const int ps = cs[0], pe = cs[TT];
-    if (pe > ps) prefetch_l2(A.st + A.pitch * which + ps, (size_t)(pe - ps) * sizeof(unsigned));
+    if (pe <= ps) return;
+    const int b0 = ps >> 5, nb = ((pe - 1) >> 5) + 1 - b0;
+    const int k0 = b0 + nb * which / PF_PIECES, k1 = b0 + nb * (which + 1) / PF_PIECES;
+    if (k1 > k0) prefetch_l2(A.st + (long)k0 * HOT_WORDS, (size_t)(k1 - k0) * HOT_WORDS * sizeof(unsigned));
 }
 
 // Tile kernel over the FP32 state: <G2P, P2G, write vel/Bp> as k_tile.
@@ -495,6 +594,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     __shared__ float2 s_v[RN];
     __shared__ float s_odd[3][RN];
     __shared__ int s_cs[TT + 1];
+    __shared__ int s_hist[CNT_BUCKETS], s_rank[TT], s_perm[TT];
     __shared__ unsigned s_touch;
     __shared__ int s_claim;
     extern __shared__ float4 s_momf4[];
@@ -507,6 +607,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     // its next item when it starts one, so that the CTAs finish together (4 %).
     if (BATCH && tid == 0) s_claim = atomicAdd(A1.claim, 1);
     for (int k = tid; k < RN; k += blockDim.x) { s_odd[0][k] = 0.f; s_odd[1][k] = 0.f; s_odd[2][k] = 0.f; }
+    if (tid < CNT_BUCKETS) s_hist[tid] = 0;
     __syncthreads();
     int ti = BATCH ? s_claim : (int)blockIdx.x;
     __syncthreads();   // everybody has read s_claim; later reads of it come before the item's last barrier
@@ -520,12 +621,18 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
 #endif
         const StepParams &P = A.P;
         const bool record = BATCH ? rec[w.inst] != 0 : A.record_pq != 0;
-        const float *fst = reinterpret_cast<const float *>(A.st);
         unsigned moved = 0;
         const int t = w.tile;
         const int tx = t % A.G.ntx, ty = t / A.G.ntx;
         const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
-        for (int c = tid; c <= TT; c += blockDim.x) s_cs[c] = A.cell_start[(long)t * TT + c];
+        {
+            // cell ranges; each thread counts its own cell's points for the cell order
+            const int *cst = A.cell_start + (long)t * TT;
+            const int c0 = cst[tid], c1 = cst[tid + 1];
+            s_cs[tid] = c0;
+            if (tid == TT - 1) s_cs[TT] = c1;
+            if (DO_P2G) cell_order_count(s_hist, s_rank, tid, c1 - c0);
+        }
         if (tid == 0) s_touch = 0;
         if (DO_G2P) {
             for (int k = tid; k < RN; k += blockDim.x) {
@@ -559,12 +666,10 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             for (int j = tid; j < ce - cs; j += blockDim.x) {
                 const long i = cs + j;
                 PointF s;
-                s.util = A.st[i];
-                if (s.util & (unsigned)kDisabled) {
+                if (!load_point_f32(A.st, i, s)) {
                     if (DO_P2G) MomF(s_momf).none(j);
                     continue;
                 }
-                load_point_f32(A.st, A.pitch, i, s);
                 if (DO_G2P) {
                     if (!g2p_update_f32(P, A.Q, A.grain_tab, s, A.status, vsrc)) {
                         if (DO_P2G) MomF(s_momf).none(j);
@@ -572,21 +677,24 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                     }
                     store_point_f32(A.st, A.pitch, i, s, WRITE_VB, record);
                 } else {
-                    s.vx = fst[i + A.pitch * S_VX];
-                    s.vy = fst[i + A.pitch * S_VY];
-                    s.B = {fst[i + A.pitch * S_B00], fst[i + A.pitch * S_B01], fst[i + A.pitch * S_B10],
-                           fst[i + A.pitch * S_B11]};
+                    const float *c = reinterpret_cast<const float *>(A.st) + cold_vec(A.pitch, i);
+                    const float4 v = *reinterpret_cast<const float4 *>(c);
+                    const float4 b = *reinterpret_cast<const float4 *>(c + 128);
+                    s.vx = v.x;
+                    s.vy = v.y;
+                    s.B = {b.x, b.y, b.z, b.w};
                 }
                 if (DO_P2G) p2g_moments_f32(P, A.Q, s, s_momf, j, A.status);
             }
             __syncthreads();
-            // threads without a cell in the cell phase (else the last ones) start the
-            // next item's loads
-            constexpr int PF0 = TT < TILE_THREADS_F32 ? TT : TILE_THREADS_F32 - (S_JP + 2);
-            if (DO_P2G && cs == ps && tid >= PF0 && tid < PF0 + S_JP + 2)
+            // the last threads start the next item's loads: its hot state in pieces
+            // and its cell ranges
+            constexpr int PF0 = TILE_THREADS_F32 - (PF_PIECES + 1);
+            if (DO_P2G && cs == ps && tid >= PF0)
                 prefetch_next_item<BATCH>(A1, Aarr, work, next, na, tid - PF0);
             // and the first threads its staged node velocities (columns of vx and vy,
             // or of the float2 velocities of a batch member)
+            static_assert(2 * RX <= PF0, "velocity-column and state prefetches on different threads");
             if (DO_G2P && DO_P2G && cs == ps && tid < (BATCH ? 1 : 2) * RX && next < na) {
                 const BatchItem wn = BATCH ? work[next] : BatchItem{0, A1.active[next]};
                 const SplitArgs &An = BATCH ? Aarr[wn.inst] : A1;
@@ -597,9 +705,15 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                     prefetch_region_column(tid < RX ? An.g.vx : An.g.vy, An.P.gridx, An.P.gridy, An.P.halo, An.g.ny,
                                            nx0, ny0, tid % RX);
             }
-            if (DO_P2G)
-                p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH>(A, tid, tx, ty, cs, ce, s_cs, s_momf, s_odd, touch, moved,
-                                                      [] { __syncthreads(); });
+            if (DO_P2G) {
+                if (cs == ps) {
+                    // the cell order, by the first warp while the point loop's registers are free
+                    if (tid < 32) cell_order_build(s_hist, s_rank, s_perm, tid);
+                    __syncthreads();
+                }
+                p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH>(A, tid, tx, ty, cs, ce, s_cs, s_perm, s_momf, s_odd,
+                                                                 touch, moved, [] { __syncthreads(); });
+            }
         }
         if (DO_P2G) {
             touch = __reduce_or_sync(0xffffffffu, touch);
@@ -689,21 +803,17 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
                                                                 double ind_x, double ind_y);
 
 // ---------------------------------------------------------------- binning / conversion
-static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__restrict__ st, long pitch, int n,
-                                int *keys, int *ranks, int *counts, int *status)
+static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__restrict__ st, int n, int *keys,
+                                       int *ranks, int *counts, int *status)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = i < n;
     int key = G.ntiles * TT;
     if (in) {
-        const unsigned u = st[i];
-        if (!(u & (unsigned)kDisabled)) {
-            int cx, cy, bx, by;
-            float fx, fy;
-            unpack_cell(st[i + pitch * S_CELL], cx, cy);
-            const float *f = reinterpret_cast<const float *>(st);
-            split_base(cx, f[i + pitch * S_OX], bx, fx);
-            split_base(cy, f[i + pitch * S_OY], by, fy);
+        const uint4 a = *reinterpret_cast<const uint4 *>(hot_vec(st, i));
+        if (!(a.w & (unsigned)kDisabled)) {
+            int bx, by;
+            split_unpack(a.x, bx, by);
             const int e = base_error(P, bx, by);
             if (e) *status = e;
             else key = G.cell_key(bx, by, P.halo);
@@ -721,77 +831,82 @@ static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned 
 }
 
 static __global__ void k_bin_scatter_f32(const unsigned *__restrict__ src, unsigned *__restrict__ dst, long pitch, int n,
-                                  const int *__restrict__ keys, const int *__restrict__ ranks,
-                                  const int *__restrict__ start, const int *__restrict__ oidx_src,
-                                  int *__restrict__ oidx_dst)
+                                         const int *__restrict__ keys, const int *__restrict__ ranks,
+                                         const int *__restrict__ start, const int *__restrict__ oidx_src,
+                                         int *__restrict__ oidx_dst)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int d = start[keys[i]] + ranks[i];
-#pragma unroll
-    for (int l = 0; l < S_NLINES; l++) dst[d + pitch * l] = src[i + pitch * l];
+    const long d = start[keys[i]] + ranks[i];
+    *reinterpret_cast<uint4 *>(hot_vec(dst, d)) = *reinterpret_cast<const uint4 *>(hot_vec(src, i));
+    *reinterpret_cast<uint4 *>(hot_vec(dst, d) + 128) = *reinterpret_cast<const uint4 *>(hot_vec(src, i) + 128);
+    dst[hot_jp(d)] = src[hot_jp(i)];
+    *reinterpret_cast<uint4 *>(dst + cold_vec(pitch, d)) = *reinterpret_cast<const uint4 *>(src + cold_vec(pitch, i));
+    *reinterpret_cast<uint4 *>(dst + cold_vec(pitch, d) + 128) =
+        *reinterpret_cast<const uint4 *>(src + cold_vec(pitch, i) + 128);
     oidx_dst[d] = oidx_src[i];
 }
 
 // FP64 HSSOA chunk (16 lines, stride cpitch) -> FP32 state slots [first, first+count)
 static __global__ void k_split_from_hssoa(const double *__restrict__ chunk, long cpitch, int count, unsigned *st,
-                                   long pitch, int first, double hinv)
+                                          long pitch, int first, double hinv)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
     const long i = first + j;
-    float *f = reinterpret_cast<float *>(st);
     auto L = [&](int l) { return chunk[j + cpitch * l]; };
-    st[i] = (unsigned)(unsigned long long)__double_as_longlong(L(0));
-    int c[2];
-    float o[2];
+    int b[2];
+    float g[2];
     for (int k = 0; k < 2; k++) {
-        const double xs = L(4 + k) * hinv;
-        const double fl = floor(xs);
-        c[k] = (int)fl;
-        o[k] = (float)(xs - fl);
-        if (o[k] >= 1.0f) { c[k] += 1; o[k] = 0.0f; }
+        const double xs = L(4 + k) * hinv;                // pos * cellsize_inv (kernels.cuh:90)
+        b[k] = (int)(xs - 0.5);
+        g[k] = (float)(xs - (double)b[k] - 1.0);
     }
-    st[i + pitch * S_CELL] = pack_cell(c[0], c[1]);
-    f[i + pitch * S_OX] = o[0];
-    f[i + pitch * S_OY] = o[1];
-    f[i + pitch * S_D00] = (float)(L(8) - 1.0);
-    f[i + pitch * S_D01] = (float)L(9);
-    f[i + pitch * S_D10] = (float)L(10);
-    f[i + pitch * S_D11] = (float)(L(11) - 1.0);
-    f[i + pitch * S_JP] = (float)L(3);
-    f[i + pitch * S_VX] = (float)L(6);
-    f[i + pitch * S_VY] = (float)L(7);
-    for (int k = 0; k < 4; k++) f[i + pitch * (S_B00 + k)] = (float)L(12 + k);
-    f[i + pitch * S_P] = (float)L(1);
-    f[i + pitch * S_Q] = (float)L(2);
+    PointF s;
+    s.bw = split_pack(b[0], b[1]);
+    s.gx = g[0];
+    s.gy = g[1];
+    s.util = (unsigned)(unsigned long long)__double_as_longlong(L(0));
+    s.D = {(float)(L(8) - 1.0), (float)L(9), (float)L(10), (float)(L(11) - 1.0)};
+    s.Jp = (float)L(3);
+    s.vx = (float)L(6);
+    s.vy = (float)L(7);
+    s.B = {(float)L(12), (float)L(13), (float)L(14), (float)L(15)};
+    s.ptr = (float)L(1);
+    s.qtr = (float)L(2);
+    store_point_f32(st, pitch, i, s, true, true);
 }
 
 // FP32 state -> FP64 HSSOA chunk of upload positions [first, first+count);
 // inv[o] is the slot holding the point uploaded at position o.
-static __global__ void k_split_to_hssoa(const unsigned *__restrict__ st, long pitch, const int *__restrict__ inv, int first,
-                                 int count, double *__restrict__ chunk, long cpitch, double h)
+static __global__ void k_split_to_hssoa(const unsigned *__restrict__ st, long pitch, const int *__restrict__ inv,
+                                        int first, int count, double *__restrict__ chunk, long cpitch, double h)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= count) return;
     const long i = inv ? inv[first + j] : first + j;
-    const float *f = reinterpret_cast<const float *>(st);
     auto W = [&](int l, double v) { chunk[j + cpitch * l] = v; };
-    W(0, __longlong_as_double((long long)st[i]));
-    int cx, cy;
-    unpack_cell(st[i + pitch * S_CELL], cx, cy);
-    W(4, ((double)cx + (double)f[i + pitch * S_OX]) * h);
-    W(5, ((double)cy + (double)f[i + pitch * S_OY]) * h);
-    W(8, 1.0 + (double)f[i + pitch * S_D00]);
-    W(9, (double)f[i + pitch * S_D01]);
-    W(10, (double)f[i + pitch * S_D10]);
-    W(11, 1.0 + (double)f[i + pitch * S_D11]);
-    W(3, (double)f[i + pitch * S_JP]);
-    W(6, (double)f[i + pitch * S_VX]);
-    W(7, (double)f[i + pitch * S_VY]);
-    for (int k = 0; k < 4; k++) W(12 + k, (double)f[i + pitch * (S_B00 + k)]);
-    W(1, (double)f[i + pitch * S_P]);
-    W(2, (double)f[i + pitch * S_Q]);
+    PointF s;
+    load_point_f32(st, i, s);
+    const float *c = reinterpret_cast<const float *>(st) + cold_vec(pitch, i);
+    const float4 v = *reinterpret_cast<const float4 *>(c);
+    const float4 bp = *reinterpret_cast<const float4 *>(c + 128);
+    W(0, __longlong_as_double((long long)s.util));
+    W(4, ((double)s.bx + 1.0 + (double)s.gx) * h);
+    W(5, ((double)s.by + 1.0 + (double)s.gy) * h);
+    W(8, 1.0 + (double)s.D.a00);
+    W(9, (double)s.D.a01);
+    W(10, (double)s.D.a10);
+    W(11, 1.0 + (double)s.D.a11);
+    W(3, (double)s.Jp);
+    W(6, (double)v.x);
+    W(7, (double)v.y);
+    W(12, (double)bp.x);
+    W(13, (double)bp.y);
+    W(14, (double)bp.z);
+    W(15, (double)bp.w);
+    W(1, (double)v.z);
+    W(2, (double)v.w);
 }
 
 static __global__ void k_inverse_perm(const int *__restrict__ oidx, int n, int *__restrict__ inv)
