@@ -28,6 +28,7 @@ ICY_ERR_CAPACITY = 106
 ICY_ERR_POINT_COUNT = 107
 ICY_ERR_TIMEOUT = 108
 ICY_ERR_NOT_SUPPORTED = 109
+ICY_ERR_DRIFT = 110
 
 PRECISION_FP64 = 0
 PRECISION_FP32_SPLIT = 1
@@ -89,7 +90,7 @@ EXPORTED = [
     "icy_batch_collect", "icy_batch_wait_steps", "icy_batch_remove", "icy_batch_step",
     "icy_batch_download", "icy_batch_synchronize", "icy_batch_set_option", "icy_batch_info",
     "icy_batch_device_bytes", "icy_mpm_device_bytes", "icy_scene_place", "icy_host_alloc", "icy_host_free",
-    "icy_batch_set_clock",
+    "icy_batch_set_clock", "icy_mpm_counters",
 ]
 
 _lib = None
@@ -136,6 +137,7 @@ def lib():
         "icy_mpm_synchronize": (C.c_int, [vp]),
         "icy_mpm_status": (C.c_int, [vp]),
         "icy_mpm_kernel_launches": (C.c_int64, [vp]),
+        "icy_mpm_counters": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "icy_mpm_profile": (C.c_int, [vp, C.c_int]),
         "icy_mpm_set_option": (C.c_int, [vp, C.c_char_p, C.c_double]),
         "icy_mpm_profile_read": (C.c_int, [vp, C.c_int, C.c_char_p, vp, vp, C.POINTER(C.c_int)]),

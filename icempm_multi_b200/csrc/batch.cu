@@ -226,7 +226,8 @@ int64_t icy_mpm_device_bytes(const icy_sim_params *p, unsigned capacity, int pre
     const long nkeys = ntiles * TT + 1;
     int64_t b = 0;
     if (precision == ICY_PRECISION_FP32_SPLIT)
-        b += 2 * (int64_t)S_NLINES * 4 * pitch + 16 * 8 * (int64_t)std::min(pitch, 1L << 20) + 6 * 4 * (int64_t)n_nodes;
+        b += 2 * (int64_t)S_NLINES * 4 * pitch + 16 * 8 * (int64_t)std::min(pitch, 1L << 20) + 7 * 4 * (int64_t)n_nodes +
+             4 * 2 * (int64_t)ntiles + 16;
     else
         b += 2 * 16 * 8 * (int64_t)pitch + 5 * 8 * (int64_t)n_nodes;
     b += 4 * 4 * (int64_t)pitch + 4 * (2 * nkeys + 1) + 4 * 2 * ntiles + 2 * 8 * p->n_indenter_subdivisions + 65536;

@@ -253,6 +253,19 @@ int icy_mpm_status(icy_mpm *h)
 
 int64_t icy_mpm_kernel_launches(icy_mpm *h) { return h ? h->launches : 0; }
 
+int icy_mpm_counters(icy_mpm *h, int64_t *moved_points, int64_t *fused_launches, int64_t *fallback_launches)
+{
+    if (!h) return ICY_ERR_INVALID_ARGUMENT;
+    unsigned long long c[3] = {0, 0, 0};
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(c, h->d_moved, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (moved_points) *moved_points = (int64_t)c[0];
+    if (fused_launches) *fused_launches = (int64_t)c[1];
+    if (fallback_launches) *fallback_launches = (int64_t)c[2];
+    return ICY_OK;
+}
+
 int icy_mpm_set_option(icy_mpm *h, const char *name, double value)
 {
     if (!h || !name) return ICY_ERR_INVALID_ARGUMENT;
@@ -270,6 +283,8 @@ int icy_mpm_set_option(icy_mpm *h, const char *name, double value)
     } else if (k == "tiled") {
         h->tiled = value != 0;
         h->primed = false;
+    } else if (k == "fuse_update") {
+        h->fuse_update = value != 0;
     } else {
         return ICY_ERR_INVALID_ARGUMENT;
     }
@@ -301,7 +316,9 @@ void icy_prof_begin(icy_mpm *h, int kernel)
     h->prof_cur = false;
     if (!h->profiling) return;
     if (h->prof_seen.size() != K_N_KERNELS) h->prof_seen.assign(K_N_KERNELS, 0);
-    if (h->prof_seen[kernel]++ % h->prof_every != 0) return;   // not a sampled launch
+    // every re-binning is timed (it is rare, and its share of a step is amortised
+    // from its own time); other kernels every prof_every-th launch
+    if (h->prof_seen[kernel]++ % h->prof_every != 0 && kernel != K_BIN) return;   // not a sampled launch
     icy_mpm::ProfRec r{kernel, pool_get(h), pool_get(h)};
     if (!r.a || !r.b) return;
     cudaEventRecord(r.a, h->stream);

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -121,13 +122,13 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
             icy_set_error("cudaMalloc(particles)", e);
             return ICY_ERR_OUT_OF_MEMORY;
         }
-        if ((e = dalloc(h, &h->d_gridf, 6 * h->n_nodes)) != cudaSuccess) {   // either layout of GridViewF
+        if ((e = dalloc(h, &h->d_gridf, 7 * h->n_nodes)) != cudaSuccess) {   // either layout of GridViewF
             icy_set_error("cudaMalloc(grid)", e);
             return ICY_ERR_OUT_OF_MEMORY;
         }
         CK(dalloc(h, reinterpret_cast<GrainConstF **>(&h->d_grainf), GRAIN_TAB_F32));
         CK(cudaMemsetAsync(h->d_st, 0, sizeof(unsigned) * S_NLINES * h->pitch, h->stream));
-        CK(cudaMemsetAsync(h->d_gridf, 0, sizeof(float) * 6 * h->n_nodes, h->stream));
+        CK(cudaMemsetAsync(h->d_gridf, 0, sizeof(float) * 7 * h->n_nodes, h->stream));
     } else {
         if ((e = dalloc(h, &h->d_pts, 16 * h->pitch)) != cudaSuccess ||
             (e = dalloc(h, &h->d_pts_alt, 16 * h->pitch)) != cudaSuccess) {
@@ -155,7 +156,10 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(dalloc(h, &h->d_flags, h->ntiles));
     CK(dalloc(h, &h->d_tlist, h->ntiles));
     CK(dalloc(h, &h->d_tlist_n, 2));
-    CK(dalloc(h, &h->d_moved, 1));
+    CK(dalloc(h, &h->d_nexp, h->ntiles));
+    CK(dalloc(h, &h->d_ncnt, h->ntiles));
+    CK(dalloc(h, &h->d_unsafe, 2));
+    CK(dalloc(h, &h->d_moved, 3));
     CK(dalloc(h, &h->d_acc, 2 * h->prm.n_indenter_subdivisions));
     CK(dalloc(h, &h->d_status, 1));
     CK(dalloc(h, &h->d_grain, GRAIN_TAB));
@@ -163,8 +167,11 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     if (!h->h_status) return ICY_ERR_OUT_OF_MEMORY;
     CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
     CK(cudaMemsetAsync(h->d_tlist_n, 0, sizeof(unsigned) * 2, h->stream));
+    CK(cudaMemsetAsync(h->d_nexp, 0, sizeof(int) * h->ntiles, h->stream));
+    CK(cudaMemsetAsync(h->d_ncnt, 0, sizeof(int) * h->ntiles, h->stream));
+    CK(cudaMemsetAsync(h->d_unsafe, 0xff, sizeof(int) * 2, h->stream));
     CK(cudaMemsetAsync(h->d_nactive, 0, sizeof(int), h->stream));
-    CK(cudaMemsetAsync(h->d_moved, 0, sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->d_moved, 0, sizeof(unsigned long long) * 3, h->stream));
     CK(cudaMemsetAsync(h->d_acc, 0, sizeof(double) * 2 * h->prm.n_indenter_subdivisions, h->stream));
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
     // persistent grid sizes
@@ -198,7 +205,7 @@ void icy_instance_free(icy_mpm *h, bool trim)
     void *ptrs[] = {h->d_pts, h->d_pts_alt, h->d_grid, h->d_oidx, h->d_oidx_alt, h->d_keys, h->d_ranks,
                     h->d_counts, h->d_start, h->d_active, h->d_nactive, h->d_flags, h->d_moved, h->d_acc,
                     h->d_status, h->d_block_sums, h->d_grain, h->d_st, h->d_st_alt, h->d_stage, h->d_gridf,
-                    h->d_grainf, h->d_tlist, h->d_tlist_n};
+                    h->d_grainf, h->d_tlist, h->d_tlist_n, h->d_nexp, h->d_ncnt, h->d_unsafe};
     cudaStream_t fs = h->stream ? h->stream : h->own_stream;
     for (void *p : ptrs)
         if (p) cudaFreeAsync(p, fs);   // back to the pool, after the stream's work
@@ -220,6 +227,7 @@ void icy_instance_free(icy_mpm *h, bool trim)
     h->d_flags = nullptr;
     h->d_tlist = nullptr;
     h->d_tlist_n = nullptr;
+    h->d_nexp = h->d_ncnt = h->d_unsafe = nullptr;
     h->d_moved = nullptr;
     h->d_grain = nullptr;
     h->own_stream = h->stream = nullptr;
@@ -316,6 +324,15 @@ int icy_instance_bin(icy_mpm *h)
     k_tiles_active<<<1, 1024, 0, h->stream>>>(h->d_start, h->ntiles, h->d_active, h->d_nactive);
     CK_LAUNCH("k_tiles_active");
     if (is_split(h)) {
+        // fused grid update: contributors per node tile for this binning, counts and
+        // margin flags from zero
+        k_node_tile_expect<<<(h->ntiles + 255) / 256, 256, 0, h->stream>>>(tile_geom(h), h->d_start, h->d_nexp);
+        CK_LAUNCH("k_node_tile_expect");
+        CK(cudaMemsetAsync(h->d_ncnt, 0, sizeof(int) * h->ntiles, h->stream));
+        CK(cudaMemsetAsync(h->d_unsafe, 0xff, sizeof(int) * 2, h->stream));
+        h->fuse_seq = 0;
+    }
+    if (is_split(h)) {
         k_bin_scatter_f32<<<nb, 256, 0, h->stream>>>(h->d_st, h->d_st_alt, h->pitch, (int)h->n, h->d_keys,
                                                      h->d_ranks, h->d_start, h->d_oidx, h->d_oidx_alt);
         std::swap(h->d_st, h->d_st_alt);
@@ -361,8 +378,11 @@ static GridViewF grid_view_f32(icy_mpm *h)
     g.m = h->d_gridf;
     g.px = h->d_gridf + h->n_nodes;
     g.py = h->d_gridf + 2 * h->n_nodes;
-    g.vx = h->d_gridf + 3 * h->n_nodes;
-    g.vy = h->d_gridf + 4 * h->n_nodes;
+    // two velocity buffers: G2P reads buffer vpar, the grid update writes the other
+    float *v0 = h->d_gridf + 3 * h->n_nodes, *v1 = h->d_gridf + 5 * h->n_nodes;
+    g.vx = h->vpar ? v1 : v0;
+    g.vy = g.vx + h->n_nodes;
+    g.nvx = h->vpar ? v0 : v1;
     g.mp = reinterpret_cast<float4 *>(h->d_gridf);               // 16-byte aligned (pool blocks: 256 B)
     g.v = reinterpret_cast<float2 *>(h->d_gridf + 4 * h->n_nodes);
     g.ny = h->prm.GridY;
@@ -393,12 +413,53 @@ static SplitArgs split_args(icy_mpm *h, bool record)
     A.record_pq = record ? 1 : 0;
     A.acc = h->d_acc;
     A.n_nodes = h->n_nodes;
+    A.nexp = h->d_nexp;
+    A.ncnt = h->d_ncnt;
+    A.unsafe = h->d_unsafe;
+    A.seq = 0;
+    A.safe_m = 0.f;
+    A.ind_x = A.ind_y = 0.0;
     return A;
 }
 
-static int launch_tile_split(icy_mpm *h, int which, bool record)
+// CTAs of the list-driven update queued after a fused tile launch: it has no
+// work unless the tile kernel fell back to marking tiles, which a re-binning
+// soon ends, so a small grid keeps its empty launch cheap.
+static int fallback_ctas(icy_mpm *h)
+{
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    return std::max(1, std::min(h->update_grid, sms));
+}
+
+// Largest move of a point in one step, in cells: the grid update clamps node
+// speeds to vmax = 0.5 h / dt, and the indenter can add twice its own speed;
+// a margin for rounding on top.
+static double step_move_cells(const icy_sim_params &p)
+{
+    return 0.5 + 2.0 * std::fabs(p.IndVelocity) * p.InitialTimeStep * p.cellsize_inv + 1e-3;
+}
+
+// which: 0 = G2P + P2G, 1 = P2G only, 2 = G2P only (writes vel and Bp).
+// A G2P + P2G launch also updates the grid for the next step (indenter at
+// (ind_x, ind_y)) where it is safe to (see k_tile_f32), the list-driven
+// update queued after it doing the rest.
+static int launch_tile_split(icy_mpm *h, int which, bool record, double ind_x = 0.0, double ind_y = 0.0)
 {
     SplitArgs A = split_args(h, record);
+    if (which != 2 && h->fuse_update) {
+        // every launch with a P2G tests whether a point can leave the staged margin
+        // in the step after it (the P2G-only launch that starts a call too, so that
+        // the test covers every step a fused launch follows); only G2P + P2G
+        // launches fuse the update
+        const double delta = step_move_cells(h->prm);
+        if (delta < 1.0) {   // beyond one cell a point that has not moved could leave the margin
+            A.seq = ++h->fuse_seq;
+            A.safe_m = (float)(1.5 - delta);
+            A.ind_x = ind_x;
+            A.ind_y = ind_y;
+        }
+    }
     switch (which) {
     case 0:
         icy_prof_begin(h, K_TILE_G2P2G);
@@ -419,14 +480,14 @@ static int launch_tile_split(icy_mpm *h, int which, bool record)
 }
 
 // which: 0 = G2P+P2G, 1 = P2G only, 2 = G2P only (writes vel and Bp)
-static int launch_tile(icy_mpm *h, int which, bool record)
+static int launch_tile(icy_mpm *h, int which, bool record, double ind_x = 0.0, double ind_y = 0.0)
 {
     if (!h->n) return ICY_OK;
     if (!h->binned) {
         int rc = icy_instance_bin(h);
         if (rc) return rc;
     }
-    if (is_split(h)) return launch_tile_split(h, which, record);
+    if (is_split(h)) return launch_tile_split(h, which, record, ind_x, ind_y);
     TileArgs A = tile_args(h, record);
     switch (which) {
     case 0:
@@ -448,14 +509,18 @@ static int launch_tile(icy_mpm *h, int which, bool record)
     return ICY_OK;
 }
 
-static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y)
+// The list-driven grid update.  FP32: it writes the velocity buffer G2P does
+// not read, and the buffers swap after it (also after a fused launch, whose
+// update it completes); `ctas` = 0: the usual grid.
+static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y, int ctas = 0)
 {
     StepParams P = icy_step_params(h->prm);
     icy_prof_begin(h, K_UPDATE_TILES);
-    if (is_split(h))
-        k_update_list_f32<false><<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
+    if (is_split(h)) {
+        k_update_list_f32<false><<<ctas > 0 ? ctas : h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
             split_args(h, false), nullptr, nullptr, h->d_tlist, h->d_tlist_n, ind_x, ind_y);
-    else
+        h->vpar ^= 1;
+    } else
         k_update_list<<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
             P, tile_geom(h), grid_view(h), h->d_flags, h->d_tlist, h->d_tlist_n, ind_x, ind_y, h->d_acc);
     icy_prof_end(h);
@@ -553,6 +618,38 @@ int icy_instance_steps(icy_mpm *h, int step0, int nsteps, double *sim_time)
         return ICY_OK;
     }
     if (nsteps == 0) return ICY_OK;
+    if (is_split(h)) {
+        // FP32: P2G(first) and its update, then [G2P(k) + P2G(k+1) + update(k+1)]
+        // per step (the update fused into the tile kernel where safe, the list
+        // update after it completing it otherwise), last G2P alone.  Each update
+        // takes the indenter position of its own sub-step, t += dt;
+        // indenter_x = x0 + t V (simulation/model.cpp:40-41).
+        if (!h->primed) {
+            const double t1 = t + p.InitialTimeStep;
+            if ((rc = launch_tile(h, 1, false))) return rc;
+            if ((rc = launch_update_tiles(h, p.indenter_x_initial + t1 * p.IndVelocity, p.indenter_y))) return rc;
+            h->primed = true;
+        }
+        for (int k = 0; k < nsteps; k++) {
+            t += p.InitialTimeStep;
+            const bool rec = ((step0 + k) % p.UpdateEveryNthStep) == 0;
+            if (k == nsteps - 1) {
+                if ((rc = launch_tile(h, 2, rec))) return rc;
+                h->primed = false;
+            } else {
+                const double tn = t + p.InitialTimeStep;
+                const double ind_x = p.indenter_x_initial + tn * p.IndVelocity;
+                if ((rc = launch_tile(h, 0, rec, ind_x, p.indenter_y))) return rc;
+                // the fused update's fallback: empty unless the tile kernel marked tiles
+                if ((rc = launch_update_tiles(h, ind_x, p.indenter_y, h->fuse_update ? fallback_ctas(h) : 0)))
+                    return rc;
+                if (h->resort_every > 0 && ++h->steps_since_bin >= h->resort_every)
+                    if ((rc = icy_instance_bin(h))) return rc;
+            }
+        }
+        *sim_time = t;
+        return ICY_OK;
+    }
     // tiled path: P2G(first), then [update(k); G2P(k)+P2G(k+1)] ..., last G2P alone
     if (!h->primed) {
         if ((rc = launch_tile(h, 1, false))) return rc;

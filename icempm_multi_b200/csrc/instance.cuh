@@ -38,7 +38,12 @@ struct icy_mpm {
     unsigned *d_st = nullptr, *d_st_alt = nullptr;
     double *d_stage = nullptr;
     long stage_n = 0;
-    float *d_gridf = nullptr;
+    float *d_gridf = nullptr;       // m, px, py, then two velocity buffers (vx, vy each)
+    int vpar = 0;                   // which velocity buffer G2P reads (the update writes the other)
+    int *d_nexp = nullptr, *d_ncnt = nullptr;   // fused grid update: per node tile expected / finished
+    int *d_unsafe = nullptr;        // [2] margin flags of the last launches, by parity
+    int fuse_seq = 0;               // fused-capable launches since the last binning
+    bool fuse_update = false;       // grid update fused into the tile kernel where safe (option "fuse_update")
     void *d_grainf = nullptr;
     int tile_grid_f32 = 0;
     icy_dev::GrainConst *d_grain = nullptr;   // failure-surface constants per grain slot

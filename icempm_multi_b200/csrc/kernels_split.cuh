@@ -39,6 +39,9 @@ constexpr int HOT_WORDS = 9 * SB;        // words of a block's hot part
 constexpr int COLD_WORDS = 8 * SB;       // words of a block's cold part
 constexpr int S_NLINES = 17;             // words per point, hot + cold
 constexpr int S_HOT = 9;                 // the cold part starts at word S_HOT * pitch
+// Device error code of a fused launch in which a point left the staged
+// margin (ICY_ERR_DRIFT): the margin test of the launch before excludes it.
+constexpr int ICY_DRIFT_CODE = 110;
 
 struct GrainConstF { float pmin2, k, msq, pad; };
 
@@ -320,7 +323,9 @@ __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const Split
 // to look up per member and fewer live addresses (the batched kernel spills
 // less and runs 10 % faster; alone the scalar layout is 2.5 % faster).
 struct GridViewF {
-    float *m, *px, *py, *vx, *vy;   // alone
+    float *m, *px, *py, *vx, *vy;   // alone: accumulators, velocities G2P reads
+    float *nvx;                     // alone: velocities the grid update writes, the next step's vx
+                                    // (its vy follows n_nodes floats later)
     float4 *mp;                     // in a batch (same memory)
     float2 *v;
     int ny, halo;
@@ -357,14 +362,27 @@ struct SplitArgs {
     int2 *tlist;        // node tiles written since the last update, each once: (inst, tile)
     unsigned *tlist_n;  // [0] entries, [1] CTAs of the update done
     int inst;           // this instance's slot in a batch (0 alone)
+    int seq;            // fused grid update: this launch's number since the last binning (>= 1); 0 = none
     int *status;
-    unsigned long long *moved;
+    unsigned long long *moved;   // [0] points off their sorted cell (counted per P2G), [1] fused launches,
+                                 // [2] launches that fell back to the update kernel (single instance)
     int *claim;         // batch: [0] next work item to hand out, [1] CTAs finished (zero between launches)
     const GrainConstF *grain_tab;   // GRAIN_TAB_F32 entries
     int record_pq;
+    float safe_m;       // fused grid update: a point at offset u (cells) from its sorted cell stays
+                        // in the staged margin during one step if -safe_m <= u < safe_m
     double *acc;        // indenter force bins
     long n_nodes;       // nodes of the grid
+    // grid update fused into the tile kernel (single instance): each node tile
+    // is updated by the CTA that brings its count of finished neighbouring
+    // cell tiles to the expected number; see k_tile_f32
+    const int *nexp;    // per node tile: active cell tiles in its 3 x 3 neighbourhood
+    int *ncnt;          // per node tile: neighbouring cell tiles finished in this launch
+    int *unsafe;        // [2]: by launch parity, the last launch that found a point able to leave
+                        // the staged margin during the next step
+    double ind_x, ind_y;   // indenter position of the fused update
 };
+static_assert(sizeof(SplitArgs) <= 496, "128 batch members' arguments fit the 64 KB constant bank");
 
 #ifdef ICY_BATCH_CONST_ARGS
 // Only in batch_cargs.cu: the member arguments of a batch of at most
@@ -465,7 +483,7 @@ template <int NT, bool AOS, typename Sync>
 __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int tid, int tx, int ty, int cs, int ce,
                                                         const int *s_cs, const int *s_perm, float *mom,
                                                         float (*s_odd)[RN], unsigned &touch, unsigned &moved,
-                                                        Sync &&sync)
+                                                        bool fused, Sync &&sync)
 {
     const StepParams &P = A.P;
     const int X0 = tx * TX - P.halo, Y0 = ty * TY;
@@ -498,6 +516,16 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                 moved++;
                 int bx, by;
                 split_unpack(pb, bx, by);
+                if (!AOS && A.seq > 0) {
+                    // can this point leave the staged margin during the next step?  (its
+                    // offset from its sorted cell, in cells, against the largest move of a
+                    // step; near the low edges, where the base truncates, always)
+                    int sx, sy;
+                    split_unpack(pbc, sx, sy);
+                    const float ux = (float)(bx - sx) + gx, uy = (float)(by - sy) + gy;
+                    if (!(ux >= -A.safe_m && ux < A.safe_m && uy >= -A.safe_m && uy < A.safe_m) || bx <= 0 || by <= 0)
+                        A.unsafe[A.seq & 1] = A.seq;
+                }
                 const int lx = bx - RX0, ly = by - RY0;
                 if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
                     point_contributions_f32(A.Q.h, gx, gy, mass, mvx, mvy, s00, s01, s10, s11,
@@ -508,6 +536,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                                                 atomicAdd(&s_odd[2][k], W * ty);
                                             });
                 } else {
+                    if (fused) *A.status = ICY_DRIFT_CODE;   // excluded by the margin test of the last launch
                     p2g_global_f32<AOS>(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by,
                                         gx, gy, mass, mvx, mvy, s00, s01, s10, s11);
                 }
@@ -545,11 +574,95 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
         if (m != 0.f || px != 0.f || py != 0.f) {
             const int gx = RX0 + i, gy = RY0 + jj;
             A.g.add<AOS>(A.g.idx(gx, gy), m, px, py);
-            const int dx = (gx + P.halo) / TX - tx + 1, dy = gy / TY - ty + 1;
-            touch |= 1u << (dy * 3 + dx);
+            if (!fused) {
+                const int dx = (gx + P.halo) / TX - tx + 1, dy = gy / TY - ty + 1;
+                touch |= 1u << (dy * 3 + dx);
+            }
         }
     }
     sync();
+}
+
+// Grid update of one node in FP32 (simulation/kernels.cuh:175-300) from its
+// mass and momentum, the indenter geometry and the force in FP64: the new
+// velocity, and the force bin of a contact node (-1 if none).
+__device__ __forceinline__ int node_velocity_f32(const StepParams &P, const SplitConsts &Q, int gx, int gy, float mass,
+                                                 float px, float py, double ind_x, double ind_y, float &vx, float &vy,
+                                                 double &fxd, double &fyd)
+{
+    vx = 0.f;
+    vy = 0.f;
+    int bin = -1;
+    if (mass != 0.f) {
+        const float rm = __fdividef(1.f, mass);   // fast reciprocal (FP32 path)
+        vx = px * rm;
+        vy = py * rm;
+        vy -= Q.dtg;
+        const float v2 = vx * vx + vy * vy;
+        if (v2 > Q.vmax_sq) {
+            const float r = sqrtf(v2);
+            vx = vx / r * Q.vmax;
+            vy = vy / r * Q.vmax;
+        }
+        // indenter contact (kernels.cuh:264-287) decided in FP64, as the reference
+        // does; an FP32 test with a 1 mm margin (FP32 errors here are ~1e-5 m)
+        // first lets the nodes far from the indenter skip the FP64 arithmetic
+        const float ex = (float)gx * Q.h - (float)ind_x, ey = (float)gy * Q.h - (float)ind_y;
+        const float rr = sqrtf((float)P.ind_rsq) + 1e-3f;
+        double nx = 0.0, ny = 0.0;
+        if (ex * ex + ey * ey < rr * rr && ((nx = (double)gx * P.h - ind_x), (ny = (double)gy * P.h - ind_y),
+                                            nx * nx + ny * ny < P.ind_rsq)) {
+            const double r = sqrt(nx * nx + ny * ny);
+            if (r > 0) { nx /= r; ny /= r; }
+            const float fnx = (float)nx, fny = (float)ny;
+            const float vrx = vx - (float)P.ind_v, vry = vy;
+            const float vn = vrx * fnx + vry * fny;
+            if (vn < 0.f) {
+                const float vtx = vrx - fnx * vn, vty = vry - fny * vn;
+                const float pvx = vx, pvy = vy;
+                vx = (float)P.ind_v + vtx;
+                vy = vty;
+                fxd = (double)(pvx - vx) * mass / P.dt;
+                fyd = (double)(pvy - vy) * mass / P.dt;
+                float angle = atan2f(fnx, fny);
+                angle = (float)((double)angle + kPi);
+                angle = (float)((double)angle * (P.nsub / (2 * kPi)));
+                bin = min(max((int)angle, 0), P.nsub - 1);
+            }
+        }
+        if (gy <= 2) { vx = 0.f; vy = 0.f; }
+        if (gy >= P.gridy - 3 && vy > 0.f) vy = 0.f;
+        if (gx <= 2 && vx < 0.f) vx = 0.f;
+        else if (gx >= P.gridx - 3 && vx > 0.f) vx = 0.f;
+    }
+    return bin;
+}
+
+// Grid update of node tile (ntx_, nty_) by one CTA of TT threads, one node
+// each (the fused update of k_tile_f32): reads the finished sums (through L2:
+// other CTAs added them), writes the next velocities, clears the sums and
+// adds the indenter force of contact nodes to the bins.
+__device__ __forceinline__ void update_node_tile_f32(const SplitArgs &A, int ntx_, int nty_, int l)
+{
+    const StepParams &P = A.P;
+    const int gx = ntx_ * TX + l / TY - P.halo, gy = nty_ * TY + l % TY;
+    if (gx >= P.gridx + P.halo || gy >= P.gridy) return;   // past the grid edge
+    const long k = A.g.idx(gx, gy);
+    const float m = __ldcg(A.g.m + k), px = __ldcg(A.g.px + k), py = __ldcg(A.g.py + k);
+    float vx, vy;
+    double fx = 0, fy = 0;
+    const int bin = node_velocity_f32(P, A.Q, gx, gy, m, px, py, A.ind_x, A.ind_y, vx, vy, fx, fy);
+    A.g.nvx[k] = vx;
+    A.g.nvx[k + A.n_nodes] = vy;
+    if (m != 0.f || px != 0.f || py != 0.f) {
+        A.g.m[k] = 0.f;
+        A.g.px[k] = 0.f;
+        A.g.py[k] = 0.f;
+    }
+    if (bin >= 0) {
+        atomicAdd(A.acc + 2 * bin, fx);
+        atomicAdd(A.acc + 2 * bin + 1, fy);
+    }
 }
 
 // Threads and resident CTAs per SM of the FP32 tile kernel.
@@ -601,6 +714,14 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     float *const s_momf = reinterpret_cast<float *>(s_momf4);
     const int na = BATCH ? *nwork : *A1.n_active;
     const int tid = threadIdx.x;
+    // This launch updates the grid itself (see the end of the tile loop) unless
+    // the launch before found a point that could leave its tile's staged margin
+    // in this step: its contributions could then reach node tiles beyond the 3 x 3
+    // neighbourhood after they were updated, so the tiles are marked for the
+    // list-driven update that follows instead.  The flag of launch s is
+    // unsafe[s & 1]: this launch reads the other one, which nobody writes now.
+    const bool fused = !BATCH && DO_G2P && DO_P2G && A1.seq > 0 && A1.unsafe[(A1.seq - 1) & 1] != A1.seq - 1;
+    if (!BATCH && DO_G2P && DO_P2G && A1.seq > 0 && blockIdx.x == 0 && tid == 0) atomicAdd(A1.moved + (fused ? 1 : 2), 1ull);
     // Alone, CTA c takes the tiles c, c + gridDim.x, ... (equal tiles, and no
     // claim to wait for: 5 % faster).  In a batch, where the items differ in
     // size, they are handed out one at a time (A1.claim[0]), each CTA claiming
@@ -712,10 +833,47 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                     __syncthreads();
                 }
                 p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH>(A, tid, tx, ty, cs, ce, s_cs, s_perm, s_momf, s_odd,
-                                                                 touch, moved, [] { __syncthreads(); });
+                                                                 touch, moved, fused, [] { __syncthreads(); });
             }
         }
-        if (DO_P2G) {
+        if (DO_P2G && fused) {
+            // Fused grid update: this tile's sums are in; count it finished for each
+            // of the 9 node tiles around it.  The CTA that brings a node tile's count
+            // to the number of active cell tiles around it (nexp, from the binning)
+            // updates that node tile: all its contributions have landed, since in a
+            // fused launch every contribution to a node tile comes from the cell tiles
+            // around it.  Release: the CTA's reductions, barrier, then a fence and the
+            // count by the counting threads (the barrier orders the other threads'
+            // reductions before the fence, which is cumulative); acquire: count,
+            // fence, barrier, reads through L2 -- the pattern of a grid-wide barrier.
+            __syncthreads();
+            if (tid < 9) {
+                const int nx = tx + tid % 3 - 1, ny = ty + tid / 3 - 1;
+                bool ready = false;
+                if (nx >= 0 && nx < A.G.ntx && ny >= 0 && ny < A.G.nty) {
+                    const int X = ny * A.G.ntx + nx;
+                    __threadfence();
+                    ready = atomicAdd(A.ncnt + X, 1) == A.nexp[X] - 1;
+                    if (ready) {
+                        A.ncnt[X] = 0;   // the last one: ready for the next launch
+                        __threadfence();
+                    }
+                }
+                const unsigned r = __ballot_sync(0x1ffu, ready);
+                if (tid == 0) s_touch = r;
+            }
+            __syncthreads();
+            unsigned r = s_touch;
+            if (r) {
+                do {
+                    const int q = __ffs(r) - 1;
+                    r &= r - 1;
+                    update_node_tile_f32(A, tx + q % 3 - 1, ty + q / 3 - 1, tid);
+                } while (r);
+            }
+            moved = __reduce_add_sync(0xffffffffu, moved);
+            if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
+        } else if (DO_P2G) {
             touch = __reduce_or_sync(0xffffffffu, touch);
             if ((tid & 31) == 0 && touch) atomicOr(&s_touch, touch);
             __syncthreads();
@@ -739,55 +897,6 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             __threadfence();
         }
     }
-}
-
-// Grid update of one node in FP32 (simulation/kernels.cuh:175-300) from its
-// mass and momentum, the indenter geometry and the force in FP64: the new
-// velocity, and the force bin of a contact node (-1 if none).
-__device__ __forceinline__ int node_velocity_f32(const StepParams &P, const SplitConsts &Q, int gx, int gy, float mass,
-                                                 float px, float py, double ind_x, double ind_y, float &vx, float &vy,
-                                                 double &fxd, double &fyd)
-{
-    vx = 0.f;
-    vy = 0.f;
-    int bin = -1;
-    if (mass != 0.f) {
-        const float rm = __fdividef(1.f, mass);   // fast reciprocal (FP32 path)
-        vx = px * rm;
-        vy = py * rm;
-        vy -= Q.dtg;
-        const float v2 = vx * vx + vy * vy;
-        if (v2 > Q.vmax_sq) {
-            const float r = sqrtf(v2);
-            vx = vx / r * Q.vmax;
-            vy = vy / r * Q.vmax;
-        }
-        double nx = (double)gx * P.h - ind_x, ny = (double)gy * P.h - ind_y;
-        if (nx * nx + ny * ny < P.ind_rsq) {
-            const double r = sqrt(nx * nx + ny * ny);
-            if (r > 0) { nx /= r; ny /= r; }
-            const float fnx = (float)nx, fny = (float)ny;
-            const float vrx = vx - (float)P.ind_v, vry = vy;
-            const float vn = vrx * fnx + vry * fny;
-            if (vn < 0.f) {
-                const float vtx = vrx - fnx * vn, vty = vry - fny * vn;
-                const float pvx = vx, pvy = vy;
-                vx = (float)P.ind_v + vtx;
-                vy = vty;
-                fxd = (double)(pvx - vx) * mass / P.dt;
-                fyd = (double)(pvy - vy) * mass / P.dt;
-                float angle = atan2f(fnx, fny);
-                angle = (float)((double)angle + kPi);
-                angle = (float)((double)angle * (P.nsub / (2 * kPi)));
-                bin = min(max((int)angle, 0), P.nsub - 1);
-            }
-        }
-        if (gy <= 2) { vx = 0.f; vy = 0.f; }
-        if (gy >= P.gridy - 3 && vy > 0.f) vy = 0.f;
-        if (gx <= 2 && vx < 0.f) vx = 0.f;
-        else if (gx >= P.gridx - 3 && vx > 0.f) vx = 0.f;
-    }
-    return bin;
 }
 
 struct BatchClock;
@@ -915,6 +1024,24 @@ static __global__ void k_inverse_perm(const int *__restrict__ oidx, int n, int *
     if (i < n) inv[oidx[i]] = i;
 }
 
+// Per node tile: the number of cell tiles with points in its 3 x 3
+// neighbourhood (the contributors the fused grid update waits for).
+static __global__ void k_node_tile_expect(TileGeom G, const int *__restrict__ cell_start, int *__restrict__ nexp)
+{
+    const int X = blockIdx.x * blockDim.x + threadIdx.x;
+    if (X >= G.ntiles) return;
+    const int x = X % G.ntx, y = X / G.ntx;
+    int e = 0;
+    for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+            const int tx = x + dx, ty = y + dy;
+            if (tx < 0 || tx >= G.ntx || ty < 0 || ty >= G.nty) continue;
+            const long t = (long)ty * G.ntx + tx;
+            e += cell_start[(t + 1) * TT] > cell_start[t * TT];
+        }
+    nexp[X] = e;
+}
+
 }  // namespace icy_dev
 
 namespace icy_dev {
@@ -957,12 +1084,15 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
                                                                 double ind_x, double ind_y)
 {
     extern __shared__ double s_acc[];   // 2*nsub (alone only)
+    const unsigned n = *(volatile unsigned *)tlist_n;
+    // nothing listed (the launch after a tile kernel that updated the grid itself):
+    // the counters stay zero, nothing to reset
+    if (!BATCH && n == 0) return;
     if (!BATCH) {
         for (int k = threadIdx.x; k < 2 * A1.P.nsub; k += blockDim.x) s_acc[k] = 0;
         __syncthreads();
     }
     bool any = false;
-    const unsigned n = *(volatile unsigned *)tlist_n;
     constexpr int TPC = 256 / TT;   // node tiles per CTA pass
     static_assert(256 % TT == 0, "whole node tiles per 256-thread CTA");
     const int l = threadIdx.x % TT;
@@ -1010,8 +1140,8 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
                 A.g.v[q[u]] = make_float2(vx, vy);
                 A.g.mp[q[u]] = make_float4(0.f, 0.f, 0.f, 0.f);
             } else {
-                A.g.vx[q[u]] = vx;
-                A.g.vy[q[u]] = vy;
+                A.g.nvx[q[u]] = vx;   // the velocities the next G2P reads
+                A.g.nvx[q[u] + A.n_nodes] = vy;
                 A.g.m[q[u]] = 0.f;
                 A.g.px[q[u]] = 0.f;
                 A.g.py[q[u]] = 0.f;

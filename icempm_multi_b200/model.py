@@ -105,6 +105,13 @@ class GPUImplementation:
     def kernel_launches(self):
         return lib().icy_mpm_kernel_launches(self._h)
 
+    def counters(self):
+        """Device counters: points off their binned cell (per P2G), FP32 launches
+        that fused the grid update, launches that fell back to the update kernel."""
+        c = [C.c_int64(0) for _ in range(3)]
+        check(lib().icy_mpm_counters(self._h, *[C.byref(x) for x in c]), "icy_mpm_counters")
+        return {"moved_points": c[0].value, "fused_launches": c[1].value, "fallback_launches": c[2].value}
+
     def set_option(self, name, value):
         """Instance tuning option (include/icempm.h: icy_mpm_set_option)."""
         check(lib().icy_mpm_set_option(self._h, name.encode(), float(value)), "icy_mpm_set_option")

@@ -52,8 +52,10 @@ def make_workload(w, pinned=False):
 
 
 # ---------------------------------------------------------------- many scenarios
-# grids available to batched / served scenarios (cells), smallest that fits first
+# grids available to served scenarios (cells), smallest that fits first
 GRIDS = [(128, 128), (256, 128), (256, 256), (512, 256), (512, 512), (1024, 512), (2048, 512), (2048, 1024)]
+# the batched workload's grids: 128 x 128 to 1024 x 512
+GRIDS_BATCH = [g for g in GRIDS if g[0] <= 1024 and g[1] <= 512]
 
 
 def wave_speed(E, nu, rho):
@@ -71,19 +73,21 @@ def cfl_dt(E, nu, rho, h, courant=0.4):
     return math.floor(dt / 10 ** (e - 1)) * 10 ** (e - 1)
 
 
-def floe_scenario(n_points, E, phi, v_ind, seed, h=0.1, aspect=4.0, ppc=4, nu=0.3, rho=980.0):
+def floe_scenario(n_points, E, phi, v_ind, seed, h=0.1, aspect=4.0, ppc=4, nu=0.3, rho=980.0, grids=GRIDS):
     """A floe-indentation scenario of about n_points points: a block of
-    aspect:1 cells at ppc points per cell on the smallest grid of GRIDS that
-    leaves room around it, dt from the CFL condition."""
+    aspect:1 cells at ppc points per cell on the smallest grid of `grids` that
+    leaves room around it (the largest grid, with the block cut to fit, if
+    none does), dt from the CFL condition."""
     import math
     cells = max(n_points // ppc, 16)
     ch = max(4, int(round(math.sqrt(cells / aspect))))
     cw = max(4, cells // ch)
-    for gx, gy in GRIDS:
+    for gx, gy in grids:
         if cw + 24 <= gx and ch + 16 <= gy:
             break
     else:
-        gx, gy = GRIDS[-1]
+        gx, gy = grids[-1]
+        cw, ch = min(cw, gx - 24), min(ch, gy - 16)
     w = dict(grid_x=gx, grid_y=gy, h=h, block_w=cw * h, block_h=ch * h, ppc=ppc,
              dt=cfl_dt(E, nu, rho, h), E=E, nu=nu, rho=rho, phi=phi, cohesion=0.0,
              ind_radius=1.0, ind_velocity=v_ind, ind_depth=0.5, seed=seed, n_grains=16)
@@ -100,5 +104,5 @@ def batch_scenarios(n_instances=256, seed=7, n_min=10_000, n_max=500_000):
     for k in range(n_instances):
         n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
         out.append(floe_scenario(n, E=float(rng.uniform(5e8, 2e9)), phi=float(rng.uniform(45, 70)),
-                                 v_ind=float(rng.uniform(0.5, 3.0)), seed=seed * 1000 + k))
+                                 v_ind=float(rng.uniform(0.5, 3.0)), seed=seed * 1000 + k, grids=GRIDS_BATCH))
     return out

@@ -48,7 +48,10 @@ enum {
     ICY_ERR_CAPACITY = 106,        /* host HSSOA capacity too small             */
     ICY_ERR_POINT_COUNT = 107,     /* active point count changed                */
     ICY_ERR_TIMEOUT = 108,         /* a bounded device wait gave up             */
-    ICY_ERR_NOT_SUPPORTED = 109
+    ICY_ERR_NOT_SUPPORTED = 109,
+    ICY_ERR_DRIFT = 110            /* FP32: a point moved further in one step than the
+                                      grid update fused into the tile kernel allows
+                                      (excluded by the test of the step before)   */
 };
 
 /* ------------------------------------------------------------------ */
@@ -252,15 +255,32 @@ int icy_mpm_status(icy_mpm *h);
  *   "pipe_fault_test" 1 = (tests of the timeout path) the producer leaves the
  *                   ring's first stage unfilled: every wait on it gives up
  *                   after 1 s and the next download reports ICY_ERR_TIMEOUT
+ *   "fuse_update"   FP32 split precision: 1 = the grid update of the next step is
+ *                   done inside the tile kernel, node tile by node tile, by the CTA
+ *                   that finishes its last neighbouring cell tile; a step in which
+ *                   a point could leave its tile's staged margin falls back to the
+ *                   list-driven update kernel; 0 = always the update kernel
+ *                   (default: the counting at every tile's end costs the tile
+ *                   kernel more than the update kernel takes)
  *   "profile_every" n = icy_mpm_profile times every n-th launch of each kernel
- *                   (default 1); an event pair on the stream costs the step
- *                   loop a few microseconds, so sampling keeps a profiled run
- *                   close to an unprofiled one
+ *                   (default 1; every re-binning is timed whatever n); an event
+ *                   pair on the stream costs the step loop a few microseconds, so
+ *                   sampling keeps a profiled run close to an unprofiled one
  */
 int icy_mpm_set_option(icy_mpm *h, const char *name, double value);
 
 /* Number of kernels this instance launched since creation. */
 int64_t icy_mpm_kernel_launches(icy_mpm *h);
+/*
+ * Device counters since creation (synchronous read; no counterpart in the
+ * reference): P2G contributions of points that had left the cell they were
+ * binned into (a re-binning hint), FP32 tile launches that fused the grid
+ * update, and FP32 tile launches that fell back to the update kernel because
+ * a point could leave its tile's staged margin (option "fuse_update").
+ * Any pointer may be NULL.
+ */
+int icy_mpm_counters(icy_mpm *h, int64_t *moved_points, int64_t *fused_launches,
+                     int64_t *fallback_launches);
 /*
  * Per-kernel timing with CUDA events recorded on the instance stream around
  * every kernel launch, or every n-th launch of each kernel with the option
