@@ -91,6 +91,8 @@ EXPORTED = [
     "icy_batch_download", "icy_batch_synchronize", "icy_batch_set_option", "icy_batch_info",
     "icy_batch_device_bytes", "icy_mpm_device_bytes", "icy_scene_place", "icy_host_alloc", "icy_host_free",
     "icy_batch_set_clock", "icy_mpm_counters",
+    "icy_part_plan", "icy_part_create", "icy_part_upload", "icy_part_step", "icy_part_download",
+    "icy_part_info", "icy_part_destroy",
 ]
 
 _lib = None
@@ -138,6 +140,14 @@ def lib():
         "icy_mpm_status": (C.c_int, [vp]),
         "icy_mpm_kernel_launches": (C.c_int64, [vp]),
         "icy_mpm_counters": (C.c_int, [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "icy_part_plan": (C.c_int, [C.POINTER(SimParams), vp, C.c_uint, C.c_uint, C.c_int, vp, vp, vp, vp]),
+        "icy_part_create": (C.c_int, [C.POINTER(SimParams), C.c_int, vp, C.c_uint, C.POINTER(vp)]),
+        "icy_part_upload": (C.c_int, [vp, vp, C.c_uint, C.c_uint]),
+        "icy_part_step": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+        "icy_part_download": (C.c_int, [vp, vp, C.c_uint, C.POINTER(C.c_uint), vp]),
+        "icy_part_info": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_uint),
+                                    C.POINTER(C.c_int)]),
+        "icy_part_destroy": (C.c_int, [vp]),
         "icy_mpm_profile": (C.c_int, [vp, C.c_int]),
         "icy_mpm_set_option": (C.c_int, [vp, C.c_char_p, C.c_double]),
         "icy_mpm_profile_read": (C.c_int, [vp, C.c_int, C.c_char_p, vp, vp, C.POINTER(C.c_int)]),

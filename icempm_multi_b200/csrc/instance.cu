@@ -188,10 +188,17 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
                             (int)MOMF_BYTES));
     CK(cudaFuncSetAttribute(k_tile_f32<false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             (int)MOMF_BYTES));
+    CK(cudaFuncSetAttribute(k_tile_f32<true, true, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)MOMF_BYTES));
+    CK(cudaFuncSetAttribute(k_tile_f32<false, true, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)MOMF_BYTES));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false>, TILE_THREADS_F32,
                                                      MOMF_BYTES));
     h->tile_grid_f32 = std::max(1, sms * std::max(per_sm, 1));
     h->update_grid = (int)std::max(1L, std::min((long)(h->ntiles + 1) / 2, (long)sms * 8));
+    per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_update_tiles_f32, TT, 0));
+    h->update_grid_f32 = (int)std::max(1L, std::min((long)h->ntiles, (long)sms * std::max(per_sm, 1)));
     if (int rc = icy_instance_constants(h)) return rc;
     CK(cudaStreamSynchronize(h->stream));
     return ICY_OK;
@@ -429,7 +436,7 @@ static int fallback_ctas(icy_mpm *h)
 {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-    return std::max(1, std::min(h->update_grid, sms));
+    return std::max(1, std::min(h->update_grid_f32, sms));
 }
 
 // Largest move of a point in one step, in cells: the grid update clamps node
@@ -460,14 +467,21 @@ static int launch_tile_split(icy_mpm *h, int which, bool record, double ind_x = 
             A.ind_y = ind_y;
         }
     }
+    const bool fuse = A.seq > 0;
     switch (which) {
     case 0:
         icy_prof_begin(h, K_TILE_G2P2G);
-        k_tile_f32<true, true, false><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
+        if (fuse)
+            k_tile_f32<true, true, false, false, true><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
+        else
+            k_tile_f32<true, true, false><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
         break;
     case 1:
         icy_prof_begin(h, K_TILE_P2G);
-        k_tile_f32<false, true, false><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
+        if (fuse)
+            k_tile_f32<false, true, false, false, true><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
+        else
+            k_tile_f32<false, true, false><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
         break;
     default:
         icy_prof_begin(h, K_TILE_G2P);
@@ -517,8 +531,12 @@ static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y, int ctas 
     StepParams P = icy_step_params(h->prm);
     icy_prof_begin(h, K_UPDATE_TILES);
     if (is_split(h)) {
-        k_update_list_f32<false><<<ctas > 0 ? ctas : h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(
-            split_args(h, false), nullptr, nullptr, h->d_tlist, h->d_tlist_n, ind_x, ind_y);
+        k_update_tiles_f32<<<ctas > 0 ? ctas : h->update_grid_f32, TT, 0, h->stream>>>(split_args(h, false),
+                                                                                     h->d_tlist, h->d_tlist_n,
+                                                                                     ind_x, ind_y);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->d_tlist_n, 0, sizeof(unsigned) * 2, h->stream);
+        if (e != cudaSuccess) { icy_set_error("k_update_tiles_f32", e); return ICY_ERR_CUDA; }
         h->vpar ^= 1;
     } else
         k_update_list<<<h->update_grid, 256, sizeof(double) * 2 * P.nsub, h->stream>>>(

@@ -53,7 +53,7 @@ struct icy_mpm {
     unsigned *d_tlist_n = nullptr;  // [0] entries, [1] CTAs of the update done
     unsigned long long *d_moved = nullptr;
     int ntx = 0, nty = 0, ntiles = 0;
-    int tile_grid = 0, update_grid = 0, pipe_grid = 0;
+    int tile_grid = 0, update_grid = 0, pipe_grid = 0, update_grid_f32 = 0;
     bool binned = false;        // points sorted by tile since the last upload
     bool permuted = false;      // device order differs from upload order
     bool primed = false;        // accumulators hold P2G of the current state

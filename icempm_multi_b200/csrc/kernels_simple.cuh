@@ -15,7 +15,12 @@ struct GridView {
     double *m, *px, *py;   // accumulators
     double *vx, *vy;       // node velocities
     int ny;                // node stride along x (= GridY)
-    int halo;              // x offset: node gx is stored at column gx + halo
+    int halo;              // x offset: node gx is stored at column gx + halo (for a slab of the
+                           // grid starting at column x0: halo - x0)
+    // stencil bases gx in [xlo, xhi] lie in this grid's columns (the whole grid:
+    // -halo .. GridX + halo - 3, as base_error's x test); nodes gx in [flo, fhi)
+    // count their indenter force (a slab: its own columns, not the neighbours')
+    int xlo = -(1 << 30), xhi = 1 << 30, flo = -(1 << 30), fhi = 1 << 30;
     __device__ __forceinline__ long idx(int gx, int gy) const { return (long)(gx + halo) * ny + gy; }
 };
 
@@ -24,12 +29,10 @@ __device__ __forceinline__ long long ld_util(const double *pts, long i)
     return __double_as_longlong(pts[i]);
 }
 
-// P2G, one thread per particle (kernels.cuh:46-122)
-static __global__ void k_p2g_simple(StepParams P, const double *__restrict__ pts, long pitch, int n, GridView g,
-                             int *status)
+// P2G of point i (kernels.cuh:46-122)
+__device__ __forceinline__ void p2g_one(const StepParams &P, const double *__restrict__ pts, long pitch, int i,
+                                        const GridView &g, int *status)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
     long long util = ld_util(pts, i);
     if (util & kDisabled) return;
     const bool liquid = (util & kLiquid) != 0;
@@ -44,6 +47,7 @@ static __global__ void k_p2g_simple(StepParams P, const double *__restrict__ pts
     const int bx = (int)(x * P.hinv - 0.5), by = (int)(y * P.hinv - 0.5);
     const double fx = x * P.hinv - (double)bx, fy = y * P.hinv - (double)by;
     int e = base_error(P, bx, by);
+    if (!e && (bx < g.xlo || bx > g.xhi)) e = bx < g.xlo ? 70 : 72;   // beyond the slab's columns
     if (e) { *status = e; return; }
     double wx[3], wy[3];
     bspline_weights(fx, wx);
@@ -64,6 +68,14 @@ static __global__ void k_p2g_simple(StepParams P, const double *__restrict__ pts
     }
 }
 
+// P2G, one thread per particle
+static __global__ void k_p2g_simple(StepParams P, const double *__restrict__ pts, long pitch, int n, GridView g,
+                                    int *status)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p2g_one(P, pts, pitch, i, g, status);
+}
+
 // indenter force bins are accumulated per block in shared memory first
 // and added to the global accumulator once per block
 static __global__ void k_update_simple(StepParams P, GridView g, long n_nodes, double ind_x, double ind_y,
@@ -81,7 +93,7 @@ static __global__ void k_update_simple(StepParams P, GridView g, long n_nodes, d
         if (node_update(P, gix, giy, g.m[idx], g.px[idx], g.py[idx], ind_x, ind_y, vx, vy, bin, fx, fy)) {
             g.vx[idx] = vx;
             g.vy[idx] = vy;
-            if (bin >= 0) {
+            if (bin >= 0 && gix >= g.flo && gix < g.fhi) {
                 atomicAdd(&s_acc[2 * bin], fx);
                 atomicAdd(&s_acc[2 * bin + 1], fy);
                 any = true;
@@ -96,12 +108,10 @@ static __global__ void k_update_simple(StepParams P, GridView g, long n_nodes, d
         if (s_acc[k] != 0.0) atomicAdd(acc + k, s_acc[k]);
 }
 
-// G2P + plasticity, one thread per particle (kernels.cuh:305-414)
-static __global__ void k_g2p_simple(StepParams P, double *__restrict__ pts, long pitch, int n, GridView g, int recordPQ,
-                             int *status)
+// G2P + plasticity of point i (kernels.cuh:305-414)
+__device__ __forceinline__ void g2p_one(const StepParams &P, double *__restrict__ pts, long pitch, int i,
+                                        const GridView &g, int recordPQ, int *status)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
     long long util = ld_util(pts, i);
     if (util & kDisabled) return;
     const bool liquid = (util & kLiquid) != 0;
@@ -112,6 +122,7 @@ static __global__ void k_g2p_simple(StepParams P, double *__restrict__ pts, long
     const int bx = (int)(x * P.hinv - 0.5), by = (int)(y * P.hinv - 0.5);
     const double fx = x * P.hinv - (double)bx, fy = y * P.hinv - (double)by;
     int e = base_error(P, bx, by);
+    if (!e && (bx < g.xlo || bx > g.xhi)) e = bx < g.xlo ? 70 : 72;   // beyond the slab's columns
     if (e) { *status = e; return; }
     double wx[3], wy[3];
     bspline_weights(fx, wx);
@@ -159,6 +170,14 @@ static __global__ void k_g2p_simple(StepParams P, double *__restrict__ pts, long
     pts[i + pitch * 8] = Fn.a00; pts[i + pitch * 9] = Fn.a01; pts[i + pitch * 10] = Fn.a10; pts[i + pitch * 11] = Fn.a11;
     pts[i + pitch * 12] = B.a00; pts[i + pitch * 13] = B.a01; pts[i + pitch * 14] = B.a10; pts[i + pitch * 15] = B.a11;
     if (recordPQ) { pts[i + pitch * 1] = ptr; pts[i + pitch * 2] = qtr; }
+}
+
+// G2P + plasticity, one thread per particle
+static __global__ void k_g2p_simple(StepParams P, double *__restrict__ pts, long pitch, int n, GridView g, int recordPQ,
+                                    int *status)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) g2p_one(P, pts, pitch, i, g, recordPQ, status);
 }
 
 }  // namespace icy_dev

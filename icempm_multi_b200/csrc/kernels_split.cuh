@@ -479,7 +479,7 @@ __device__ __forceinline__ void cell_order_build(int (&hist)[CNT_BUCKETS], const
 }
 
 // phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32
-template <int NT, bool AOS, typename Sync>
+template <int NT, bool AOS, bool FUSE, typename Sync>
 __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int tid, int tx, int ty, int cs, int ce,
                                                         const int *s_cs, const int *s_perm, float *mom,
                                                         float (*s_odd)[RN], unsigned &touch, unsigned &moved,
@@ -516,7 +516,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                 moved++;
                 int bx, by;
                 split_unpack(pb, bx, by);
-                if (!AOS && A.seq > 0) {
+                if (FUSE && A.seq > 0) {
                     // can this point leave the staged margin during the next step?  (its
                     // offset from its sorted cell, in cells, against the largest move of a
                     // step; near the low edges, where the base truncates, always)
@@ -536,7 +536,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                                                 atomicAdd(&s_odd[2][k], W * ty);
                                             });
                 } else {
-                    if (fused) *A.status = ICY_DRIFT_CODE;   // excluded by the margin test of the last launch
+                    if (FUSE && fused) *A.status = ICY_DRIFT_CODE;   // excluded by the margin test of the last launch
                     p2g_global_f32<AOS>(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by,
                                         gx, gy, mass, mvx, mvy, s00, s01, s10, s11);
                 }
@@ -574,7 +574,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
         if (m != 0.f || px != 0.f || py != 0.f) {
             const int gx = RX0 + i, gy = RY0 + jj;
             A.g.add<AOS>(A.g.idx(gx, gy), m, px, py);
-            if (!fused) {
+            if (!FUSE || !fused) {
                 const int dx = (gx + P.halo) / TX - tx + 1, dy = gy / TY - ty + 1;
                 touch |= 1u << (dy * 3 + dx);
             }
@@ -642,7 +642,8 @@ __device__ __forceinline__ int node_velocity_f32(const StepParams &P, const Spli
 // each (the fused update of k_tile_f32): reads the finished sums (through L2:
 // other CTAs added them), writes the next velocities, clears the sums and
 // adds the indenter force of contact nodes to the bins.
-__device__ __forceinline__ void update_node_tile_f32(const SplitArgs &A, int ntx_, int nty_, int l)
+__device__ __forceinline__ void update_node_tile_f32(const SplitArgs &A, int ntx_, int nty_, int l, double ind_x,
+                                                     double ind_y)
 {
     const StepParams &P = A.P;
     const int gx = ntx_ * TX + l / TY - P.halo, gy = nty_ * TY + l % TY;
@@ -651,7 +652,7 @@ __device__ __forceinline__ void update_node_tile_f32(const SplitArgs &A, int ntx
     const float m = __ldcg(A.g.m + k), px = __ldcg(A.g.px + k), py = __ldcg(A.g.py + k);
     float vx, vy;
     double fx = 0, fy = 0;
-    const int bin = node_velocity_f32(P, A.Q, gx, gy, m, px, py, A.ind_x, A.ind_y, vx, vy, fx, fy);
+    const int bin = node_velocity_f32(P, A.Q, gx, gy, m, px, py, ind_x, ind_y, vx, vy, fx, fy);
     A.g.nvx[k] = vx;
     A.g.nvx[k + A.n_nodes] = vy;
     if (m != 0.f || px != 0.f || py != 0.f) {
@@ -662,6 +663,61 @@ __device__ __forceinline__ void update_node_tile_f32(const SplitArgs &A, int ntx
     if (bin >= 0) {
         atomicAdd(A.acc + 2 * bin, fx);
         atomicAdd(A.acc + 2 * bin + 1, fy);
+    }
+}
+
+// Grid update of the node tiles P2G listed (single instance): TT threads per
+// CTA, one node of each of UPD_FLAT list entries per thread and pass, their
+// loads issued together so that many tiles' loads are in flight; contact
+// forces go to the bins directly (a few hundred nodes touch the indenter).
+// The host clears the list after the kernel.
+constexpr int UPD_FLAT = 4;
+static __global__ void __launch_bounds__(TT) k_update_tiles_f32(const __grid_constant__ SplitArgs A,
+                                                               const int2 *__restrict__ tlist,
+                                                               const unsigned *__restrict__ tlist_n, double ind_x,
+                                                               double ind_y)
+{
+    const StepParams &P = A.P;
+    const unsigned n = *tlist_n;
+    const int l = threadIdx.x;
+    for (unsigned e0 = blockIdx.x; e0 < n; e0 += gridDim.x * UPD_FLAT) {
+        long q[UPD_FLAT];
+        int gx[UPD_FLAT], gy[UPD_FLAT];
+        float m[UPD_FLAT], px[UPD_FLAT], py[UPD_FLAT];
+#pragma unroll
+        for (int u = 0; u < UPD_FLAT; u++) {
+            const unsigned e = e0 + u * gridDim.x;
+            q[u] = -1;
+            if (e >= n) continue;
+            const int2 it = tlist[e];
+            const int tx = it.y & 0xffff, ty = it.y >> 16;
+            if (l == 0) A.flags[ty * A.G.ntx + tx] = 0u;
+            gx[u] = tx * TX + l / TY - P.halo;
+            gy[u] = ty * TY + l % TY;
+            if (gx[u] >= P.gridx + P.halo || gy[u] >= P.gridy) continue;   // past the grid edge
+            q[u] = A.g.idx(gx[u], gy[u]);
+            m[u] = A.g.m[q[u]];
+            px[u] = A.g.px[q[u]];
+            py[u] = A.g.py[q[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < UPD_FLAT; u++) {
+            if (q[u] < 0) continue;
+            float vx, vy;
+            double fx = 0, fy = 0;
+            const int bin = node_velocity_f32(P, A.Q, gx[u], gy[u], m[u], px[u], py[u], ind_x, ind_y, vx, vy, fx, fy);
+            A.g.nvx[q[u]] = vx;
+            A.g.nvx[q[u] + A.n_nodes] = vy;
+            if (m[u] != 0.f || px[u] != 0.f || py[u] != 0.f) {
+                A.g.m[q[u]] = 0.f;
+                A.g.px[q[u]] = 0.f;
+                A.g.py[q[u]] = 0.f;
+            }
+            if (bin >= 0) {
+                atomicAdd(A.acc + 2 * bin, fx);
+                atomicAdd(A.acc + 2 * bin + 1, fy);
+            }
+        }
     }
 }
 
@@ -698,8 +754,10 @@ __device__ __forceinline__ void prefetch_next_item(const SplitArgs &A1, const Sp
 // Tile kernel over the FP32 state: <G2P, P2G, write vel/Bp> as k_tile.
 // With BATCH, the CTAs walk the (instance, tile) list of many independent
 // instances, each with its own parameters, grid and points (Aarr[inst]), and
-// the record-PQ flag of each instance comes from rec[inst].
-template <bool DO_G2P, bool DO_P2G, bool WRITE_VB, bool BATCH = false>
+// the record-PQ flag of each instance comes from rec[inst].  FUSE (single
+// instance, option "fuse_update"): P2G tests the drift margin for the next
+// step, and a G2P + P2G launch updates the grid itself where that is safe.
+template <bool DO_G2P, bool DO_P2G, bool WRITE_VB, bool BATCH = false, bool FUSE = false>
 static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     k_tile_f32(const __grid_constant__ SplitArgs A1, const SplitArgs *__restrict__ Aarr = nullptr, const BatchItem *__restrict__ work = nullptr,
                const int *__restrict__ nwork = nullptr, const int *__restrict__ rec = nullptr)
@@ -720,8 +778,10 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     // neighbourhood after they were updated, so the tiles are marked for the
     // list-driven update that follows instead.  The flag of launch s is
     // unsafe[s & 1]: this launch reads the other one, which nobody writes now.
-    const bool fused = !BATCH && DO_G2P && DO_P2G && A1.seq > 0 && A1.unsafe[(A1.seq - 1) & 1] != A1.seq - 1;
-    if (!BATCH && DO_G2P && DO_P2G && A1.seq > 0 && blockIdx.x == 0 && tid == 0) atomicAdd(A1.moved + (fused ? 1 : 2), 1ull);
+    static_assert(!(FUSE && BATCH), "the fused grid update is single-instance only");
+    const bool fused = FUSE && DO_G2P && DO_P2G && A1.seq > 0 && A1.unsafe[(A1.seq - 1) & 1] != A1.seq - 1;
+    if (FUSE && DO_G2P && DO_P2G && A1.seq > 0 && blockIdx.x == 0 && tid == 0)
+        atomicAdd(A1.moved + (fused ? 1 : 2), 1ull);
     // Alone, CTA c takes the tiles c, c + gridDim.x, ... (equal tiles, and no
     // claim to wait for: 5 % faster).  In a batch, where the items differ in
     // size, they are handed out one at a time (A1.claim[0]), each CTA claiming
@@ -832,11 +892,11 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                     if (tid < 32) cell_order_build(s_hist, s_rank, s_perm, tid);
                     __syncthreads();
                 }
-                p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH>(A, tid, tx, ty, cs, ce, s_cs, s_perm, s_momf, s_odd,
+                p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH, FUSE>(A, tid, tx, ty, cs, ce, s_cs, s_perm, s_momf, s_odd,
                                                                  touch, moved, fused, [] { __syncthreads(); });
             }
         }
-        if (DO_P2G && fused) {
+        if (FUSE && DO_P2G && fused) {
             // Fused grid update: this tile's sums are in; count it finished for each
             // of the 9 node tiles around it.  The CTA that brings a node tile's count
             // to the number of active cell tiles around it (nexp, from the binning)
@@ -868,7 +928,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                 do {
                     const int q = __ffs(r) - 1;
                     r &= r - 1;
-                    update_node_tile_f32(A, tx + q % 3 - 1, ty + q / 3 - 1, tid);
+                    update_node_tile_f32(A, tx + q % 3 - 1, ty + q / 3 - 1, tid, A.ind_x, A.ind_y);
                 } while (r);
             }
             moved = __reduce_add_sync(0xffffffffu, moved);
@@ -1085,9 +1145,6 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
 {
     extern __shared__ double s_acc[];   // 2*nsub (alone only)
     const unsigned n = *(volatile unsigned *)tlist_n;
-    // nothing listed (the launch after a tile kernel that updated the grid itself):
-    // the counters stay zero, nothing to reset
-    if (!BATCH && n == 0) return;
     if (!BATCH) {
         for (int k = threadIdx.x; k < 2 * A1.P.nsub; k += blockDim.x) s_acc[k] = 0;
         __syncthreads();

@@ -371,6 +371,59 @@ int64_t icy_batch_device_bytes(icy_batch *b, int slot);
 int64_t icy_mpm_device_bytes(const icy_sim_params *p, unsigned capacity, int precision);
 
 /* ------------------------------------------------------------------ */
+/* one instance in slabs of grid columns (partitions)                   */
+/* ------------------------------------------------------------------ */
+/*
+ * GPU_Implementation5 with several partitions
+ * (simulation/gpu_implementation5.cpp:31-204,221-326): the grid's columns
+ * are cut into slabs, each partition holding its columns plus GridHaloSize
+ * columns on both sides and the points whose stencil base lies in its
+ * columns, on its own device (several on one device, as the reference
+ * allows, or one device each with peer access between neighbours).  FP64,
+ * one thread per point / node (the reference's kernel structure).  Per
+ * sub-step: P2G; the 2*GridHaloSize boundary columns of mass and momentum
+ * copied to each neighbour and added there (the reference's
+ * receive_halos); grid update; G2P; every UpdateEveryNthStep /
+ * PointTransferFrequency sub-steps, points more than 3 columns past their
+ * slab move to the neighbour (packed, then appended by the neighbour from
+ * the sender's memory: the reference's receive_points).  Results match the
+ * one-domain path within FP64 round-off (the order of the sums differs);
+ * each node's indenter force is counted once, by the partition owning its
+ * column (the reference adds the boundary columns' forces in both).
+ */
+typedef struct icy_part icy_part;
+/* The split of GPU_Implementation5::split_hssoa_into_partitions
+   (gpu_implementation5.cpp:284-326): the HSSOA's points (sorted by cell, as
+   LoadRawPoints leaves them) in equal shares, each boundary at the x cell of
+   the first point of the next share.  Per partition: first column x0[i],
+   columns width[i], first point first[i], points count[i].
+   ICY_ERR_INVALID_ARGUMENT if a slab would be narrower than 2*GridHaloSize
+   columns (its boundary regions would not cover what its neighbours'
+   points can reach). */
+int icy_part_plan(const icy_sim_params *p, const double *hssoa, unsigned capacity, unsigned size,
+                  int n_partitions, int *x0, int *width, unsigned *first, unsigned *count);
+/* n_partitions partitions, partition i on device devices[i] (NULL: all on
+   device 0), each with room for capacity_per_partition points (points that
+   move in are appended; ICY_ERR_NO_SPACE, the reference's code 5, when full).
+   Neighbours on different devices need peer access (ICY_ERR_NOT_SUPPORTED). */
+int icy_part_create(const icy_sim_params *p, int n_partitions, const int *devices,
+                    unsigned capacity_per_partition, icy_part **out);
+/* Split the HSSOA (line stride = capacity) by icy_part_plan and upload. */
+int icy_part_upload(icy_part *h, const double *hssoa, unsigned capacity, unsigned size);
+/* Sub-steps step0 .. step0+nsteps-1 of icy::Model::Step (model.cpp:38-54),
+   queued on the partitions' streams; *sim_time is advanced. */
+int icy_part_step(icy_part *h, int step0, int nsteps, double *sim_time);
+/* All points back in upload order (synchronises), the indenter force bins
+   summed over the partitions (may be NULL), *size = points uploaded; the
+   first partition's device error code, ICY_ERR_POINT_COUNT if points were
+   lost. */
+int icy_part_download(icy_part *h, double *hssoa, unsigned capacity, unsigned *size, double *bins);
+/* Partition `part`: first column, columns, points in its slots (moved-away
+   slots included), device. */
+int icy_part_info(icy_part *h, int part, int *x0, int *width, unsigned *count, int *device);
+int icy_part_destroy(icy_part *h);
+
+/* ------------------------------------------------------------------ */
 /* stepping without allocation                                          */
 /* ------------------------------------------------------------------ */
 /*
