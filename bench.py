@@ -407,32 +407,28 @@ def measure_batch(n_instances=256, steps=500, seed=7):
                         "E U(5e8,2e9), phi U(45,70), indenter U(0.5,3) m/s, CFL dt, FP32 split, CUDA graph"}
 
 
-def measure_serve(rate=10.0, duration=12.0, seed=11):
-    """Served Poisson request stream: scenarios of 5k-2M points (log-uniform),
-    200-5000 steps, `rate` arrivals per second for `duration` seconds (a fixed
-    trace: same requests and arrival times every run), admitted by a 150 GB
-    device-memory budget, continuous batching in rounds of 50 steps; p50/p99
-    completion latency; the offered load (requested particle-steps per second
-    of arrivals) is reported beside the served throughput."""
-    import numpy as np
-    from icempm_multi_b200.serve import Server, poisson_requests
-    from icempm_multi_b200.workloads import floe_scenario, make_workload as mk
-    rng = np.random.default_rng(seed)
-    scenes = []
-    for k in range(16):
-        n = int(round(np.exp(rng.uniform(np.log(5e3), np.log(2e6)))))
-        w = floe_scenario(n, E=float(rng.uniform(5e8, 2e9)), phi=float(rng.uniform(45, 70)),
-                          v_ind=float(rng.uniform(0.5, 3.0)), seed=seed * 100 + k)
-        scenes.append(mk(w, pinned=True))
+def measure_serve(rate=10.0, duration=12.0, seed=11, budget=150e9, max_instances=128):
+    """Served Poisson request stream (the serving workload): every request its
+    own seeded floe-indentation scenario -- points log-uniform 5k-2M, E, friction
+    angle and indenter speed drawn per request, steps uniform 200-5000 --
+    arriving at `rate` per second for `duration` seconds (the same trace every
+    run), admitted by a device-memory budget, continuous batching in rounds of
+    50 steps; p50/p99 completion latency; the offered load (requested
+    particle-steps per second of arrivals) beside the served throughput.  Each
+    scenario is built when its request reaches the head of the queue and its
+    host copy released once uploaded."""
+    from icempm_multi_b200.serve import Server, seeded_requests
     n_req = max(8, int(rate * duration))
-    reqs = poisson_requests(scenes, rate, n_req, round_steps=50, seed=seed)
-    offered = sum(r.soa.size * r.steps for r in reqs) / max(reqs[-1].arrival, 1e-9)
-    srv = Server(budget_bytes=150e9, round_steps=50, keep_results=False)
+    reqs = seeded_requests(rate, n_req, round_steps=50, seed=seed)
+    srv = Server(budget_bytes=budget, max_instances=max_instances, round_steps=50, keep_results=False,
+                 keep_inputs=False)
     st = srv.run(reqs)
     srv.close()
-    st.update({"arrival_rate_per_s": rate, "offered_particle_steps_per_s": offered, "budget_bytes": 150e9, "round_steps": 50, "unit": METRIC,
-               "workload": "Poisson arrivals, points log-uniform 5k-2M, steps U(200,5000), FP32 split, "
-                           "150 GB budget, continuous batching"})
+    offered = sum(r.npts * r.steps for r in reqs) / max(reqs[-1].arrival, 1e-9)
+    st.update({"arrival_rate_per_s": rate, "offered_particle_steps_per_s": offered, "round_steps": 50,
+               "slots": max_instances, "unit": METRIC,
+               "workload": "Poisson arrivals, a seeded scenario per request: points log-uniform 5k-2M, "
+                           "steps U(200,5000), FP32 split, continuous batching"})
     return st
 
 
@@ -547,9 +543,13 @@ def main():
             try:
                 out["batched"] = measure_batch()
                 out["served"] = measure_serve()
-                # the same trace at twice the arrival rate: more than the GPU can take,
-                # so throughput shows the serving capacity and latency the queueing
+                # the same kind of trace at twice the arrival rate: more than the GPU can
+                # take, so throughput shows the serving capacity and latency the queueing
                 out["served_overload"] = measure_serve(rate=20.0, duration=6.0)
+                # over capacity with a budget the admitted scenarios fill: admission is
+                # held back by device memory, not by slots (at these request sizes the
+                # 150 GB budget would need about 1,300 resident requests to bind)
+                out["served_budget"] = measure_serve(rate=20.0, duration=6.0, budget=6e9, max_instances=512)
             except Exception as e:
                 out["batched_or_served_error"] = str(e)[:300]
         # ---- CPU baseline ------------------------------------------------------------------

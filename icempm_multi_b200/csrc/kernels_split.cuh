@@ -212,7 +212,11 @@ __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitC
         split_dev(s.D, jm1, d00, d01);
         const float Je = 1.f + jm1;
         s.ptr = -(Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
-        s.qtr = __fdividef(2.f * Q.mu, Je) * sqrtf(d00 * d00 + d01 * d01);   // sqrt(2) mu/J |dev|, |dev| = sqrt(2(d00^2+d01^2))
+        // sqrt(2) mu/J |dev|, |dev| = sqrt(2(d00^2+d01^2)); the square root to FP32
+        // accuracy by the hardware approximation (relative error 2^-23)
+        float sq;
+        asm("sqrt.approx.f32 %0, %1;" : "=f"(sq) : "f"(d00 * d00 + d01 * d01));
+        s.qtr = __fdividef(2.f * Q.mu, Je) * sq;   // sqrt(2) mu/J |dev|, |dev| = sqrt(2(d00^2+d01^2))
         if (!(s.util & (unsigned)kCrushed)) {
             const float4 gc = __ldg(reinterpret_cast<const float4 *>(tab) + grain_entry_f32(s.util));
             const float pmin2 = gc.x, k = gc.y, msq = gc.z;
@@ -934,17 +938,18 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             moved = __reduce_add_sync(0xffffffffu, moved);
             if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
         } else if (DO_P2G) {
+            // each warp marks the node tiles it wrote (no barrier: the node phase's
+            // last barrier already ended every use of the shared buffers)
             touch = __reduce_or_sync(0xffffffffu, touch);
-            if ((tid & 31) == 0 && touch) atomicOr(&s_touch, touch);
-            __syncthreads();
-            if (tid < 9 && ((s_touch >> tid) & 1u)) {
-                const int ntx = tx + tid % 3 - 1, nty = ty + tid / 3 - 1;
+            const int lane = tid & 31;
+            if (lane < 9 && ((touch >> lane) & 1u)) {
+                const int ntx = tx + lane % 3 - 1, nty = ty + lane / 3 - 1;
                 mark_tile(A.flags, A.tlist, A.tlist_n, A.inst, ntx, nty, A.G.ntx);
             }
             moved = __reduce_add_sync(0xffffffffu, moved);
             if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
         }
-        __syncthreads();
+        if (FUSE || !DO_P2G) __syncthreads();   // the fused path reads s_touch; G2P only: s_v, s_cs reused
         ti = next;
     }
     // the last CTA to finish resets the counters for the next launch: every

@@ -38,9 +38,10 @@ from .hssoa import HostSideSOA
 class Request:
     rid: int
     arrival: float              # seconds after the start of the run
-    params: object              # SimParams
-    soa: HostSideSOA            # initial state (kept only until admission)
+    params: object              # SimParams (None until `make` has built the scenario)
+    soa: HostSideSOA            # initial state (released once its upload is done)
     steps: int                  # sub-steps to run (a multiple of the round length)
+    make: object = None         # () -> (params, soa): builds the scenario when it reaches the queue head
     slot: int = -1
     admitted: float = None
     done: float = None
@@ -54,10 +55,22 @@ class Request:
     resume_time: float = 0.0     # simulation time / step index to resume from after an eviction
     resume_step: int = 0
     bins_before: np.ndarray = None
+    npts: int = 0                # points and HSSOA capacity of the scenario (kept after release)
+    capacity: int = 0
+    upload_round: int = -1       # the round queued after the upload: the buffer is free once it is done
+
+    def ensure(self):
+        """Build the scenario now if it was deferred; returns (params, soa)."""
+        if self.soa is None and self.make is not None:
+            self.params, self.soa = self.make()
+            self.make = None
+        if self.soa is not None:
+            self.npts, self.capacity = self.soa.size, self.soa.capacity
+        return self.params, self.soa
 
     @property
     def points(self):
-        return self.soa.size if self.soa is not None else (self.result.size if self.result is not None else 0)
+        return self.npts
 
 
 class Server:
@@ -67,8 +80,10 @@ class Server:
     128 slots keeps its members' kernel arguments in the constant bank
     (faster steps), so the default stays there."""
 
-    def __init__(self, budget_bytes=150e9, max_instances=128, round_steps=50, device=0, keep_results=True):
+    def __init__(self, budget_bytes=150e9, max_instances=128, round_steps=50, device=0, keep_results=True,
+                 keep_inputs=True):
         self.batch = Batch(max_instances, device=device)
+        self.keep_inputs = keep_inputs   # False: release each request's initial state once uploaded
         self.budget = float(budget_bytes)
         self.round_steps = int(round_steps)
         self.max_instances = int(max_instances)
@@ -89,13 +104,15 @@ class Server:
     def _admit(self, now):
         while self.queue and len(self.running) < self.max_instances:
             r = self.queue[0]
-            need = device_bytes(r.params, r.soa.capacity)
+            r.ensure()
+            need = device_bytes(r.params, r.capacity)
             if need > self.budget:   # larger than the whole budget: refuse instead of waiting forever
                 raise RuntimeError(f"request {r.rid} needs {need} bytes, budget {self.budget}")
             if self.used + need > self.budget:
                 break
             self.queue.popleft()
             r.slot = self.batch.add_async(r.params, r.soa)
+            r.upload_round = self.rounds + 1
             if r.evictions:
                 self.batch.set_clock(r.slot, r.resume_time, r.resume_step)
             r.bytes = need
@@ -125,7 +142,7 @@ class Server:
         out = []
         for slot, r in list(self.running.items()):
             if r.steps_done >= r.steps:
-                buf = self._out_buffer(r.soa.capacity)
+                buf = self._out_buffer(r.capacity)
                 self.batch.retire(slot, buf)
                 del self.running[slot]
                 out.append((slot, r, buf))
@@ -174,7 +191,7 @@ class Server:
         slot, r = self._running(rid)
         if r is None:
             return False
-        state = HostSideSOA(r.soa.capacity)
+        state = HostSideSOA(r.capacity)
         r.resume_time, r.resume_step, bins = self.batch.download(slot, state)
         r.bins_before = bins if r.bins_before is None else r.bins_before + bins
         self.batch.remove(slot)
@@ -211,6 +228,12 @@ class Server:
             # at most this round in flight; the previous round's results are copied by now
             self.batch.wait_steps(1)
             self._collect(retired, t0)
+            # the rounds before this one are done: uploads queued before them no longer
+            # read their host buffers
+            if not self.keep_inputs:
+                for r in self.running.values():
+                    if r.soa is not None and 0 <= r.upload_round < self.rounds:
+                        r.soa = None
             retired = finished
             if stepped and on_round is not None:
                 on_round(self, self.rounds)
@@ -221,6 +244,8 @@ class Server:
         lat = np.array([r.done - r.arrival for r in self.completed]) if self.completed else np.zeros(1)
         return {
             "requests": len(self.completed),
+            "budget_bytes": self.budget,
+            "peak_budget_fraction": self.peak_bytes / self.budget if self.budget > 0 else None,
             "cancelled": len(self.cancelled),
             "evictions": sum(r.evictions for r in self.completed),
             "makespan_s": makespan,
@@ -247,5 +272,32 @@ def poisson_requests(scenes, rate, n, steps_range=(200, 5000), round_steps=50, s
         t += rng.exponential(1.0 / rate)
         p, soa = scenes[k % len(scenes)]
         steps = int(rng.integers(lo // round_steps, hi // round_steps + 1)) * round_steps
-        out.append(Request(rid=k, arrival=t, params=p.copy(), soa=soa, steps=max(steps, round_steps)))
+        r = Request(rid=k, arrival=t, params=p.copy(), soa=soa, steps=max(steps, round_steps))
+        r.ensure()
+        out.append(r)
+    return out
+
+
+def seeded_requests(rate, n, points_range=(5_000, 2_000_000), steps_range=(200, 5000), round_steps=50, seed=11,
+                    pinned=True):
+    """n requests at Poisson arrival `rate` (per second), each its own seeded
+    floe-indentation scenario: points log-uniform in points_range, E uniform
+    5e8-2e9 Pa, friction angle uniform 45-70 deg, indenter 0.5-3 m/s, a step
+    count uniform in steps_range rounded to a multiple of round_steps.  The
+    scenario (parameters and initial points) is built when the request
+    reaches the head of the queue, so the host holds only the ones waiting
+    for admission or being uploaded."""
+    from .workloads import floe_scenario, make_workload
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    lo, hi = steps_range
+    for k in range(n):
+        t += rng.exponential(1.0 / rate)
+        npts = int(round(np.exp(rng.uniform(np.log(points_range[0]), np.log(points_range[1])))))
+        w = floe_scenario(npts, E=float(rng.uniform(5e8, 2e9)), phi=float(rng.uniform(45, 70)),
+                          v_ind=float(rng.uniform(0.5, 3.0)), seed=seed * 100000 + k)
+        steps = int(rng.integers(lo // round_steps, hi // round_steps + 1)) * round_steps
+        out.append(Request(rid=k, arrival=t, params=None, soa=None, steps=max(steps, round_steps),
+                           make=lambda w=w: make_workload(w, pinned=pinned)))
     return out
