@@ -269,8 +269,10 @@ def reference_gpu_rate(p, soa, steps, warmup):
 PROFILE_EVERY = 8
 
 
-def measure_instance(p, soa, precision, steps, warmup, local, pg, opts=(), profile=True, clocks=True):
-    """Device-timed steps of one instance (inputs resident in HBM)."""
+def measure_instance(p, soa, precision, steps, warmup, local, pg, opts=(), profile=True, clocks=True, tune=False):
+    """Device-timed steps of one instance (inputs resident in HBM); with
+    `tune`, the FP32 tile shape is picked first by timing each shape on this
+    instance (before the warm-up: the tuning steps are not timed)."""
     import torch
     from icempm_multi_b200 import GPUImplementation
     from icempm_multi_b200._lib import PRECISION_FP32_SPLIT, PRECISION_FP64
@@ -284,6 +286,13 @@ def measure_instance(p, soa, precision, steps, warmup, local, pg, opts=(), profi
     g.update_constants()
     g.transfer_ponts_to_device()
     g.reset_indenter_force_accumulator()
+    tuned = None
+    if tune and precision == "fp32" and not any(o.startswith("tile_shape=") for o in opts):
+        from icempm_multi_b200.autotune import SHAPES, tune_instance
+        tuned = tune_instance(g, p, soa.size, steps=10, resorts=(), stream=stream)
+        tuned = {"tile_shape": SHAPES[tuned["settings"]["tile_shape"]],
+                 "trials": [{"tile_shape": SHAPES[t["tile_shape"]], "ms_per_step": round(t["ms_per_step"], 5)}
+                            for t in tuned["trials"]]}
     # the clock sampler runs from before the warm-up to the end of the timed region
     sampler = ClockSampler(local) if clocks else None
     if sampler:
@@ -313,7 +322,7 @@ def measure_instance(p, soa, precision, steps, warmup, local, pg, opts=(), profi
     g.profile(False)
     timing = amortise_binning(g, ms, steps, prof, opts)
     return g, stream, {"ms": ms, "ms_amortised": timing["ms_amortised"], "timing": timing, "launches": launches,
-                       "prof": prof, "clocks": sampler.summary() if sampler else None}
+                       "prof": prof, "clocks": sampler.summary() if sampler else None, "tuned": tuned}
 
 
 RESORT_EVERY = 64   # the library's default re-binning interval (icy_mpm "resort_every")
@@ -378,10 +387,13 @@ def measure_batch(n_instances=256, steps=500, seed=7):
     from icempm_multi_b200.batch import Batch
     from icempm_multi_b200.workloads import batch_scenarios, make_workload as mk
     ws = batch_scenarios(n_instances, seed=seed)
+    scenes = [mk(w) for w in ws]
+    from icempm_multi_b200.autotune import SHAPES, tune_batch_shape
+    shape = tune_batch_shape(scenes, sample=32, steps=10)
     b = Batch(n_instances)
+    b.set_option("tile_shape", shape["tile_shape"])
     npts = 0
-    for w in ws:
-        p, soa = mk(w)
+    for p, soa in scenes:
         b.add(p, soa)
         npts += soa.size
     from icempm_multi_b200.autotune import tune_batch
@@ -401,7 +413,9 @@ def measure_batch(n_instances=256, steps=500, seed=7):
     b.close()
     return {"value": npts * steps / (ms / 1e3), "unit": METRIC, "instances": n_instances, "points": npts,
             "steps": steps, "ms_per_step": ms / steps, "gpu_launches": int(launches),
-            "autotuned": tuned["settings"],
+            "autotuned": dict(tuned["settings"], tile_shape=SHAPES[shape["tile_shape"]]),
+            "shape_trials": [{"tile_shape": SHAPES[t["tile_shape"]], "ps_per_point_step": round(t["ps_per_point_step"], 2)}
+                             for t in shape["trials"]],
             "timing": f"one call of {steps} steps, the members' re-binnings (every 256 steps) included",
             "workload": "floe scenarios: points log-uniform 10k-500k, grids 128x128..1024x512 (h=0.1 m), "
                         "E U(5e8,2e9), phi U(45,70), indenter U(0.5,3) m/s, CFL dt, FP32 split, CUDA graph"}
@@ -439,6 +453,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default tile shape (no autotuning)")
     ap.add_argument("--no-extra", action="store_true",
                     help="time only the headline path (no other precision, batched or served legs)")
     ap.add_argument("--workload", default="large", choices=["large", "medium", "small"],
@@ -465,7 +480,8 @@ def main():
     soa0 = soa.clone() if not args.no_extra else None
 
     # ---- headline path, device-resident timed region ----------------------------------
-    g, stream, r = measure_instance(p, soa, args.precision, args.steps, args.warmup, local, pg, args.opt)
+    g, stream, r = measure_instance(p, soa, args.precision, args.steps, args.warmup, local, pg, args.opt,
+                                    tune=not args.no_tune)
     ms = max_over_ranks(pg, r["ms_amortised"], local)
     value = replica_rate(n, args.steps, world, ms)
 
@@ -502,7 +518,9 @@ def main():
                    "points": n, "precision": args.precision + (" split" if args.precision == "fp32" else ""),
                    "l2": f"inputs larger than L2 (particle state {n * (36 if args.precision == 'fp32' else 128) / 1e9:.2f} GB "
                          "read and written per step; no extra flush)", "replicas": world,
-                   "options": args.opt},
+                   "options": args.opt,
+                   "tile_shape": (r["tuned"] or {}).get("tile_shape", "32x8"),
+                   "autotune": r["tuned"]},
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 16 * 8 * n / args.steps,
                 "d2h_bytes_per_step": 16 * 8 * n * downloads / args.steps, "frame_steps": frame,
                 "downloads": downloads},

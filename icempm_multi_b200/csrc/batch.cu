@@ -25,7 +25,7 @@ bool batch_const_acquire(int device, const void *batch);
 void batch_const_release(int device, const void *batch);
 cudaError_t batch_const_upload(const SplitArgs *args, int n, cudaStream_t s);
 cudaError_t batch_const_setup();
-void batch_const_launch_tile(int kind, int grid, cudaStream_t s, const SplitArgs &none, const SplitArgs *args,
+void batch_const_launch_tile(int kind, int shape, int grid, cudaStream_t s, const SplitArgs &none, const SplitArgs *args,
                              const BatchItem *work, const int *nwork, const int *rec);
 }
 
@@ -71,6 +71,7 @@ struct icy_batch {
     std::map<int, cudaGraphExec_t> graphs;
     std::map<int, int> graph_launches;   // kernels per replay
     int tile_grid = 0, update_grid = 0;
+    int shape = SHAPE_32X8;         // members' tile shape (option "tile_shape", set while the batch is empty)
     bool cargs = false;              // owns the device's constant-bank argument table (batch_cargs.cu)
     int64_t launches = 0;
 };
@@ -170,10 +171,13 @@ template <bool DO_G2P, bool DO_P2G, bool WRITE_VB>
 static void launch_tile_batch(icy_batch *b, const SplitArgs &none, size_t smem, int kind)
 {
     if (b->cargs)
-        batch_const_launch_tile(kind, b->tile_grid, b->stream, none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+        batch_const_launch_tile(kind, b->shape, b->tile_grid, b->stream, none, b->d_args, b->d_work, b->d_nwork,
+                                b->d_rec);
     else
-        k_tile_f32<DO_G2P, DO_P2G, WRITE_VB, true><<<b->tile_grid, TILE_THREADS_F32, smem, b->stream>>>(
-            none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+        with_shape(b->shape, [&](auto sh) {
+            k_tile_f32<DO_G2P, DO_P2G, WRITE_VB, true, false, decltype(sh)>
+                <<<b->tile_grid, TILE_THREADS_F32, smem, b->stream>>>(none, b->d_args, b->d_work, b->d_nwork, b->d_rec);
+        });
 }
 
 // Capture [P2G] + nsteps x [advance, update, G2P(+P2G)] as a graph.
@@ -188,8 +192,10 @@ static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
     n++;
     for (int k = 0; k < nsteps; k++) {
         k_batch_advance<<<(b->nslots + 127) / 128, 128, 0, b->stream>>>(b->d_clk, b->d_rec, b->nslots);
-        k_update_list_f32<true><<<b->update_grid, 256, 0, b->stream>>>(SplitArgs{}, b->d_args, b->d_clk, b->d_tlist,
-                                                                          b->d_tlist_n, 0.0, 0.0);
+        with_shape(b->shape, [&](auto sh) {
+            k_update_list_f32<true, decltype(sh)><<<b->update_grid, 256, 0, b->stream>>>(
+                SplitArgs{}, b->d_args, b->d_clk, b->d_tlist, b->d_tlist_n, 0.0, 0.0);
+        });
         if (k + 1 < nsteps)
             launch_tile_batch<true, true, false>(b, none, MOMF_BYTES, 1);
         else
@@ -275,10 +281,14 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
     cudaMemsetAsync(b->d_tlist_n, 0, sizeof(unsigned) * 2, b->stream);
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaFuncSetAttribute(k_tile_f32<true, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)MOMF_BYTES);
-    cudaFuncSetAttribute(k_tile_f32<false, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)MOMF_BYTES);
+    for (int sh = 0; sh < N_SHAPES; sh++)
+        with_shape(sh, [&](auto s) {
+            using S = decltype(s);
+            cudaFuncSetAttribute(k_tile_f32<true, true, false, true, false, S>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MOMF_BYTES);
+            cudaFuncSetAttribute(k_tile_f32<false, true, false, true, false, S>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MOMF_BYTES);
+        });
     if ((e = batch_const_setup()) != cudaSuccess) return fail(e, "cudaFuncSetAttribute");
     b->cargs = max_instances <= batch_const_slots() && batch_const_acquire(device, b);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false, true>, TILE_THREADS_F32,
@@ -346,6 +356,10 @@ static int add_member(icy_batch *b, const icy_sim_params *p, const double *hssoa
     icy_mpm *h = nullptr;
     int rc = icy_mpm_create(p, b->device, std::max(size, 1u), ICY_PRECISION_FP32_SPLIT, &h);
     if (rc) return rc;
+    if (b->shape != SHAPE_32X8 && (rc = icy_instance_set_shape(h, b->shape))) {
+        icy_mpm_destroy(h);
+        return rc;
+    }
     h->stream = b->side;
     if ((rc = icy_mpm_update_constants(h, p)) || (rc = icy_mpm_transfer_points_to_device(h, hssoa, capacity, size)) ||
         (rc = icy_mpm_reset_indenter_force_accumulator(h)) || (rc = icy_instance_bin(h))) {
@@ -604,6 +618,13 @@ int icy_batch_set_option(icy_batch *b, const char *name, double value)
     }
     if (std::strcmp(name, "update_ctas") == 0 && value >= 1 && value <= (1 << 20)) {   // CTAs of the grid update
         b->update_grid = (int)value;
+        drop_graphs(b);
+        return ICY_OK;
+    }
+    if (std::strcmp(name, "tile_shape") == 0 && value >= 0 && value < N_SHAPES) {   // members' tile shape
+        for (int k = 0; k < b->nslots; k++)
+            if (b->members[k] || b->retiring[k].h) return ICY_ERR_NOT_SUPPORTED;   // only while empty
+        b->shape = (int)value;
         drop_graphs(b);
         return ICY_OK;
     }

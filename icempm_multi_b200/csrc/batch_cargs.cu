@@ -49,24 +49,36 @@ cudaError_t batch_const_upload(const SplitArgs *args, int n, cudaStream_t s)
 
 cudaError_t batch_const_setup()
 {
-    cudaError_t e = cudaFuncSetAttribute(k_tile_f32<true, true, false, true>,
+    cudaError_t e = cudaSuccess;
+    for (int sh = 0; sh < N_SHAPES; sh++)
+        with_shape(sh, [&](auto s) {
+            using S = decltype(s);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_tile_f32<true, true, false, true, false, S>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MOMF_BYTES);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_tile_f32<false, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)MOMF_BYTES);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_tile_f32<false, true, false, true, false, S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MOMF_BYTES);
+        });
     return e;
 }
 
-// kind 0: first P2G, 1: fused G2P + P2G, 2: last G2P (as in batch.cu)
-void batch_const_launch_tile(int kind, int grid, cudaStream_t s, const SplitArgs &none, const SplitArgs *args,
-                             const BatchItem *work, const int *nwork, const int *rec)
+// kind 0: first P2G, 1: fused G2P + P2G, 2: last G2P (as in batch.cu), tile shape `shape`
+void batch_const_launch_tile(int kind, int shape, int grid, cudaStream_t s, const SplitArgs &none,
+                             const SplitArgs *args, const BatchItem *work, const int *nwork, const int *rec)
 {
-    if (kind == 0)
-        k_tile_f32<false, true, false, true><<<grid, TILE_THREADS_F32, MOMF_BYTES, s>>>(none, args, work, nwork, rec);
-    else if (kind == 1)
-        k_tile_f32<true, true, false, true><<<grid, TILE_THREADS_F32, MOMF_BYTES, s>>>(none, args, work, nwork, rec);
-    else
-        k_tile_f32<true, false, true, true><<<grid, TILE_THREADS_F32, 0, s>>>(none, args, work, nwork, rec);
+    with_shape(shape, [&](auto sh) {
+        using S = decltype(sh);
+        if (kind == 0)
+            k_tile_f32<false, true, false, true, false, S><<<grid, TILE_THREADS_F32, MOMF_BYTES, s>>>(none, args, work,
+                                                                                                      nwork, rec);
+        else if (kind == 1)
+            k_tile_f32<true, true, false, true, false, S><<<grid, TILE_THREADS_F32, MOMF_BYTES, s>>>(none, args, work,
+                                                                                                     nwork, rec);
+        else
+            k_tile_f32<true, false, true, true, false, S><<<grid, TILE_THREADS_F32, 0, s>>>(none, args, work, nwork,
+                                                                                            rec);
+    });
 }
 
 }  // namespace icy_dev

@@ -285,6 +285,8 @@ int icy_mpm_set_option(icy_mpm *h, const char *name, double value)
         h->primed = false;
     } else if (k == "fuse_update") {
         h->fuse_update = value != 0;
+    } else if (k == "tile_shape") {
+        return icy_instance_set_shape(h, (int)value);
     } else {
         return ICY_ERR_INVALID_ARGUMENT;
     }

@@ -97,6 +97,107 @@ static void status_slot_put(int *s)
     g_free_slots.push_back(s);
 }
 
+// tile dimensions of the instance: FP32 instances take their shape, FP64 32 x 8
+static void tile_dims(const icy_mpm *h, int &tx, int &ty)
+{
+    tx = TX;
+    ty = TY;
+    if (h->precision == ICY_PRECISION_FP32_SPLIT)
+        with_shape(h->shape, [&](auto sh) {
+            tx = decltype(sh)::TX;
+            ty = decltype(sh)::TY;
+        });
+}
+
+// The arrays whose size depends on the tile shape (cell ranges, sort counts,
+// tile lists and marks) and the launch sizes of the tile kernels.
+static int alloc_tiles(icy_mpm *h)
+{
+    int tx, ty;
+    tile_dims(h, tx, ty);
+    const int nx = h->prm.GridXTotal + 2 * h->prm.GridHaloSize;
+    h->ntx = (nx + tx - 1) / tx;
+    h->nty = (h->prm.GridY + ty - 1) / ty;
+    h->ntiles = h->ntx * h->nty;
+    const long nkeys = (long)h->ntiles * tx * ty + 1;   // cells + the disabled / out-of-grid bucket
+    h->scan_blocks = (int)((nkeys + SCAN_BLOCK - 1) / SCAN_BLOCK);
+    CK(dalloc(h, &h->d_counts, nkeys));
+    CK(dalloc(h, &h->d_start, nkeys + 1));
+    CK(dalloc(h, &h->d_block_sums, h->scan_blocks));
+    CK(dalloc(h, &h->d_active, h->ntiles));
+    CK(dalloc(h, &h->d_flags, h->ntiles));
+    CK(dalloc(h, &h->d_tlist, h->ntiles));
+    CK(dalloc(h, &h->d_nexp, h->ntiles));
+    CK(dalloc(h, &h->d_ncnt, h->ntiles));
+    CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
+    CK(cudaMemsetAsync(h->d_nexp, 0, sizeof(int) * h->ntiles, h->stream));
+    CK(cudaMemsetAsync(h->d_ncnt, 0, sizeof(int) * h->ntiles, h->stream));
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+    h->update_grid = (int)std::max(1L, std::min((long)(h->ntiles + 1) / 2, (long)sms * 8));
+    if (h->precision == ICY_PRECISION_FP32_SPLIT) {
+        cudaError_t e = cudaSuccess;
+        with_shape(h->shape, [&](auto sh) {
+            using S = decltype(sh);
+            int per_sm = 0;
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_tile_f32<true, true, false, false, false, S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MOMF_BYTES);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_tile_f32<false, true, false, false, false, S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MOMF_BYTES);
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false, false, false, S>,
+                                                                  TILE_THREADS_F32, MOMF_BYTES);
+            h->tile_grid_f32 = std::max(1, sms * std::max(per_sm, 1));
+            per_sm = 0;
+            if (e == cudaSuccess)
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_update_tiles_f32<S>, S::TT, 0);
+            h->update_grid_f32 = (int)std::max(1L, std::min((long)h->ntiles, (long)sms * std::max(per_sm, 1)));
+        });
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_tile_f32<true, true, false, false, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MOMF_BYTES);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_tile_f32<false, true, false, false, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MOMF_BYTES);
+        CK(e);
+    }
+    return ICY_OK;
+}
+
+static void free_tiles(icy_mpm *h)
+{
+    void *ptrs[] = {h->d_counts, h->d_start, h->d_block_sums, h->d_active, h->d_flags, h->d_tlist, h->d_nexp,
+                    h->d_ncnt};
+    for (void *p : ptrs)
+        if (p) cudaFreeAsync(p, h->stream);
+    h->d_counts = h->d_start = h->d_block_sums = h->d_active = nullptr;
+    h->d_flags = nullptr;
+    h->d_tlist = nullptr;
+    h->d_nexp = h->d_ncnt = nullptr;
+}
+
+// FP32 tile shape of an instance (option "tile_shape"): the shape-dependent
+// arrays are made anew and the points binned again at the next step.
+int icy_instance_set_shape(icy_mpm *h, int shape)
+{
+    if (shape < 0 || shape >= N_SHAPES) return ICY_ERR_INVALID_ARGUMENT;
+    if (h->precision != ICY_PRECISION_FP32_SPLIT || shape == h->shape) {
+        if (h->precision != ICY_PRECISION_FP32_SPLIT && shape != SHAPE_32X8) return ICY_ERR_NOT_SUPPORTED;
+        return ICY_OK;
+    }
+    CK(cudaSetDevice(h->device));
+    free_tiles(h);
+    h->shape = shape;
+    if (int rc = alloc_tiles(h)) return rc;
+    CK(cudaMemsetAsync(h->d_tlist_n, 0, sizeof(unsigned) * 2, h->stream));
+    CK(cudaMemsetAsync(h->d_nactive, 0, sizeof(int), h->stream));
+    h->binned = false;
+    h->primed = false;
+    return ICY_OK;
+}
+
 int icy_instance_allocate(icy_mpm *h, unsigned capacity)
 {
     const bool split = h->precision == ICY_PRECISION_FP32_SPLIT;
@@ -107,9 +208,6 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     h->pitch = ((long)capacity + 31) / 32 * 32;
     const int nx = h->prm.GridXTotal + 2 * h->prm.GridHaloSize;
     h->n_nodes = (long)h->prm.GridY * nx;
-    h->ntx = (nx + TX - 1) / TX;
-    h->nty = (h->prm.GridY + TY - 1) / TY;
-    h->ntiles = h->ntx * h->nty;
     if (nx > 32767 || h->prm.GridY > 32767) return ICY_ERR_INVALID_ARGUMENT;   // packed 16-bit base/cell indices
     cudaError_t e;
     if (split) {
@@ -146,18 +244,9 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(dalloc(h, &h->d_oidx_alt, h->pitch));
     CK(dalloc(h, &h->d_keys, h->pitch));
     CK(dalloc(h, &h->d_ranks, h->pitch));
-    const long nkeys = (long)h->ntiles * TT + 1;   // cells + the disabled / out-of-grid bucket
-    h->scan_blocks = (int)((nkeys + SCAN_BLOCK - 1) / SCAN_BLOCK);
-    CK(dalloc(h, &h->d_counts, nkeys));
-    CK(dalloc(h, &h->d_start, nkeys + 1));
-    CK(dalloc(h, &h->d_block_sums, h->scan_blocks));
-    CK(dalloc(h, &h->d_active, h->ntiles));
+    if (int rc = alloc_tiles(h)) return rc;
     CK(dalloc(h, &h->d_nactive, 1));
-    CK(dalloc(h, &h->d_flags, h->ntiles));
-    CK(dalloc(h, &h->d_tlist, h->ntiles));
     CK(dalloc(h, &h->d_tlist_n, 2));
-    CK(dalloc(h, &h->d_nexp, h->ntiles));
-    CK(dalloc(h, &h->d_ncnt, h->ntiles));
     CK(dalloc(h, &h->d_unsafe, 2));
     CK(dalloc(h, &h->d_moved, 3));
     CK(dalloc(h, &h->d_acc, 2 * h->prm.n_indenter_subdivisions));
@@ -165,10 +254,7 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(dalloc(h, &h->d_grain, GRAIN_TAB));
     h->h_status = status_slot_get();
     if (!h->h_status) return ICY_ERR_OUT_OF_MEMORY;
-    CK(cudaMemsetAsync(h->d_flags, 0, sizeof(unsigned) * h->ntiles, h->stream));
     CK(cudaMemsetAsync(h->d_tlist_n, 0, sizeof(unsigned) * 2, h->stream));
-    CK(cudaMemsetAsync(h->d_nexp, 0, sizeof(int) * h->ntiles, h->stream));
-    CK(cudaMemsetAsync(h->d_ncnt, 0, sizeof(int) * h->ntiles, h->stream));
     CK(cudaMemsetAsync(h->d_unsafe, 0xff, sizeof(int) * 2, h->stream));
     CK(cudaMemsetAsync(h->d_nactive, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_moved, 0, sizeof(unsigned long long) * 3, h->stream));
@@ -183,22 +269,6 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     h->tile_grid = std::max(1, sms * std::max(per_sm, 1));
     CK(cudaFuncSetAttribute(k_tile_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PIPE_SMEM));
     h->pipe_grid = sms;
-    per_sm = 0;
-    CK(cudaFuncSetAttribute(k_tile_f32<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)MOMF_BYTES));
-    CK(cudaFuncSetAttribute(k_tile_f32<false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)MOMF_BYTES));
-    CK(cudaFuncSetAttribute(k_tile_f32<true, true, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)MOMF_BYTES));
-    CK(cudaFuncSetAttribute(k_tile_f32<false, true, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)MOMF_BYTES));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tile_f32<true, true, false>, TILE_THREADS_F32,
-                                                     MOMF_BYTES));
-    h->tile_grid_f32 = std::max(1, sms * std::max(per_sm, 1));
-    h->update_grid = (int)std::max(1L, std::min((long)(h->ntiles + 1) / 2, (long)sms * 8));
-    per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_update_tiles_f32, TT, 0));
-    h->update_grid_f32 = (int)std::max(1L, std::min((long)h->ntiles, (long)sms * std::max(per_sm, 1)));
     if (int rc = icy_instance_constants(h)) return rc;
     CK(cudaStreamSynchronize(h->stream));
     return ICY_OK;
@@ -312,12 +382,16 @@ int icy_instance_bin(icy_mpm *h)
     if (!h->n) { h->binned = true; return ICY_OK; }
     StepParams P = icy_step_params(h->prm);
     const int nb = (h->n + 255) / 256;
-    const int nkeys = h->ntiles * TT + 1;
+    int stx, sty;
+    tile_dims(h, stx, sty);
+    const int nkeys = h->ntiles * stx * sty + 1;
     icy_prof_begin(h, K_BIN);
     CK(cudaMemsetAsync(h->d_counts, 0, sizeof(int) * nkeys, h->stream));
     if (is_split(h))
-        k_bin_count_f32<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_st, (int)h->n, h->d_keys, h->d_ranks,
-                                                   h->d_counts, h->d_status);
+        with_shape(h->shape, [&](auto sh) {
+            k_bin_count_f32<decltype(sh)><<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_st, (int)h->n, h->d_keys,
+                                                                      h->d_ranks, h->d_counts, h->d_status);
+        });
     else
         k_bin_count<<<nb, 256, 0, h->stream>>>(P, tile_geom(h), h->d_pts, h->pitch, (int)h->n, h->d_keys,
                                                h->d_ranks, h->d_counts, h->d_status);
@@ -328,12 +402,21 @@ int icy_instance_bin(icy_mpm *h)
     CK_LAUNCH("k_scan_blocks");
     k_scan_apply<<<h->scan_blocks, SCAN_NT, 0, h->stream>>>(h->d_counts, nkeys, h->d_block_sums, h->d_start);
     CK_LAUNCH("k_scan_apply");
-    k_tiles_active<<<1, 1024, 0, h->stream>>>(h->d_start, h->ntiles, h->d_active, h->d_nactive);
+    if (is_split(h))
+        with_shape(h->shape, [&](auto sh) {
+            k_tiles_active<decltype(sh)::TT><<<1, 1024, 0, h->stream>>>(h->d_start, h->ntiles, h->d_active,
+                                                                         h->d_nactive);
+        });
+    else
+        k_tiles_active<<<1, 1024, 0, h->stream>>>(h->d_start, h->ntiles, h->d_active, h->d_nactive);
     CK_LAUNCH("k_tiles_active");
     if (is_split(h)) {
         // fused grid update: contributors per node tile for this binning, counts and
         // margin flags from zero
-        k_node_tile_expect<<<(h->ntiles + 255) / 256, 256, 0, h->stream>>>(tile_geom(h), h->d_start, h->d_nexp);
+        with_shape(h->shape, [&](auto sh) {
+            k_node_tile_expect<decltype(sh)><<<(h->ntiles + 255) / 256, 256, 0, h->stream>>>(tile_geom(h), h->d_start,
+                                                                                           h->d_nexp);
+        });
         CK_LAUNCH("k_node_tile_expect");
         CK(cudaMemsetAsync(h->d_ncnt, 0, sizeof(int) * h->ntiles, h->stream));
         CK(cudaMemsetAsync(h->d_unsafe, 0xff, sizeof(int) * 2, h->stream));
@@ -454,7 +537,7 @@ static double step_move_cells(const icy_sim_params &p)
 static int launch_tile_split(icy_mpm *h, int which, bool record, double ind_x = 0.0, double ind_y = 0.0)
 {
     SplitArgs A = split_args(h, record);
-    if (which != 2 && h->fuse_update) {
+    if (which != 2 && h->fuse_update && h->shape == SHAPE_32X8) {
         // every launch with a P2G tests whether a point can leave the staged margin
         // in the step after it (the P2G-only launch that starts a call too, so that
         // the test covers every step a fused launch follows); only G2P + P2G
@@ -467,27 +550,30 @@ static int launch_tile_split(icy_mpm *h, int which, bool record, double ind_x = 
             A.ind_y = ind_y;
         }
     }
-    const bool fuse = A.seq > 0;
-    switch (which) {
-    case 0:
-        icy_prof_begin(h, K_TILE_G2P2G);
-        if (fuse)
-            k_tile_f32<true, true, false, false, true><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
-        else
-            k_tile_f32<true, true, false><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
-        break;
-    case 1:
-        icy_prof_begin(h, K_TILE_P2G);
-        if (fuse)
-            k_tile_f32<false, true, false, false, true><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
-        else
-            k_tile_f32<false, true, false><<<h->tile_grid_f32, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
-        break;
-    default:
-        icy_prof_begin(h, K_TILE_G2P);
-        k_tile_f32<true, false, true><<<h->tile_grid_f32, TILE_THREADS_F32, 0, h->stream>>>(A);
-        break;
-    }
+    const bool fuse = A.seq > 0;   // only with the 32 x 8 shape (see above)
+    const int kinds[3] = {K_TILE_G2P2G, K_TILE_P2G, K_TILE_G2P};
+    icy_prof_begin(h, kinds[which < 0 || which > 2 ? 2 : which]);
+    with_shape(h->shape, [&](auto sh) {
+        using S = decltype(sh);
+        const int grid = h->tile_grid_f32;
+        switch (which) {
+        case 0:
+            if (fuse)
+                k_tile_f32<true, true, false, false, true><<<grid, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
+            else
+                k_tile_f32<true, true, false, false, false, S><<<grid, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
+            break;
+        case 1:
+            if (fuse)
+                k_tile_f32<false, true, false, false, true><<<grid, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
+            else
+                k_tile_f32<false, true, false, false, false, S><<<grid, TILE_THREADS_F32, MOMF_BYTES, h->stream>>>(A);
+            break;
+        default:
+            k_tile_f32<true, false, true, false, false, S><<<grid, TILE_THREADS_F32, 0, h->stream>>>(A);
+            break;
+        }
+    });
     icy_prof_end(h);
     CK_LAUNCH("k_tile_f32");
     return ICY_OK;
@@ -531,9 +617,11 @@ static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y, int ctas 
     StepParams P = icy_step_params(h->prm);
     icy_prof_begin(h, K_UPDATE_TILES);
     if (is_split(h)) {
-        k_update_tiles_f32<<<ctas > 0 ? ctas : h->update_grid_f32, TT, 0, h->stream>>>(split_args(h, false),
-                                                                                     h->d_tlist, h->d_tlist_n,
-                                                                                     ind_x, ind_y);
+        with_shape(h->shape, [&](auto sh) {
+            using S = decltype(sh);
+            k_update_tiles_f32<S><<<ctas > 0 ? ctas : h->update_grid_f32, S::TT, 0, h->stream>>>(
+                split_args(h, false), h->d_tlist, h->d_tlist_n, ind_x, ind_y);
+        });
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemsetAsync(h->d_tlist_n, 0, sizeof(unsigned) * 2, h->stream);
         if (e != cudaSuccess) { icy_set_error("k_update_tiles_f32", e); return ICY_ERR_CUDA; }

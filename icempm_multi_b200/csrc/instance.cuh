@@ -44,6 +44,7 @@ struct icy_mpm {
     int *d_unsafe = nullptr;        // [2] margin flags of the last launches, by parity
     int fuse_seq = 0;               // fused-capable launches since the last binning
     bool fuse_update = false;       // grid update fused into the tile kernel where safe (option "fuse_update")
+    int shape = 0;                  // FP32 tile shape (option "tile_shape", kernels_split.cuh SHAPE_*)
     void *d_grainf = nullptr;
     int tile_grid_f32 = 0;
     icy_dev::GrainConst *d_grain = nullptr;   // failure-surface constants per grain slot
@@ -108,3 +109,4 @@ int icy_phase_g2p(icy_mpm *h, bool recordPQ);
 int icy_instance_steps(icy_mpm *h, int step0, int nsteps, double *sim_time);
 int icy_instance_bin(icy_mpm *h);
 int icy_instance_constants(icy_mpm *h);
+int icy_instance_set_shape(icy_mpm *h, int shape);

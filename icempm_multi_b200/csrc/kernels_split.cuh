@@ -34,6 +34,35 @@
 
 namespace icy_dev {
 
+// Tile shapes of the FP32 path: TX x TY cells (stencil bases) per tile and
+// the tile's staged node region (its bases, a drift margin of RM cells and
+// the +2 stencil reach).  32 x 8 is the default; the autotuner times the
+// others per workload (icempm_multi_b200/autotune.py).  Functions templated
+// on a shape declare its constants locally (ICY_TILE_SHAPE), shadowing the
+// 32 x 8 constants of kernels_tiled.cuh.
+template <int TX_, int TY_>
+struct TileShape {
+    static constexpr int TX = TX_, TY = TY_, TT = TX_ * TY_;
+    static constexpr int RX = TX_ + 2 + 2 * RM, RY = TY_ + 2 + 2 * RM, RN = RX * RY;
+};
+using Shape32x8 = TileShape<32, 8>;
+using Shape16x16 = TileShape<16, 16>;
+using Shape16x8 = TileShape<16, 8>;
+enum { SHAPE_32X8 = 0, SHAPE_16X16 = 1, SHAPE_16X8 = 2, N_SHAPES = 3 };
+#define ICY_TILE_SHAPE(S)                                                                                  \
+    [[maybe_unused]] constexpr int TX = S::TX, TY = S::TY, TT = S::TT, RX = S::RX, RY = S::RY, RN = S::RN
+
+// Runs f(S{}) with S the tile shape numbered `shape` (host code).
+template <class F>
+inline void with_shape(int shape, F &&f)
+{
+    switch (shape) {
+    case SHAPE_16X16: f(Shape16x16{}); break;
+    case SHAPE_16X8: f(Shape16x8{}); break;
+    default: f(Shape32x8{}); break;
+    }
+}
+
 constexpr int SB = 32;                   // points per block of the state
 constexpr int HOT_WORDS = 9 * SB;        // words of a block's hot part
 constexpr int COLD_WORDS = 8 * SB;       // words of a block's cold part
@@ -278,7 +307,6 @@ __device__ __forceinline__ bool load_point_f32(const unsigned *__restrict__ st, 
 constexpr int CAPF = 1280;                // points per chunk of the FP32 tile kernel
 constexpr int MOMF_N = CAPF + CAPF / 4;
 constexpr size_t MOMF_BYTES = (2 * sizeof(float4) + sizeof(float2)) * MOMF_N;
-static_assert(9 * TT * sizeof(float4) <= MOMF_BYTES, "cell partials alias the moment buffer");
 __device__ __forceinline__ int momf_col(int j) { return j + (j >> 2); }
 struct MomF {
     float4 *m0, *m1;
@@ -427,12 +455,13 @@ __device__ __forceinline__ void point_contributions_f32(float h, float gx, float
     }
 }
 
-template <bool AOS>
+template <bool AOS, class S>
 static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags, int2 *tlist, unsigned *tlist_n,
                                                    int inst, int ntx, int halo, float h, int bx, int by, float gx,
                                                    float gy, float mass, float mvx, float mvy, float s00, float s01,
                                                    float s10, float s11)
 {
+    ICY_TILE_SHAPE(S);
     point_contributions_f32(h, gx, gy, mass, mvx, mvy, s00, s01, s10, s11,
                             [&](int a, int b, float W, float dm, float tx, float ty) {
                                 g.add<AOS>(g.idx(bx + a, by + b), dm, W * tx, W * ty);
@@ -456,13 +485,15 @@ static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags,
 // gives the same sums: each cell's partials have a fixed place.
 constexpr int CNT_BUCKETS = 16;
 // every thread of the tile (tid < TT): its cell's count
-__device__ __forceinline__ void cell_order_count(int (&hist)[CNT_BUCKETS], int (&rank)[TT], int tid, int cnt)
+template <int NC>
+__device__ __forceinline__ void cell_order_count(int (&hist)[CNT_BUCKETS], int (&rank)[NC], int tid, int cnt)
 {
     const int b = CNT_BUCKETS - 1 - min(cnt, CNT_BUCKETS - 1);   // largest first
     rank[tid] = (b << 16) | atomicAdd(hist + b, 1);
 }
 // the first warp, after a barrier that follows every count
-__device__ __forceinline__ void cell_order_build(int (&hist)[CNT_BUCKETS], const int (&rank)[TT], int (&perm)[TT],
+template <int NC>
+__device__ __forceinline__ void cell_order_build(int (&hist)[CNT_BUCKETS], const int (&rank)[NC], int (&perm)[NC],
                                                  int lane)
 {
     const int h = lane < CNT_BUCKETS ? hist[lane] : 0;
@@ -476,19 +507,20 @@ __device__ __forceinline__ void cell_order_build(int (&hist)[CNT_BUCKETS], const
     __syncwarp();
     if (lane < CNT_BUCKETS) hist[lane] = 0;   // ready for the next tile
 #pragma unroll
-    for (int c = lane; c < TT; c += 32) {
+    for (int c = lane; c < NC; c += 32) {
         const int r = rank[c];
         perm[__shfl_sync(0xffffffffu, off, r >> 16) + (r & 0xffff)] = c;
     }
 }
 
 // phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32
-template <int NT, bool AOS, bool FUSE, typename Sync>
+template <int NT, bool AOS, bool FUSE, class S, typename Sync>
 __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int tid, int tx, int ty, int cs, int ce,
                                                         const int *s_cs, const int *s_perm, float *mom,
-                                                        float (*s_odd)[RN], unsigned &touch, unsigned &moved,
+                                                        float (*s_odd)[S::RN], unsigned &touch, unsigned &moved,
                                                         bool fused, Sync &&sync)
 {
+    ICY_TILE_SHAPE(S);
     const StepParams &P = A.P;
     const int X0 = tx * TX - P.halo, Y0 = ty * TY;
     const int RX0 = X0 - RM, RY0 = Y0 - RM;
@@ -541,7 +573,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                                             });
                 } else {
                     if (FUSE && fused) *A.status = ICY_DRIFT_CODE;   // excluded by the margin test of the last launch
-                    p2g_global_f32<AOS>(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by,
+                    p2g_global_f32<AOS, S>(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by,
                                         gx, gy, mass, mvx, mvy, s00, s01, s10, s11);
                 }
             }
@@ -646,10 +678,13 @@ __device__ __forceinline__ int node_velocity_f32(const StepParams &P, const Spli
 // each (the fused update of k_tile_f32): reads the finished sums (through L2:
 // other CTAs added them), writes the next velocities, clears the sums and
 // adds the indenter force of contact nodes to the bins.
+template <class S>
 __device__ __forceinline__ void update_node_tile_f32(const SplitArgs &A, int ntx_, int nty_, int l, double ind_x,
                                                      double ind_y)
 {
+    ICY_TILE_SHAPE(S);
     const StepParams &P = A.P;
+    if (l >= TT) return;
     const int gx = ntx_ * TX + l / TY - P.halo, gy = nty_ * TY + l % TY;
     if (gx >= P.gridx + P.halo || gy >= P.gridy) return;   // past the grid edge
     const long k = A.g.idx(gx, gy);
@@ -676,11 +711,13 @@ __device__ __forceinline__ void update_node_tile_f32(const SplitArgs &A, int ntx
 // forces go to the bins directly (a few hundred nodes touch the indenter).
 // The host clears the list after the kernel.
 constexpr int UPD_FLAT = 4;
-static __global__ void __launch_bounds__(TT) k_update_tiles_f32(const __grid_constant__ SplitArgs A,
-                                                               const int2 *__restrict__ tlist,
-                                                               const unsigned *__restrict__ tlist_n, double ind_x,
-                                                               double ind_y)
+template <class S>
+static __global__ void __launch_bounds__(S::TT) k_update_tiles_f32(const __grid_constant__ SplitArgs A,
+                                                                  const int2 *__restrict__ tlist,
+                                                                  const unsigned *__restrict__ tlist_n, double ind_x,
+                                                                  double ind_y)
 {
+    ICY_TILE_SHAPE(S);
     const StepParams &P = A.P;
     const unsigned n = *tlist_n;
     const int l = threadIdx.x;
@@ -727,7 +764,6 @@ static __global__ void __launch_bounds__(TT) k_update_tiles_f32(const __grid_con
 
 // Threads and resident CTAs per SM of the FP32 tile kernel.
 constexpr int TILE_THREADS_F32 = 256, TILE_CTAS_F32 = 3;
-static_assert(TILE_THREADS_F32 == TT, "one thread per cell of a tile in the cell phase");
 
 // Work items of a batch: (instance, tile) pairs over all instances.
 struct BatchItem { int inst, tile; };
@@ -736,10 +772,11 @@ struct BatchItem { int inst, tile; };
 // contiguous block range) or cell ranges (which == 8) into L2 while this CTA
 // is in its cell phase.
 constexpr int PF_PIECES = 8;
-template <bool BATCH>
+template <bool BATCH, class S>
 __device__ __forceinline__ void prefetch_next_item(const SplitArgs &A1, const SplitArgs *Aarr, const BatchItem *work,
                                                    int next, int na, int which)
 {
+    ICY_TILE_SHAPE(S);
     if (next >= na) return;
     const BatchItem w = BATCH ? work[next] : BatchItem{0, A1.active[next]};
     const SplitArgs &A = BATCH ? Aarr[w.inst] : A1;
@@ -761,11 +798,14 @@ __device__ __forceinline__ void prefetch_next_item(const SplitArgs &A1, const Sp
 // the record-PQ flag of each instance comes from rec[inst].  FUSE (single
 // instance, option "fuse_update"): P2G tests the drift margin for the next
 // step, and a G2P + P2G launch updates the grid itself where that is safe.
-template <bool DO_G2P, bool DO_P2G, bool WRITE_VB, bool BATCH = false, bool FUSE = false>
+template <bool DO_G2P, bool DO_P2G, bool WRITE_VB, bool BATCH = false, bool FUSE = false, class S = Shape32x8>
 static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     k_tile_f32(const __grid_constant__ SplitArgs A1, const SplitArgs *__restrict__ Aarr = nullptr, const BatchItem *__restrict__ work = nullptr,
                const int *__restrict__ nwork = nullptr, const int *__restrict__ rec = nullptr)
 {
+    ICY_TILE_SHAPE(S);
+    static_assert(TT <= TILE_THREADS_F32, "at most one cell per thread in the cell phase");
+    static_assert(9 * TT * sizeof(float4) <= MOMF_BYTES, "cell partials alias the moment buffer");
     __shared__ float2 s_v[RN];
     __shared__ float s_odd[3][RN];
     __shared__ int s_cs[TT + 1];
@@ -813,10 +853,12 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
         {
             // cell ranges; each thread counts its own cell's points for the cell order
             const int *cst = A.cell_start + (long)t * TT;
-            const int c0 = cst[tid], c1 = cst[tid + 1];
-            s_cs[tid] = c0;
-            if (tid == TT - 1) s_cs[TT] = c1;
-            if (DO_P2G) cell_order_count(s_hist, s_rank, tid, c1 - c0);
+            if (tid < TT) {
+                const int c0 = cst[tid], c1 = cst[tid + 1];
+                s_cs[tid] = c0;
+                if (tid == TT - 1) s_cs[TT] = c1;
+                if (DO_P2G) cell_order_count(s_hist, s_rank, tid, c1 - c0);
+            }
         }
         if (tid == 0) s_touch = 0;
         if (DO_G2P) {
@@ -876,7 +918,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             // and its cell ranges
             constexpr int PF0 = TILE_THREADS_F32 - (PF_PIECES + 1);
             if (DO_P2G && cs == ps && tid >= PF0)
-                prefetch_next_item<BATCH>(A1, Aarr, work, next, na, tid - PF0);
+                prefetch_next_item<BATCH, S>(A1, Aarr, work, next, na, tid - PF0);
             // and the first threads its staged node velocities (columns of vx and vy,
             // or of the float2 velocities of a batch member)
             static_assert(2 * RX <= PF0, "velocity-column and state prefetches on different threads");
@@ -885,10 +927,10 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                 const SplitArgs &An = BATCH ? Aarr[wn.inst] : A1;
                 const int nx0 = (wn.tile % An.G.ntx) * TX - An.P.halo - RM, ny0 = (wn.tile / An.G.ntx) * TY - RM;
                 if (BATCH)
-                    prefetch_region_column(An.g.v, An.P.gridx, An.P.gridy, An.P.halo, An.g.ny, nx0, ny0, tid);
+                    prefetch_region_column(An.g.v, An.P.gridx, An.P.gridy, An.P.halo, An.g.ny, nx0, ny0, tid, RY);
                 else
                     prefetch_region_column(tid < RX ? An.g.vx : An.g.vy, An.P.gridx, An.P.gridy, An.P.halo, An.g.ny,
-                                           nx0, ny0, tid % RX);
+                                           nx0, ny0, tid % RX, RY);
             }
             if (DO_P2G) {
                 if (cs == ps) {
@@ -896,7 +938,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                     if (tid < 32) cell_order_build(s_hist, s_rank, s_perm, tid);
                     __syncthreads();
                 }
-                p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH, FUSE>(A, tid, tx, ty, cs, ce, s_cs, s_perm, s_momf, s_odd,
+                p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH, FUSE, S>(A, tid, tx, ty, cs, ce, s_cs, s_perm, s_momf, s_odd,
                                                                  touch, moved, fused, [] { __syncthreads(); });
             }
         }
@@ -932,7 +974,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                 do {
                     const int q = __ffs(r) - 1;
                     r &= r - 1;
-                    update_node_tile_f32(A, tx + q % 3 - 1, ty + q / 3 - 1, tid, A.ind_x, A.ind_y);
+                    update_node_tile_f32<S>(A, tx + q % 3 - 1, ty + q / 3 - 1, tid, A.ind_x, A.ind_y);
                 } while (r);
             }
             moved = __reduce_add_sync(0xffffffffu, moved);
@@ -969,7 +1011,7 @@ constexpr int UPD_TILES = 4;
 
 // Grid update of the listed node tiles (see k_update_list in kernels_tiled.cuh),
 // defined after BatchClock below.
-template <bool BATCH>
+template <bool BATCH, class S = Shape32x8>
 static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_constant__ SplitArgs A1,
                                                                 const SplitArgs *__restrict__ Aarr,
                                                                 const BatchClock *__restrict__ clk,
@@ -977,9 +1019,11 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
                                                                 double ind_x, double ind_y);
 
 // ---------------------------------------------------------------- binning / conversion
+template <class S>
 static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__restrict__ st, int n, int *keys,
                                        int *ranks, int *counts, int *status)
 {
+    ICY_TILE_SHAPE(S);
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = i < n;
     int key = G.ntiles * TT;
@@ -990,7 +1034,7 @@ static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned 
             split_unpack(a.x, bx, by);
             const int e = base_error(P, bx, by);
             if (e) *status = e;
-            else key = G.cell_key(bx, by, P.halo);
+            else key = G.cell_key_s<TX, TY>(bx, by, P.halo);
         }
     }
     const unsigned act = __ballot_sync(0xffffffffu, in);
@@ -1091,8 +1135,10 @@ static __global__ void k_inverse_perm(const int *__restrict__ oidx, int n, int *
 
 // Per node tile: the number of cell tiles with points in its 3 x 3
 // neighbourhood (the contributors the fused grid update waits for).
+template <class S>
 static __global__ void k_node_tile_expect(TileGeom G, const int *__restrict__ cell_start, int *__restrict__ nexp)
 {
+    ICY_TILE_SHAPE(S);
     const int X = blockIdx.x * blockDim.x + threadIdx.x;
     if (X >= G.ntiles) return;
     const int x = X % G.ntx, y = X / G.ntx;
@@ -1141,13 +1187,14 @@ static __global__ void k_batch_advance(BatchClock *clk, int *rec, int nslots)
 // the list.  Alone (BATCH = false) the forces are summed per CTA in shared
 // memory; in a batch every entry names its member, whose indenter position
 // comes from the member's clock and whose force bins take the force directly.
-template <bool BATCH>
+template <bool BATCH, class S>
 static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_constant__ SplitArgs A1,
                                                                 const SplitArgs *__restrict__ Aarr,
                                                                 const BatchClock *__restrict__ clk,
                                                                 const int2 *__restrict__ tlist, unsigned *tlist_n,
                                                                 double ind_x, double ind_y)
 {
+    ICY_TILE_SHAPE(S);
     extern __shared__ double s_acc[];   // 2*nsub (alone only)
     const unsigned n = *(volatile unsigned *)tlist_n;
     if (!BATCH) {

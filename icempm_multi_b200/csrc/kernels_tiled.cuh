@@ -43,6 +43,13 @@ struct TileGeom {
         const int gx = bx + halo;
         return ((by / TY) * ntx + gx / TX) * TT + (gx % TX) * TY + (by % TY);
     }
+    // the same for tiles of STX x STY cells
+    template <int STX, int STY>
+    __device__ __forceinline__ int cell_key_s(int bx, int by, int halo) const
+    {
+        const int gx = bx + halo;
+        return ((by / STY) * ntx + gx / STX) * (STX * STY) + (gx % STX) * STY + (by % STY);
+    }
 };
 
 struct TileArgs {
@@ -189,8 +196,10 @@ static __global__ void __launch_bounds__(SCAN_NT) k_scan_apply(const int *in, in
 }
 
 // one CTA: ordered list of tiles that hold points
+template <int CELLS = TT>
 static __global__ void __launch_bounds__(1024) k_tiles_active(const int *cell_start, int ntiles, int *active, int *n_active)
 {
+    constexpr int TT = CELLS;   // cells per tile
     __shared__ int s_warp[32];
     const int per = (ntiles + 1023) / 1024;
     const int b = min((int)threadIdx.x * per, ntiles), e = min(b + per, ntiles);
@@ -581,7 +590,7 @@ __device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes)
 // the first and the last node's lines (a column spans at most two lines).
 template <typename T>
 __device__ __forceinline__ void prefetch_region_column(const T *arr, int gridx, int gridy, int halo, int ny, int RX0,
-                                                       int RY0, int col)
+                                                       int RY0, int col, int RY = icy_dev::RY)
 {
     const int gx = RX0 + col;
     if (gx < -halo || gx >= gridx + halo) return;

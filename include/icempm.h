@@ -262,6 +262,11 @@ int icy_mpm_status(icy_mpm *h);
  *                   list-driven update kernel; 0 = always the update kernel
  *                   (default: the counting at every tile's end costs the tile
  *                   kernel more than the update kernel takes)
+ *   "tile_shape"    FP32 split precision: cells per tile of the binned kernels,
+ *                   0 = 32 x 8 (default), 1 = 16 x 16, 2 = 16 x 8; the points are
+ *                   binned again at the next step (icempm_multi_b200/autotune.py
+ *                   times the shapes on a workload); the fused grid update runs
+ *                   with 32 x 8 tiles only; FP64 instances: 0 only
  *   "profile_every" n = icy_mpm_profile times every n-th launch of each kernel
  *                   (default 1; every re-binning is timed whatever n); an event
  *                   pair on the stream costs the step loop a few microseconds, so
@@ -360,7 +365,9 @@ int icy_batch_set_clock(icy_batch *b, int slot, double sim_time, int64_t step);
 /* "resort_every" (steps between re-binning, 0 = never), "tile_ctas"
    (persistent CTAs of the tile kernel), "update_ctas" (CTAs of the grid
    update); the CTA counts take effect from the next step call (the captured
-   graphs are dropped).  icempm_multi_b200/autotune.py picks them by timing. */
+   graphs are dropped); "tile_shape" (the members' cells per tile, as the
+   instance option; only while the batch has no members, else
+   ICY_ERR_NOT_SUPPORTED).  icempm_multi_b200/autotune.py picks them by timing. */
 int icy_batch_set_option(icy_batch *b, const char *name, double value);
 /* Live members, their total points, kernels launched so far, the batch stream. */
 int icy_batch_info(icy_batch *b, int *live, int64_t *points, int64_t *kernel_launches,
