@@ -193,11 +193,9 @@ static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
     for (int k = 0; k < nsteps; k++) {
         k_batch_advance<<<(b->nslots + 127) / 128, 128, 0, b->stream>>>(b->d_clk, b->d_rec, b->nslots);
         with_shape(b->shape, [&](auto sh) {
-            using S = decltype(sh);
-            k_update_tiles_f32<S, true><<<b->update_grid, S::TT, 0, b->stream>>>(SplitArgs{}, b->d_args, b->d_clk,
-                                                                                  b->d_tlist, b->d_tlist_n, 0.0, 0.0);
+            k_update_list_f32<true, decltype(sh)><<<b->update_grid, 256, 0, b->stream>>>(
+                SplitArgs{}, b->d_args, b->d_clk, b->d_tlist, b->d_tlist_n, 0.0, 0.0);
         });
-        cudaMemsetAsync(b->d_tlist_n, 0, sizeof(unsigned) * 2, b->stream);   // the list, for the next step
         if (k + 1 < nsteps)
             launch_tile_batch<true, true, false>(b, none, MOMF_BYTES, 1);
         else

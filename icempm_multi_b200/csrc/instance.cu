@@ -620,7 +620,7 @@ static int launch_update_tiles(icy_mpm *h, double ind_x, double ind_y, int ctas 
         with_shape(h->shape, [&](auto sh) {
             using S = decltype(sh);
             k_update_tiles_f32<S><<<ctas > 0 ? ctas : h->update_grid_f32, S::TT, 0, h->stream>>>(
-                split_args(h, false), nullptr, nullptr, h->d_tlist, h->d_tlist_n, ind_x, ind_y);
+                split_args(h, false), h->d_tlist, h->d_tlist_n, ind_x, ind_y);
         });
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemsetAsync(h->d_tlist_n, 0, sizeof(unsigned) * 2, h->stream);

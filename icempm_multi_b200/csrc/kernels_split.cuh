@@ -950,6 +950,15 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
 }
 
 struct BatchClock;
+constexpr int UPD_TILES = 4;
+
+// Grid update of a batch's listed node tiles, defined after BatchClock below.
+template <bool BATCH, class S = Shape32x8>
+static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_constant__ SplitArgs A1,
+                                                                const SplitArgs *__restrict__ Aarr,
+                                                                const BatchClock *__restrict__ clk,
+                                                                const int2 *__restrict__ tlist, unsigned *tlist_n,
+                                                                double ind_x, double ind_y);
 
 // ---------------------------------------------------------------- binning / conversion
 template <class S>
@@ -1115,33 +1124,100 @@ static __global__ void k_batch_advance(BatchClock *clk, int *rec, int nslots)
     clk[i] = c;
 }
 
-// Grid update of the node tiles P2G listed: TT threads per CTA, one node of
-// each of UPD_FLAT list entries per thread and pass, their loads issued
-// together so that many tiles' loads are in flight; contact forces go to the
-// bins directly (a few hundred nodes touch the indenter).  Alone the
-// velocities go to the buffer the next G2P reads; in a batch each entry
-// names its member (arguments Aarr[inst], indenter from its clock, grid as
-// float4 sums and float2 velocities).  The host clears the list after the
-// kernel.
+// Grid update of the node tiles P2G listed (single instance): TT threads per
+// CTA, one node of each of UPD_FLAT list entries per thread and pass, their
+// loads issued together so that many tiles' loads are in flight; contact
+// forces go to the bins directly (a few hundred nodes touch the indenter);
+// the velocities go to the buffer the next G2P reads.  The host clears the
+// list after the kernel.
 constexpr int UPD_FLAT = 4;
-template <class S, bool BATCH = false>
-static __global__ void __launch_bounds__(S::TT) k_update_tiles_f32(const __grid_constant__ SplitArgs A1,
-                                                                  const SplitArgs *__restrict__ Aarr,
-                                                                  const BatchClock *__restrict__ clk,
+template <class S>
+static __global__ void __launch_bounds__(S::TT) k_update_tiles_f32(const __grid_constant__ SplitArgs A,
                                                                   const int2 *__restrict__ tlist,
                                                                   const unsigned *__restrict__ tlist_n, double ind_x,
                                                                   double ind_y)
 {
     ICY_TILE_SHAPE(S);
+    const StepParams &P = A.P;
     const unsigned n = *tlist_n;
     const int l = threadIdx.x;
     for (unsigned e0 = blockIdx.x; e0 < n; e0 += gridDim.x * UPD_FLAT) {
         long q[UPD_FLAT];
-        int gx[UPD_FLAT], gy[UPD_FLAT], inst[UPD_FLAT];
+        int gx[UPD_FLAT], gy[UPD_FLAT];
         float m[UPD_FLAT], px[UPD_FLAT], py[UPD_FLAT];
 #pragma unroll
         for (int u = 0; u < UPD_FLAT; u++) {
             const unsigned e = e0 + u * gridDim.x;
+            q[u] = -1;
+            if (e >= n) continue;
+            const int2 it = tlist[e];
+            const int tx = it.y & 0xffff, ty = it.y >> 16;
+            if (l == 0) A.flags[ty * A.G.ntx + tx] = 0u;
+            gx[u] = tx * TX + l / TY - P.halo;
+            gy[u] = ty * TY + l % TY;
+            if (gx[u] >= P.gridx + P.halo || gy[u] >= P.gridy) continue;   // past the grid edge
+            q[u] = A.g.idx(gx[u], gy[u]);
+            m[u] = A.g.m[q[u]];
+            px[u] = A.g.px[q[u]];
+            py[u] = A.g.py[q[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < UPD_FLAT; u++) {
+            if (q[u] < 0) continue;
+            float vx, vy;
+            double fx = 0, fy = 0;
+            const int bin = node_velocity_f32(P, A.Q, gx[u], gy[u], m[u], px[u], py[u], ind_x, ind_y, vx, vy, fx, fy);
+            A.g.nvx[q[u]] = vx;
+            A.g.nvx[q[u] + A.n_nodes] = vy;
+            if (m[u] != 0.f || px[u] != 0.f || py[u] != 0.f) {
+                A.g.m[q[u]] = 0.f;
+                A.g.px[q[u]] = 0.f;
+                A.g.py[q[u]] = 0.f;
+            }
+            if (bin >= 0) {
+                atomicAdd(A.acc + 2 * bin, fx);
+                atomicAdd(A.acc + 2 * bin + 1, fy);
+            }
+        }
+    }
+}
+
+// Grid update of a batch's listed node tiles: each group of TT threads takes
+// one TX x TY node tile (one thread per node), clears its mark, and the last
+// CTA empties the list.  Every entry names its member, whose arguments are
+// looked up once per tile group, whose indenter position comes from the
+// member's clock and whose force bins take the force directly (for batches
+// this is faster than a batch form of k_update_tiles_f32 measured: its
+// per-entry lookups of member arguments cost more than its extra loads in
+// flight gain).  BATCH = false sums the forces per CTA in shared memory (no
+// caller: a single instance uses k_update_tiles_f32).
+template <bool BATCH, class S>
+static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_constant__ SplitArgs A1,
+                                                                const SplitArgs *__restrict__ Aarr,
+                                                                const BatchClock *__restrict__ clk,
+                                                                const int2 *__restrict__ tlist, unsigned *tlist_n,
+                                                                double ind_x, double ind_y)
+{
+    ICY_TILE_SHAPE(S);
+    extern __shared__ double s_acc[];   // 2*nsub (alone only)
+    const unsigned n = *(volatile unsigned *)tlist_n;
+    if (!BATCH) {
+        for (int k = threadIdx.x; k < 2 * A1.P.nsub; k += blockDim.x) s_acc[k] = 0;
+        __syncthreads();
+    }
+    bool any = false;
+    constexpr int TPC = 256 / TT;   // node tiles per CTA pass
+    static_assert(256 % TT == 0, "whole node tiles per 256-thread CTA");
+    const int l = threadIdx.x % TT;
+    const unsigned stride = gridDim.x * TPC;
+    // UPD_TILES tiles per pass, their loads issued together
+    for (unsigned e0 = blockIdx.x * TPC + threadIdx.x / TT; e0 < n; e0 += stride * UPD_TILES) {
+        long q[UPD_TILES];
+        int inst[UPD_TILES], gx[UPD_TILES], gy[UPD_TILES];
+        float m[UPD_TILES], px[UPD_TILES], py[UPD_TILES];
+#pragma unroll
+        for (int u = 0; u < UPD_TILES; u++) {
+            const unsigned e = e0 + u * stride;
             q[u] = -1;
             if (e >= n) continue;
             const int2 it = tlist[e];
@@ -1150,7 +1226,7 @@ static __global__ void __launch_bounds__(S::TT) k_update_tiles_f32(const __grid_
             const int tx = it.y & 0xffff, ty = it.y >> 16;
             if (l == 0) A.flags[ty * A.G.ntx + tx] = 0u;
             gx[u] = tx * TX + l / TY - A.P.halo;
-            gy[u] = ty * TY + l % TY;
+            gy[u] = ty * TY + (l & (TY - 1));
             if (gx[u] >= A.P.gridx + A.P.halo || gy[u] >= A.P.gridy) continue;   // past the grid edge
             q[u] = A.g.idx(gx[u], gy[u]);
             if constexpr (BATCH) {
@@ -1165,7 +1241,7 @@ static __global__ void __launch_bounds__(S::TT) k_update_tiles_f32(const __grid_
             }
         }
 #pragma unroll
-        for (int u = 0; u < UPD_FLAT; u++) {
+        for (int u = 0; u < UPD_TILES; u++) {
             if (q[u] < 0) continue;
             const SplitArgs &A = BATCH ? Aarr[inst[u]] : A1;
             float vx, vy;
@@ -1175,24 +1251,32 @@ static __global__ void __launch_bounds__(S::TT) k_update_tiles_f32(const __grid_
                                               vx, vy, fx, fy);
             if constexpr (BATCH) {
                 A.g.v[q[u]] = make_float2(vx, vy);
-                if (m[u] != 0.f || px[u] != 0.f || py[u] != 0.f) A.g.mp[q[u]] = make_float4(0.f, 0.f, 0.f, 0.f);
+                A.g.mp[q[u]] = make_float4(0.f, 0.f, 0.f, 0.f);
             } else {
-                A.g.nvx[q[u]] = vx;
+                A.g.nvx[q[u]] = vx;   // the velocities the next G2P reads
                 A.g.nvx[q[u] + A.n_nodes] = vy;
-                if (m[u] != 0.f || px[u] != 0.f || py[u] != 0.f) {
-                    A.g.m[q[u]] = 0.f;
-                    A.g.px[q[u]] = 0.f;
-                    A.g.py[q[u]] = 0.f;
-                }
+                A.g.m[q[u]] = 0.f;
+                A.g.px[q[u]] = 0.f;
+                A.g.py[q[u]] = 0.f;
             }
             if (bin >= 0) {
-                atomicAdd(A.acc + 2 * bin, fx);
-                atomicAdd(A.acc + 2 * bin + 1, fy);
+                if (BATCH) {
+                    atomicAdd(A.acc + 2 * bin, fx);
+                    atomicAdd(A.acc + 2 * bin + 1, fy);
+                } else {
+                    atomicAdd(&s_acc[2 * bin], fx);
+                    atomicAdd(&s_acc[2 * bin + 1], fy);
+                    any = true;
+                }
             }
         }
     }
+    if (!BATCH && __syncthreads_or(any))
+        for (int k = threadIdx.x; k < 2 * A1.P.nsub; k += blockDim.x)
+            if (s_acc[k] != 0.0) atomicAdd(A1.acc + k, s_acc[k]);
+    if (BATCH) __syncthreads();
+    if (threadIdx.x == 0) tile_list_done(tlist_n);
 }
-
 
 // (instance, tile) work list: offsets by an exclusive scan over the members'
 // non-empty-tile counts (one CTA), then a fill
