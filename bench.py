@@ -510,7 +510,8 @@ def main():
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get(f"{name}:{args.precision}")
+            per_point = json.load(open(tf))["bytes_per_point"].get(f"{name}:{args.precision}")
+            traffic = per_point * n if per_point is not None else None
         except Exception:
             traffic = None
 
