@@ -574,7 +574,7 @@ def main():
                 # over capacity with a budget the admitted scenarios fill: admission is
                 # held back by device memory, not by slots (at these request sizes the
                 # 150 GB budget would need about 1,300 resident requests to bind)
-                out["served_budget"] = measure_serve(rate=20.0, duration=6.0, budget=2.5e9, max_instances=512)
+                out["served_budget"] = measure_serve(rate=20.0, duration=6.0, budget=2.5e9, max_instances=300)
             except Exception as e:
                 out["batched_or_served_error"] = str(e)[:300]
         # ---- CPU baseline ------------------------------------------------------------------

@@ -23,7 +23,7 @@ namespace icy_dev {   // batch_cargs.cu
 int batch_const_slots();
 bool batch_const_acquire(int device, const void *batch);
 void batch_const_release(int device, const void *batch);
-cudaError_t batch_const_upload(const SplitArgs *args, int n, cudaStream_t s);
+cudaError_t batch_const_upload(const SplitArgs *args, const SplitArgs *d_args, int n, cudaStream_t s);
 cudaError_t batch_const_setup();
 void batch_const_launch_tile(int kind, int shape, int grid, cudaStream_t s, const SplitArgs &none, const SplitArgs *args,
                              const BatchItem *work, const int *nwork, const int *rec);
@@ -141,7 +141,7 @@ static int rebuild(icy_batch *b)
     for (int s = 0; s < b->nslots; s++)
         if (b->members[s]) args[s] = member_args(b, b->members[s], s);
     CKB(cudaMemcpyAsync(b->d_args, args.data(), sizeof(SplitArgs) * b->nslots, cudaMemcpyHostToDevice, b->stream));
-    if (b->cargs) CKB(batch_const_upload(args.data(), b->nslots, b->stream));
+    if (b->cargs) CKB(batch_const_upload(args.data(), b->d_args, b->nslots, b->stream));
     k_batch_work_offsets<<<1, 1024, 0, b->stream>>>(b->d_args, b->d_clk, b->nslots, b->d_woff, b->d_nwork);
     k_batch_work_fill<<<dim3(8, b->nslots), 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_woff, b->d_work);
     CKB(cudaGetLastError());

@@ -1,12 +1,13 @@
-// batch_cargs.cu -- the batched tile kernel for batches of at most 128 slots,
-// reading its members' arguments from a constant-bank copy of the batch's
-// argument table (ICY_BATCH_CONST_ARGS in kernels_split.cuh).  The batched
-// step is 5-6 % faster at 120 members than with the global table, which the
-// kernels of batch.cu read for larger batches.
+// batch_cargs.cu -- the batched tile kernel for batches of at most
+// BATCH_CONST_SLOTS (300) slots, reading its members' arguments from a
+// compact constant-bank copy of the batch's argument table (SplitMember,
+// ICY_BATCH_CONST_ARGS in kernels_split.cuh).  The kernels of batch.cu read
+// the global table, for larger batches.
 #include <cuda_runtime.h>
 
 #include <map>
 #include <mutex>
+#include <vector>
 
 #include "../../include/icempm.h"
 #define ICY_BATCH_CONST_ARGS
@@ -40,11 +41,14 @@ void batch_const_release(int device, const void *batch)
     if (it != g_owner.end() && it->second == batch) it->second = nullptr;
 }
 
-// args[0 .. n) into the constant bank of this module, on stream s (n <= 128)
-cudaError_t batch_const_upload(const SplitArgs *args, int n, cudaStream_t s)
+// args[0 .. n) (whose device copy is d_args) into the constant bank of this
+// module as compact member arguments, on stream s (n <= BATCH_CONST_SLOTS)
+cudaError_t batch_const_upload(const SplitArgs *args, const SplitArgs *d_args, int n, cudaStream_t s)
 {
     if (n > BATCH_CONST_SLOTS) return cudaErrorInvalidValue;
-    return cudaMemcpyToSymbolAsync(c_batch_args, args, sizeof(SplitArgs) * n, 0, cudaMemcpyHostToDevice, s);
+    std::vector<SplitMember> m(n);
+    for (int i = 0; i < n; i++) m[i] = split_member(args[i], d_args + i);
+    return cudaMemcpyToSymbolAsync(c_batch_mem, m.data(), sizeof(SplitMember) * n, 0, cudaMemcpyHostToDevice, s);
 }
 
 cudaError_t batch_const_setup()

@@ -173,6 +173,37 @@ __device__ __forceinline__ const unsigned *hot_vec(const unsigned *st, long i)
 __device__ __forceinline__ long hot_jp(long i) { return (i >> 5) * HOT_WORDS + 256 + (i & 31); }
 __device__ __forceinline__ long cold_vec(long pitch, long i) { return S_HOT * pitch + (i >> 5) * COLD_WORDS + (i & 31) * 4; }
 
+// The parameters a batch member's tile kernel reads from the constant bank:
+// the grid extent as ints, and the FP64 block (in global memory) for the
+// rare paths -- the crushed-point return mapping and liquid points.
+struct MemberP {
+    int halo, gridx, gridy;
+    unsigned blo, bhi;           // the valid stencil bases (-halo, 0) .. (gridx + halo - 3, gridy - 3), packed
+    const StepParams *p64;
+};
+__device__ __forceinline__ const StepParams &rare_params(const StepParams &P) { return P; }
+__device__ __forceinline__ const StepParams &rare_params(const MemberP &P) { return *P.p64; }
+
+// The reference's error code of a stencil base outside the grid (0 inside).
+// A batch member tests both axes at once on the packed base word bw, against
+// two packed bounds (the three separate bounds of base_error cost the batched
+// kernel registers and spills: 3 % of a batched step).
+__device__ __forceinline__ int split_base_error(const StepParams &P, unsigned, int bx, int by)
+{
+    return base_error(P, bx, by);
+}
+__device__ __forceinline__ int split_base_error(const MemberP &P, unsigned bw, int, int)
+{
+    const unsigned lo = __vcmpgeu2(bw, P.blo), hi = __vcmpgeu2(P.bhi, bw);   // per 16-bit half: 0xffff if in
+    if ((lo & hi) == 0xffffffffu) return 0;
+    int e = 0;                       // codes in base_error's order: the last that applies
+    if (!(lo >> 16)) e = 70;
+    if (!(lo & 0xffffu)) e = 71;
+    if (!(hi >> 16)) e = 72;
+    if (!(hi & 0xffffu)) e = 73;
+    return e;
+}
+
 // The return mapping of a crushed point in FP64 (kernels.cuh:540-545, 623-674)
 // from its FP32 state, out of line: few points take it, and keeping its FP64
 // registers out of the tile kernel's main path leaves room for more warps.
@@ -190,11 +221,11 @@ static __device__ __noinline__ SplitRm return_map_split(const StepParams &P, flo
     return SplitRm{(float)(F.a00 - 1.0), (float)F.a01, (float)F.a10, (float)(F.a11 - 1.0), (float)Jp};
 }
 
-template <typename VSrc>
-__device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitConsts &Q, const GrainConstF *tab,
+template <class PT, typename VSrc>
+__device__ __forceinline__ bool g2p_update_f32(const PT &P, const SplitConsts &Q, const GrainConstF *tab,
                                                PointF &s, int *status, VSrc &&vsrc)
 {
-    const int e = base_error(P, s.bx, s.by);
+    const int e = split_base_error(P, s.bw, s.bx, s.by);
     if (e) { *status = e; return false; }
     float wx[3], wy[3];
     weights_g(s.gx, wx);
@@ -255,7 +286,7 @@ __device__ __forceinline__ bool g2p_update_f32(const StepParams &P, const SplitC
             if (crushed) s.util |= (unsigned)kCrushed;
         }
         if (s.util & (unsigned)kCrushed) {
-            const SplitRm r = return_map_split(P, s.D.a00, s.D.a01, s.D.a10, s.D.a11, s.Jp);
+            const SplitRm r = return_map_split(rare_params(P), s.D.a00, s.D.a01, s.D.a10, s.D.a11, s.Jp);
             s.D = {r.d00, r.d01, r.d10, r.d11};
             s.Jp = r.jp;
         }
@@ -317,13 +348,14 @@ struct MomF {
     __device__ __forceinline__ void none(int j) const { m2[momf_col(j)] = make_float2(0.f, __int_as_float(BASE_NONE)); }
 };
 
-__device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const SplitConsts &Q, const PointF &s,
+template <class PT>
+__device__ __forceinline__ void p2g_moments_f32(const PT &P, const SplitConsts &Q, const PointF &s,
                                                 float *mom, int j, int *status)
 {
     const MomF M(mom);
     const bool liquid = (s.util & (unsigned)kLiquid) != 0;
     const float mass = liquid ? Q.mass_water : Q.mass_ice;
-    const int e = base_error(P, s.bx, s.by);
+    const int e = split_base_error(P, s.bw, s.bx, s.by);
     if (e) {
         *status = e;
         M.none(j);
@@ -331,7 +363,7 @@ __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const Split
     }
     M2<float> tau;
     if (liquid) {
-        const float sw = (float)(P.kappa * (1. - pow((double)s.Jp, -5.0)));   // Water (kernels.cuh:37-44)
+        const float sw = (float)(rare_params(P).kappa * (1. - pow((double)s.Jp, -5.0)));   // Water (kernels.cuh:37-44)
         tau = {sw, 0.f, 0.f, sw};
     } else {
         // KirchhoffStress_Wolper (kernels.cuh:24-34) from De
@@ -346,6 +378,15 @@ __device__ __forceinline__ void p2g_moments_f32(const StepParams &P, const Split
     M.m1[c] = make_float4(s.vy * mass, mass * s.B.a00 - Q.dtvd * tau.a00, mass * s.B.a01 - Q.dtvd * tau.a01,
                           mass * s.B.a10 - Q.dtvd * tau.a10);
     M.m2[c] = make_float2(mass * s.B.a11 - Q.dtvd * tau.a11, __uint_as_float(s.bw));
+}
+
+// (m, px, py) += (dm, dpx, dpy) on a float4 node with one vector reduction
+// (red: no value comes back, unlike atomicAdd on a float4, which returns the
+// old value and costs registers and latency); each component is added
+// atomically on its own, as with atomicAdd.
+__device__ __forceinline__ void red_add_f4(float4 *p, float dm, float dpx, float dpy)
+{
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(dm), "f"(dpx), "f"(dpy), "f"(0.f));
 }
 
 // FP32 grid of n nodes in one allocation of 6 n floats, in one of two layouts.
@@ -366,7 +407,7 @@ struct GridViewF {
     __device__ __forceinline__ void add(long k, float dm, float dpx, float dpy) const
     {
         if constexpr (AOS) {
-            atomicAdd(mp + k, make_float4(dm, dpx, dpy, 0.f));
+            red_add_f4(mp + k, dm, dpx, dpy);
         } else {
             atomicAdd(m + k, dm);
             atomicAdd(px + k, dpx);
@@ -414,17 +455,97 @@ struct SplitArgs {
                         // the staged margin during the next step
     double ind_x, ind_y;   // indenter position of the fused update
 };
-static_assert(sizeof(SplitArgs) <= 496, "128 batch members' arguments fit the 64 KB constant bank");
 
+// A batch member's FP32 grid as the batched tile kernel sees it: (m, px, py, -)
+// float4 accumulators and float2 velocities (GridViewF's batch layout).
+struct GridViewB {
+    float4 *mp;
+    float2 *v;
+    int ny, halo;
+    template <bool AOS>
+    __device__ __forceinline__ void add(long k, float dm, float dpx, float dpy) const
+    {
+        static_assert(AOS, "batch layout");
+        red_add_f4(mp + k, dm, dpx, dpy);
+    }
+    template <bool AOS>
+    __device__ __forceinline__ float2 vel(long k) const
+    {
+        static_assert(AOS, "batch layout");
+        return v[k];
+    }
+    __device__ __forceinline__ long idx(int gx, int gy) const { return (long)(gx + halo) * ny + gy; }
+};
+
+// The member arguments the batched tile kernel reads per work item, 208 of
+// SplitArgs' bytes: the FP64 parameters stay in the global table (p64), read
+// only by the rare paths.  300 members fit the 64 KB constant bank.
+struct SplitMember {
+    MemberP P;
+    SplitConsts Q;
+    TileGeom G;
+    GridViewB g;
+    unsigned *st;
+    long pitch;
+    const int *cell_start;
+    const GrainConstF *grain_tab;
+    int *status;
+    unsigned *flags;
+    int2 *tlist;
+    unsigned *tlist_n;
+    unsigned long long *moved;
+    int inst;
+};
+constexpr int BATCH_CONST_SLOTS = 300;
+static_assert(sizeof(SplitMember) * BATCH_CONST_SLOTS <= 64000, "the members' arguments fit the constant bank");
+
+// member i of a batch whose argument table is `d_args` on the device
+inline SplitMember split_member(const SplitArgs &a, const SplitArgs *d_args_i)
+{
+    SplitMember m{};
+    m.P = MemberP{a.P.halo, a.P.gridx, a.P.gridy, split_pack(-a.P.halo, 0),
+                  split_pack(a.P.gridx + a.P.halo - 3, a.P.gridy - 3), &d_args_i->P};
+    m.Q = a.Q;
+    m.G = a.G;
+    m.g = GridViewB{a.g.mp, a.g.v, a.g.ny, a.g.halo};
+    m.st = a.st;
+    m.pitch = a.pitch;
+    m.cell_start = a.cell_start;
+    m.grain_tab = a.grain_tab;
+    m.status = a.status;
+    m.flags = a.flags;
+    m.tlist = a.tlist;
+    m.tlist_n = a.tlist_n;
+    m.moved = a.moved;
+    m.inst = a.inst;
+    return m;
+}
+
+// Where the batched tile kernel finds its members' arguments: the global
+// table, or (batch_cargs.cu, batches of at most BATCH_CONST_SLOTS slots) a
+// compact copy in the constant bank, read as the single-instance kernel
+// reads its own (no global loads and fewer spills in the point loop).
+struct GlobalMembers {
+    const SplitArgs *a;
+    __device__ __forceinline__ const SplitArgs &operator[](int i) const { return a[i]; }
+};
 #ifdef ICY_BATCH_CONST_ARGS
-// Only in batch_cargs.cu: the member arguments of a batch of at most
-// BATCH_CONST_SLOTS slots, copied to the constant bank, where the batched
-// tile kernel reads them as the single-instance kernel reads its own (no
-// global loads and fewer spills in the point loop).  In its own translation
-// unit so that the kernels reading the global table compile as before.
-constexpr int BATCH_CONST_SLOTS = 128;
-static __constant__ SplitArgs c_batch_args[BATCH_CONST_SLOTS];
+static __constant__ SplitMember c_batch_mem[BATCH_CONST_SLOTS];
+struct ConstMembers {
+    __device__ __forceinline__ const SplitMember &operator[](int i) const { return c_batch_mem[i]; }
+};
+using BatchMembers = ConstMembers;
+#else
+using BatchMembers = GlobalMembers;
 #endif
+
+// The arguments of member `inst` (a batch), or the launch's own (alone).
+template <bool BATCH, class TAB>
+__device__ __forceinline__ decltype(auto) member_at(const SplitArgs &A1, const TAB &tab, int inst)
+{
+    if constexpr (BATCH) return tab[inst];
+    else return (A1);
+}
 
 // P2G contributions of one point to its 3 x 3 nodes (simulation/kernels.cuh:
 // 100-120): node (a, b) gets W m and W (m v + S d) with W = wx[a] wy[b] and
@@ -455,8 +576,8 @@ __device__ __forceinline__ void point_contributions_f32(float h, float gx, float
     }
 }
 
-template <bool AOS, class S>
-static __device__ __noinline__ void p2g_global_f32(GridViewF g, unsigned *flags, int2 *tlist, unsigned *tlist_n,
+template <bool AOS, class S, class GV>
+static __device__ __noinline__ void p2g_global_f32(GV g, unsigned *flags, int2 *tlist, unsigned *tlist_n,
                                                    int inst, int ntx, int halo, float h, int bx, int by, float gx,
                                                    float gy, float mass, float mvx, float mvy, float s00, float s01,
                                                    float s10, float s11)
@@ -514,14 +635,14 @@ __device__ __forceinline__ void cell_order_build(int (&hist)[CNT_BUCKETS], const
 }
 
 // phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32
-template <int NT, bool AOS, bool FUSE, class S, typename Sync>
-__device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int tid, int tx, int ty, int cs, int ce,
+template <int NT, bool AOS, bool FUSE, class S, class AT, typename Sync>
+__device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, int tx, int ty, int cs, int ce,
                                                         const int *s_cs, const int *s_perm, float *mom,
                                                         float (*s_odd)[S::RN], unsigned &touch, unsigned &moved,
                                                         bool fused, Sync &&sync)
 {
     ICY_TILE_SHAPE(S);
-    const StepParams &P = A.P;
+    const auto &P = A.P;
     const int X0 = tx * TX - P.halo, Y0 = ty * TY;
     const int RX0 = X0 - RM, RY0 = Y0 - RM;
     float acc[27];
@@ -552,15 +673,18 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const SplitArgs &A, int 
                 moved++;
                 int bx, by;
                 split_unpack(pb, bx, by);
-                if (FUSE && A.seq > 0) {
+                if constexpr (FUSE) {
                     // can this point leave the staged margin during the next step?  (its
                     // offset from its sorted cell, in cells, against the largest move of a
                     // step; near the low edges, where the base truncates, always)
-                    int sx, sy;
-                    split_unpack(pbc, sx, sy);
-                    const float ux = (float)(bx - sx) + gx, uy = (float)(by - sy) + gy;
-                    if (!(ux >= -A.safe_m && ux < A.safe_m && uy >= -A.safe_m && uy < A.safe_m) || bx <= 0 || by <= 0)
-                        A.unsafe[A.seq & 1] = A.seq;
+                    if (A.seq > 0) {
+                        int sx, sy;
+                        split_unpack(pbc, sx, sy);
+                        const float ux = (float)(bx - sx) + gx, uy = (float)(by - sy) + gy;
+                        if (!(ux >= -A.safe_m && ux < A.safe_m && uy >= -A.safe_m && uy < A.safe_m) || bx <= 0 ||
+                            by <= 0)
+                            A.unsafe[A.seq & 1] = A.seq;
+                    }
                 }
                 const int lx = bx - RX0, ly = by - RY0;
                 if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
@@ -715,14 +839,14 @@ struct BatchItem { int inst, tile; };
 // contiguous block range) or cell ranges (which == 8) into L2 while this CTA
 // is in its cell phase.
 constexpr int PF_PIECES = 8;
-template <bool BATCH, class S>
-__device__ __forceinline__ void prefetch_next_item(const SplitArgs &A1, const SplitArgs *Aarr, const BatchItem *work,
+template <bool BATCH, class S, class TAB>
+__device__ __forceinline__ void prefetch_next_item(const SplitArgs &A1, const TAB &tab, const BatchItem *work,
                                                    int next, int na, int which)
 {
     ICY_TILE_SHAPE(S);
     if (next >= na) return;
     const BatchItem w = BATCH ? work[next] : BatchItem{0, A1.active[next]};
-    const SplitArgs &A = BATCH ? Aarr[w.inst] : A1;
+    const auto &A = member_at<BATCH>(A1, tab, w.inst);
     const int *cs = A.cell_start + (long)w.tile * TT;
     if (which == PF_PIECES) {
         prefetch_l2(cs, (TT + 1) * sizeof(int));
@@ -783,12 +907,13 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
         const BatchItem w = BATCH ? work[ti] : BatchItem{0, A1.active[ti]};
         if (BATCH && tid == 0) s_claim = atomicAdd(A1.claim, 1);
 #ifdef ICY_BATCH_CONST_ARGS
-        const SplitArgs &A = BATCH ? c_batch_args[w.inst] : A1;
+        const BatchMembers tab{};
 #else
-        const SplitArgs &A = BATCH ? Aarr[w.inst] : A1;
+        const BatchMembers tab{Aarr};
 #endif
-        const StepParams &P = A.P;
-        const bool record = BATCH ? rec[w.inst] != 0 : A.record_pq != 0;
+        const auto &A = member_at<BATCH>(A1, tab, w.inst);
+        const auto &P = A.P;
+        const bool record = BATCH ? rec[w.inst] != 0 : A1.record_pq != 0;
         unsigned moved = 0;
         const int t = w.tile;
         const int tx = t % A.G.ntx, ty = t / A.G.ntx;
@@ -861,15 +986,15 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             // and its cell ranges
             constexpr int PF0 = TILE_THREADS_F32 - (PF_PIECES + 1);
             if (DO_P2G && cs == ps && tid >= PF0)
-                prefetch_next_item<BATCH, S>(A1, Aarr, work, next, na, tid - PF0);
+                prefetch_next_item<BATCH, S>(A1, tab, work, next, na, tid - PF0);
             // and the first threads its staged node velocities (columns of vx and vy,
             // or of the float2 velocities of a batch member)
             static_assert(2 * RX <= PF0, "velocity-column and state prefetches on different threads");
             if (DO_G2P && DO_P2G && cs == ps && tid < (BATCH ? 1 : 2) * RX && next < na) {
                 const BatchItem wn = BATCH ? work[next] : BatchItem{0, A1.active[next]};
-                const SplitArgs &An = BATCH ? Aarr[wn.inst] : A1;
+                const auto &An = member_at<BATCH>(A1, tab, wn.inst);
                 const int nx0 = (wn.tile % An.G.ntx) * TX - An.P.halo - RM, ny0 = (wn.tile / An.G.ntx) * TY - RM;
-                if (BATCH)
+                if constexpr (BATCH)
                     prefetch_region_column(An.g.v, An.P.gridx, An.P.gridy, An.P.halo, An.g.ny, nx0, ny0, tid, RY);
                 else
                     prefetch_region_column(tid < RX ? An.g.vx : An.g.vy, An.P.gridx, An.P.gridy, An.P.halo, An.g.ny,
@@ -885,44 +1010,49 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                                                                  touch, moved, fused, [] { __syncthreads(); });
             }
         }
-        if (FUSE && DO_P2G && fused) {
-            // Fused grid update: this tile's sums are in; count it finished for each
-            // of the 9 node tiles around it.  The CTA that brings a node tile's count
-            // to the number of active cell tiles around it (nexp, from the binning)
-            // updates that node tile: all its contributions have landed, since in a
-            // fused launch every contribution to a node tile comes from the cell tiles
-            // around it.  Release: the CTA's reductions, barrier, then a fence and the
-            // count by the counting threads (the barrier orders the other threads'
-            // reductions before the fence, which is cumulative); acquire: count,
-            // fence, barrier, reads through L2 -- the pattern of a grid-wide barrier.
-            __syncthreads();
-            if (tid < 9) {
-                const int nx = tx + tid % 3 - 1, ny = ty + tid / 3 - 1;
-                bool ready = false;
-                if (nx >= 0 && nx < A.G.ntx && ny >= 0 && ny < A.G.nty) {
-                    const int X = ny * A.G.ntx + nx;
-                    __threadfence();
-                    ready = atomicAdd(A.ncnt + X, 1) == A.nexp[X] - 1;
-                    if (ready) {
-                        A.ncnt[X] = 0;   // the last one: ready for the next launch
+        bool tail_done = false;
+        if constexpr (FUSE) {
+            if (DO_P2G && fused) {
+                tail_done = true;
+                // Fused grid update: this tile's sums are in; count it finished for each
+                // of the 9 node tiles around it.  The CTA that brings a node tile's count
+                // to the number of active cell tiles around it (nexp, from the binning)
+                // updates that node tile: all its contributions have landed, since in a
+                // fused launch every contribution to a node tile comes from the cell tiles
+                // around it.  Release: the CTA's reductions, barrier, then a fence and the
+                // count by the counting threads (the barrier orders the other threads'
+                // reductions before the fence, which is cumulative); acquire: count,
+                // fence, barrier, reads through L2 -- the pattern of a grid-wide barrier.
+                __syncthreads();
+                if (tid < 9) {
+                    const int nx = tx + tid % 3 - 1, ny = ty + tid / 3 - 1;
+                    bool ready = false;
+                    if (nx >= 0 && nx < A.G.ntx && ny >= 0 && ny < A.G.nty) {
+                        const int X = ny * A.G.ntx + nx;
                         __threadfence();
+                        ready = atomicAdd(A.ncnt + X, 1) == A.nexp[X] - 1;
+                        if (ready) {
+                            A.ncnt[X] = 0;   // the last one: ready for the next launch
+                            __threadfence();
+                        }
                     }
+                    const unsigned r = __ballot_sync(0x1ffu, ready);
+                    if (tid == 0) s_touch = r;
                 }
-                const unsigned r = __ballot_sync(0x1ffu, ready);
-                if (tid == 0) s_touch = r;
+                __syncthreads();
+                unsigned r = s_touch;
+                if (r) {
+                    do {
+                        const int q = __ffs(r) - 1;
+                        r &= r - 1;
+                        update_node_tile_f32<S>(A, tx + q % 3 - 1, ty + q / 3 - 1, tid, A.ind_x, A.ind_y);
+                    } while (r);
+                }
+                moved = __reduce_add_sync(0xffffffffu, moved);
+                if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
             }
-            __syncthreads();
-            unsigned r = s_touch;
-            if (r) {
-                do {
-                    const int q = __ffs(r) - 1;
-                    r &= r - 1;
-                    update_node_tile_f32<S>(A, tx + q % 3 - 1, ty + q / 3 - 1, tid, A.ind_x, A.ind_y);
-                } while (r);
-            }
-            moved = __reduce_add_sync(0xffffffffu, moved);
-            if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
-        } else if (DO_P2G) {
+        }
+        if (DO_P2G && !tail_done) {
             // each warp marks the node tiles it wrote (no barrier: the node phase's
             // last barrier already ended every use of the shared buffers)
             touch = __reduce_or_sync(0xffffffffu, touch);

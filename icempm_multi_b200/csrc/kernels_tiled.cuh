@@ -99,7 +99,8 @@ static __global__ void k_grain_table(StepParams P, GrainConst *tab)
     if (s < GRAIN_TAB) tab[s] = grain_constants(P, s / GRAIN_N11 - 29, s % GRAIN_N11 - 10);
 }
 
-__device__ __forceinline__ bool node_in_grid(const StepParams &P, int gx, int gy)
+template <class PT>
+__device__ __forceinline__ bool node_in_grid(const PT &P, int gx, int gy)
 {
     return gx >= -P.halo && gx < P.gridx + P.halo && gy >= 0 && gy < P.gridy;
 }

@@ -279,7 +279,9 @@ __device__ __forceinline__ bool node_update(const StepParams &P, int gix, int gi
 }
 
 // reference error codes for a stencil base outside the grid (kernels.cuh:94-97)
-__device__ __forceinline__ int base_error(const StepParams &P, int bx, int by)
+// (P: any parameter block with the int fields halo, gridx, gridy)
+template <class PT>
+__device__ __forceinline__ int base_error(const PT &P, int bx, int by)
 {
     int e = 0;
     if (bx < -P.halo) e = 70;

@@ -77,8 +77,8 @@ class Server:
     """Continuous batching of requests on one device under a memory budget.
 
     max_instances bounds the requests resident at once; a batch of at most
-    128 slots keeps its members' kernel arguments in the constant bank
-    (faster steps), so the default stays there."""
+    300 slots keeps its members' kernel arguments in the constant bank
+    (faster steps)."""
 
     def __init__(self, budget_bytes=150e9, max_instances=128, round_steps=50, device=0, keep_results=True,
                  keep_inputs=True):

@@ -156,3 +156,21 @@ def test_two_small_batches_at_once(oracle):
     b3.download(s3, o3)
     assert field_errors(o3, rb)["pos"] <= POS_TOL
     b3.close()
+
+
+def test_batch_beyond_the_constant_bank(oracle):
+    """A batch of more slots than the constant-bank table holds (300) reads
+    its members' arguments from the global table: members still match their
+    single-instance runs (the constant-bank path is the one of the tests
+    above)."""
+    sc = scenarios()[:3]
+    b = Batch(400)
+    slots = [b.add(p, soa) for p, soa in sc]
+    b.step(30)
+    b.step(30)
+    for (p, soa), s in zip(sc, slots):
+        out = soa.clone()
+        assert b.download(s, out)[1] == 60
+        one, _ = single_f32(p, soa, 60, 30)
+        assert field_errors(out, one)["pos"] <= 1e-6
+    b.close()
