@@ -90,6 +90,7 @@ class Server:
         self.keep_results = keep_results
         self.used = 0.0
         self.running = {}
+        self.retired = []        # [(slot, request, buffer)] taken out, results being copied: slots still held
         self.queue = collections.deque()
         self.completed = []
         self.cancelled = []
@@ -102,7 +103,8 @@ class Server:
         self.batch.close()
 
     def _admit(self, now):
-        while self.queue and len(self.running) < self.max_instances:
+        # a retired member's slot stays taken until its results are collected
+        while self.queue and len(self.running) + len(self.retired) < self.max_instances:
             r = self.queue[0]
             r.ensure()
             need = device_bytes(r.params, r.capacity)
@@ -208,9 +210,8 @@ class Server:
         pending = sorted(requests, key=lambda r: r.arrival)
         pi = 0
         work = 0.0
-        retired = []            # taken out after the previous round; results being copied
         t0 = time.perf_counter()
-        while pi < len(pending) or self.queue or self.running or retired:
+        while pi < len(pending) or self.queue or self.running or self.retired:
             now = time.perf_counter() - t0
             while pi < len(pending) and pending[pi].arrival <= now:
                 self.queue.append(pending[pi])
@@ -227,17 +228,17 @@ class Server:
             finished = self._retire_finished()
             # at most this round in flight; the previous round's results are copied by now
             self.batch.wait_steps(1)
-            self._collect(retired, t0)
+            self._collect(self.retired, t0)
             # the rounds before this one are done: uploads queued before them no longer
             # read their host buffers
             if not self.keep_inputs:
                 for r in self.running.values():
                     if r.soa is not None and 0 <= r.upload_round < self.rounds:
                         r.soa = None
-            retired = finished
+            self.retired = finished
             if stepped and on_round is not None:
                 on_round(self, self.rounds)
-            if not self.running and not retired and not self.queue and pi < len(pending):
+            if not self.running and not self.retired and not self.queue and pi < len(pending):
                 time.sleep(max(0.0, min(0.01, pending[pi].arrival - (time.perf_counter() - t0))))
         self.batch.wait_steps(0)
         makespan = time.perf_counter() - t0

@@ -130,6 +130,23 @@ def test_budget_bounds_residency_including_retiring_members(fake):
         assert len(live) <= 2
 
 
+def test_slots_bound_residency_including_retiring_members(fake):
+    """With slots, not memory, the limit: a retired member holds its slot
+    until its results are collected, so admission counts it (the batch has
+    no free slot for a new member before that)."""
+    reqs = _requests(9, [20, 40, 20, 60, 20, 40, 20, 20, 40])
+    srv = S.Server(budget_bytes=1e12, max_instances=3, round_steps=20)
+    stats = srv.run(reqs)
+    assert stats["requests"] == 9 and stats["peak_live"] <= 3
+    held = set()
+    for e in fake[0].log:
+        if e[0] == "add":
+            held.add(e[1])
+        elif e[0] == "collect":
+            held.discard(e[1])
+        assert len(held) <= 3
+
+
 def test_request_larger_than_the_budget_is_refused(fake):
     p, soa = standard(seed=3)
     srv = S.Server(budget_bytes=0.5 * device_bytes(p, soa.capacity), round_steps=20)
