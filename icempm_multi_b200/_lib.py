@@ -89,7 +89,7 @@ EXPORTED = [
     "icy_batch_create", "icy_batch_destroy", "icy_batch_add", "icy_batch_add_async", "icy_batch_retire",
     "icy_batch_collect", "icy_batch_wait_steps", "icy_batch_remove", "icy_batch_step",
     "icy_batch_download", "icy_batch_synchronize", "icy_batch_set_option", "icy_batch_info",
-    "icy_batch_device_bytes", "icy_mpm_device_bytes", "icy_scene_place", "icy_host_alloc", "icy_host_free",
+    "icy_batch_device_bytes", "icy_mpm_device_bytes", "icy_mpm_reserve", "icy_scene_place", "icy_host_alloc", "icy_host_free",
     "icy_batch_set_clock", "icy_mpm_counters",
     "icy_part_plan", "icy_part_create", "icy_part_upload", "icy_part_step", "icy_part_download",
     "icy_part_info", "icy_part_destroy",
@@ -170,6 +170,7 @@ def lib():
                                      C.POINTER(vp)]),
         "icy_batch_device_bytes": (C.c_int64, [vp, C.c_int]),
         "icy_mpm_device_bytes": (C.c_int64, [P, C.c_uint, C.c_int]),
+        "icy_mpm_reserve": (C.c_int, [C.c_int, C.c_int64]),
         "icy_version": (C.c_char_p, []),
         "icy_last_error": (C.c_char_p, []),
     }

@@ -14,6 +14,7 @@ from ._lib import PRECISION_FP32_SPLIT, check, lib
 
 class Batch:
     def __init__(self, max_instances, device=0):
+        self.device = device
         self._b = C.c_void_p()
         check(lib().icy_batch_create(device, int(max_instances), C.byref(self._b)), "icy_batch_create")
         self.params = {}
@@ -112,6 +113,11 @@ class Batch:
 
     def set_option(self, name, value):
         check(lib().icy_batch_set_option(self._b, name.encode(), float(value)), "icy_batch_set_option")
+
+    def reserve(self, nbytes):
+        """Grow the device's instance memory pool to at least nbytes (icy_mpm_reserve):
+        members admitted later take their buffers from memory already mapped."""
+        check(lib().icy_mpm_reserve(self.device, int(nbytes)), "icy_mpm_reserve")
 
     def info(self):
         live, pts, launches, stream = C.c_int(0), C.c_int64(0), C.c_int64(0), C.c_void_p()

@@ -23,7 +23,8 @@ namespace icy_dev {   // batch_cargs.cu
 int batch_const_slots();
 bool batch_const_acquire(int device, const void *batch);
 void batch_const_release(int device, const void *batch);
-cudaError_t batch_const_upload(const SplitArgs *args, const SplitArgs *d_args, int n, cudaStream_t s);
+cudaError_t batch_const_upload(const SplitArgs *args, const SplitArgs *d_args, int n, SplitMember *staging,
+                               cudaStream_t s);
 cudaError_t batch_const_setup();
 void batch_const_launch_tile(int kind, int shape, int grid, cudaStream_t s, const SplitArgs &none, const SplitArgs *args,
                              const BatchItem *work, const int *nwork, const int *rec);
@@ -74,7 +75,24 @@ struct icy_batch {
     int shape = SHAPE_32X8;         // members' tile shape (option "tile_shape", set while the batch is empty)
     bool cargs = false;              // owns the device's constant-bank argument table (batch_cargs.cu)
     int64_t launches = 0;
+    // page-locked staging of the argument tables a rebuild uploads, a ring of
+    // NARGS (a copy from pageable memory would wait for the queued rounds)
+    static constexpr int NARGS = 3;
+    SplitArgs *h_args[NARGS] = {};
+    SplitMember *h_mem[NARGS] = {};
+    cudaEvent_t ev_args[NARGS] = {};
+    bool args_used[NARGS] = {};
+    int args_next = 0;
 };
+
+// A member's device memory back to the pool in the order of the batch's second
+// stream, where its last work (upload or download) ran: no host wait.
+static void member_destroy(icy_batch *b, icy_mpm *h)
+{
+    h->stream = b->side;
+    icy_instance_free(h, false, false);
+    delete h;
+}
 
 static SplitArgs member_args(icy_batch *b, icy_mpm *h, int slot)
 {
@@ -122,7 +140,11 @@ static void drop_graphs(icy_batch *b)
 // node-tile lists to the members' total tile count).
 static int rebuild(icy_batch *b)
 {
-    std::vector<SplitArgs> args(b->nslots);
+    // the staging buffer of the rebuild NARGS ago: its copies are long done
+    const int k = b->args_next;
+    b->args_next = (k + 1) % icy_batch::NARGS;
+    if (b->args_used[k]) CKB(cudaEventSynchronize(b->ev_args[k]));
+    SplitArgs *args = b->h_args[k];
     long tiles = 0;
     for (int s = 0; s < b->nslots; s++)
         tiles += b->members[s] ? b->members[s]->ntiles : 0;
@@ -138,16 +160,15 @@ static int rebuild(icy_batch *b)
         if (e != cudaSuccess) { icy_set_error("cudaMalloc(batch work list)", e); return ICY_ERR_OUT_OF_MEMORY; }
         b->work_cap = cap;
     }
-    for (int s = 0; s < b->nslots; s++)
-        if (b->members[s]) args[s] = member_args(b, b->members[s], s);
-    CKB(cudaMemcpyAsync(b->d_args, args.data(), sizeof(SplitArgs) * b->nslots, cudaMemcpyHostToDevice, b->stream));
-    if (b->cargs) CKB(batch_const_upload(args.data(), b->d_args, b->nslots, b->stream));
+    for (int s = 0; s < b->nslots; s++) args[s] = b->members[s] ? member_args(b, b->members[s], s) : SplitArgs{};
+    CKB(cudaMemcpyAsync(b->d_args, args, sizeof(SplitArgs) * b->nslots, cudaMemcpyHostToDevice, b->stream));
+    if (b->cargs) CKB(batch_const_upload(args, b->d_args, b->nslots, b->h_mem[k], b->stream));
+    CKB(cudaEventRecord(b->ev_args[k], b->stream));
+    b->args_used[k] = true;
     k_batch_work_offsets<<<1, 1024, 0, b->stream>>>(b->d_args, b->d_clk, b->nslots, b->d_woff, b->d_nwork);
     k_batch_work_fill<<<dim3(8, b->nslots), 256, 0, b->stream>>>(b->d_args, b->d_clk, b->d_woff, b->d_work);
     CKB(cudaGetLastError());
     b->launches += 2;
-    // no synchronisation: a copy from pageable memory is staged before
-    // cudaMemcpyAsync returns, so `args` may go out of scope
     b->dirty = false;
     return ICY_OK;
 }
@@ -220,6 +241,12 @@ static int64_t icy_instance_device_bytes(icy_mpm *h)
 
 extern "C" {
 
+int icy_mpm_reserve(int device, int64_t bytes)
+{
+    if (bytes < 0) return ICY_ERR_INVALID_ARGUMENT;
+    return icy_instance_pool_reserve(device, (size_t)bytes);
+}
+
 // Device memory an instance of this size takes (as allocated by
 // icy_instance_allocate), for admission by memory budget.
 int64_t icy_mpm_device_bytes(const icy_sim_params *p, unsigned capacity, int precision)
@@ -266,6 +293,15 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     if ((e = cudaMallocHost(&b->h_clk, sizeof(BatchClock) * max_instances)) != cudaSuccess)
         return fail(e, "cudaMallocHost(batch clocks)");
+    for (int k = 0; k < icy_batch::NARGS; k++) {
+        if ((e = cudaMallocHost(&b->h_args[k], sizeof(SplitArgs) * max_instances)) != cudaSuccess)
+            return fail(e, "cudaMallocHost(batch arguments)");
+        if (max_instances <= batch_const_slots() &&
+            (e = cudaMallocHost(&b->h_mem[k], sizeof(SplitMember) * max_instances)) != cudaSuccess)
+            return fail(e, "cudaMallocHost(batch arguments)");
+        if ((e = cudaEventCreateWithFlags(&b->ev_args[k], cudaEventDisableTiming)) != cudaSuccess)
+            return fail(e, "event");
+    }
     if ((e = cudaMalloc(&b->d_args, sizeof(SplitArgs) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_clk, sizeof(BatchClock) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_rec, sizeof(int) * max_instances)) != cudaSuccess ||
@@ -308,15 +344,9 @@ int icy_batch_destroy(icy_batch *b)
     if (b->side) cudaStreamSynchronize(b->side);
     drop_graphs(b);
     for (icy_mpm *h : b->members)
-        if (h) {
-            h->stream = h->own_stream;
-            icy_mpm_destroy(h);
-        }
+        if (h) member_destroy(b, h);
     for (Retiring &r : b->retiring) {
-        if (r.h) {
-            r.h->stream = r.h->own_stream;
-            icy_mpm_destroy(r.h);
-        }
+        if (r.h) member_destroy(b, r.h);
         if (r.done) cudaEventDestroy(r.done);
         if (r.h_bins) cudaFreeHost(r.h_bins);
     }
@@ -331,6 +361,11 @@ int icy_batch_destroy(icy_batch *b)
     cudaFree(b->d_claim);
     if (b->cargs) batch_const_release(b->device, b);
     if (b->h_clk) cudaFreeHost(b->h_clk);
+    for (int k = 0; k < icy_batch::NARGS; k++) {
+        if (b->h_args[k]) cudaFreeHost(b->h_args[k]);
+        if (b->h_mem[k]) cudaFreeHost(b->h_mem[k]);
+        if (b->ev_args[k]) cudaEventDestroy(b->ev_args[k]);
+    }
     for (cudaEvent_t ev : b->ev_steps)
         if (ev) cudaEventDestroy(ev);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
@@ -353,8 +388,10 @@ static int add_member(icy_batch *b, const icy_sim_params *p, const double *hssoa
         if (!b->members[k] && !b->retiring[k].h) { s = k; break; }
     if (s < 0) return ICY_ERR_NO_SPACE;
     CKB(cudaSetDevice(b->device));
+    // the member's memory is allocated and cleared on the batch's second stream,
+    // behind nothing but earlier admissions and retirements, without waiting
     icy_mpm *h = nullptr;
-    int rc = icy_mpm_create(p, b->device, std::max(size, 1u), ICY_PRECISION_FP32_SPLIT, &h);
+    int rc = icy_mpm_create_on(p, b->device, std::max(size, 1u), ICY_PRECISION_FP32_SPLIT, b->side, &h);
     if (rc) return rc;
     if (b->shape != SHAPE_32X8 && (rc = icy_instance_set_shape(h, b->shape))) {
         icy_mpm_destroy(h);
@@ -363,9 +400,7 @@ static int add_member(icy_batch *b, const icy_sim_params *p, const double *hssoa
     h->stream = b->side;
     if ((rc = icy_mpm_update_constants(h, p)) || (rc = icy_mpm_transfer_points_to_device(h, hssoa, capacity, size)) ||
         (rc = icy_mpm_reset_indenter_force_accumulator(h)) || (rc = icy_instance_bin(h))) {
-        cudaStreamSynchronize(b->side);
-        h->stream = h->own_stream;
-        icy_mpm_destroy(h);
+        member_destroy(b, h);
         return rc;
     }
     BatchClock c{};
@@ -498,8 +533,7 @@ int icy_batch_collect(icy_batch *b, int slot, int wait, int *done, unsigned *siz
             if (!(u & ICY_STATUS_DISABLED)) active++;
         }
     const bool count_ok = !r.hssoa || active == h->prm.nPtsTotal;
-    h->stream = h->own_stream;
-    icy_mpm_destroy(h);
+    member_destroy(b, h);
     r.h = nullptr;
     r.hssoa = nullptr;
     r.bins = nullptr;
@@ -519,9 +553,7 @@ int icy_batch_remove(icy_batch *b, int slot)
     CKB(cudaStreamSynchronize(b->side));
     BatchClock c{};
     CKB(cudaMemcpy(b->d_clk + slot, &c, sizeof(c), cudaMemcpyHostToDevice));
-    icy_mpm *h = b->members[slot];
-    h->stream = h->own_stream;
-    icy_mpm_destroy(h);
+    member_destroy(b, b->members[slot]);
     b->members[slot] = nullptr;
     b->dirty = true;
     return ICY_OK;

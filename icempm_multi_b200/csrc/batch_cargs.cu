@@ -42,13 +42,15 @@ void batch_const_release(int device, const void *batch)
 }
 
 // args[0 .. n) (whose device copy is d_args) into the constant bank of this
-// module as compact member arguments, on stream s (n <= BATCH_CONST_SLOTS)
-cudaError_t batch_const_upload(const SplitArgs *args, const SplitArgs *d_args, int n, cudaStream_t s)
+// module as compact member arguments, through `staging` (page-locked, n
+// entries, not reused before the copy is done), on stream s
+// (n <= BATCH_CONST_SLOTS)
+cudaError_t batch_const_upload(const SplitArgs *args, const SplitArgs *d_args, int n, SplitMember *staging,
+                               cudaStream_t s)
 {
-    if (n > BATCH_CONST_SLOTS) return cudaErrorInvalidValue;
-    std::vector<SplitMember> m(n);
-    for (int i = 0; i < n; i++) m[i] = split_member(args[i], d_args + i);
-    return cudaMemcpyToSymbolAsync(c_batch_mem, m.data(), sizeof(SplitMember) * n, 0, cudaMemcpyHostToDevice, s);
+    if (n > BATCH_CONST_SLOTS || !staging) return cudaErrorInvalidValue;
+    for (int i = 0; i < n; i++) staging[i] = split_member(args[i], d_args + i);
+    return cudaMemcpyToSymbolAsync(c_batch_mem, staging, sizeof(SplitMember) * n, 0, cudaMemcpyHostToDevice, s);
 }
 
 cudaError_t batch_const_setup()

@@ -78,6 +78,13 @@ const char *icy_last_error(void) { return g_last_error.c_str(); }
 
 int icy_mpm_create(const icy_sim_params *p, int device, unsigned capacity, int precision, icy_mpm **out)
 {
+    return icy_mpm_create_on(p, device, capacity, precision, nullptr, out);
+}
+}  // extern "C"
+
+int icy_mpm_create_on(const icy_sim_params *p, int device, unsigned capacity, int precision, cudaStream_t stream,
+                      icy_mpm **out)
+{
     if (!p || !out || capacity == 0) return ICY_ERR_INVALID_ARGUMENT;
     if (precision != ICY_PRECISION_FP64 && precision != ICY_PRECISION_FP32_SPLIT) return ICY_ERR_INVALID_ARGUMENT;
     if (p->GridXTotal < 4 || p->GridY < 4 || p->GridHaloSize < 0 || p->n_indenter_subdivisions < 1)
@@ -87,7 +94,7 @@ int icy_mpm_create(const icy_sim_params *p, int device, unsigned capacity, int p
     h->device = device;
     h->prm = *p;
     h->precision = precision;
-    int rc = icy_instance_allocate(h, capacity);
+    int rc = icy_instance_allocate(h, capacity, stream);
     if (rc != ICY_OK) {
         icy_instance_free(h, rc == ICY_ERR_OUT_OF_MEMORY);
         delete h;
@@ -96,6 +103,8 @@ int icy_mpm_create(const icy_sim_params *p, int device, unsigned capacity, int p
     *out = h;
     return ICY_OK;
 }
+
+extern "C" {
 
 int icy_mpm_destroy(icy_mpm *h)
 {

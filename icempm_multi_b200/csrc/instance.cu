@@ -63,6 +63,28 @@ static cudaMemPool_t instance_pool(int device)
     return pool;
 }
 
+int icy_instance_pool_reserve(int device, size_t bytes)
+{
+    CK(cudaSetDevice(device));
+    cudaMemPool_t pool = instance_pool(device);
+    if (!pool) return ICY_ERR_OUT_OF_MEMORY;
+    size_t have = 0;
+    CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &have));
+    if (have >= bytes) return ICY_OK;
+    cudaStream_t s;
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    void *p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes - have, pool, s);
+    if (e == cudaSuccess) e = cudaFreeAsync(p, s);   // kept by the pool (release threshold: never)
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        icy_set_error("icy_mpm_reserve", e != cudaSuccess ? e : e2);
+        return e == cudaErrorMemoryAllocation ? ICY_ERR_OUT_OF_MEMORY : ICY_ERR_CUDA;
+    }
+    return ICY_OK;
+}
+
 template <typename T>
 static cudaError_t dalloc(icy_mpm *h, T **p, size_t count)
 {
@@ -198,12 +220,16 @@ int icy_instance_set_shape(icy_mpm *h, int shape)
     return ICY_OK;
 }
 
-int icy_instance_allocate(icy_mpm *h, unsigned capacity)
+int icy_instance_allocate(icy_mpm *h, unsigned capacity, cudaStream_t work_stream)
 {
     const bool split = h->precision == ICY_PRECISION_FP32_SPLIT;
     CK(cudaSetDevice(h->device));
-    CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
-    h->stream = h->own_stream;
+    if (work_stream) {
+        h->stream = work_stream;   // no stream of its own (creating one cost 2 ms)
+    } else {
+        CK(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+        h->stream = h->own_stream;
+    }
     h->capacity = capacity;
     h->pitch = ((long)capacity + 31) / 32 * 32;
     const int nx = h->prm.GridXTotal + 2 * h->prm.GridHaloSize;
@@ -270,15 +296,17 @@ int icy_instance_allocate(icy_mpm *h, unsigned capacity)
     CK(cudaFuncSetAttribute(k_tile_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PIPE_SMEM));
     h->pipe_grid = sms;
     if (int rc = icy_instance_constants(h)) return rc;
-    CK(cudaStreamSynchronize(h->stream));
+    // a caller's stream is not waited for: waiting here, behind the kernels
+    // already queued on a busy device, cost a served batch 12 ms per admission
+    if (!work_stream) CK(cudaStreamSynchronize(h->stream));
     return ICY_OK;
 }
 
-void icy_instance_free(icy_mpm *h, bool trim)
+void icy_instance_free(icy_mpm *h, bool trim, bool wait)
 {
     icy_prof_free(h);
-    if (h->own_stream) cudaStreamSynchronize(h->own_stream);
-    if (h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
+    if (wait && h->own_stream) cudaStreamSynchronize(h->own_stream);
+    if (wait && h->stream && h->stream != h->own_stream) cudaStreamSynchronize(h->stream);
     void *ptrs[] = {h->d_pts, h->d_pts_alt, h->d_grid, h->d_oidx, h->d_oidx_alt, h->d_keys, h->d_ranks,
                     h->d_counts, h->d_start, h->d_active, h->d_nactive, h->d_flags, h->d_moved, h->d_acc,
                     h->d_status, h->d_block_sums, h->d_grain, h->d_st, h->d_st_alt, h->d_stage, h->d_gridf,

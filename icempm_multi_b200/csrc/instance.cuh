@@ -98,8 +98,21 @@ icy_dev::StepParams icy_step_params(const icy_sim_params &p);
 void icy_set_error(const char *where, cudaError_t e);
 void icy_set_error_msg(const std::string &m);
 
-int icy_instance_allocate(icy_mpm *h, unsigned capacity);
-void icy_instance_free(icy_mpm *h, bool trim = false);   // trim: give unused pool memory back
+// Allocates and clears an instance's device memory.  With work_stream, the
+// allocations and clearing are queued there and the call returns without
+// waiting for them (work_stream becomes the instance's stream); otherwise on
+// the instance's own stream, waited for.
+int icy_instance_allocate(icy_mpm *h, unsigned capacity, cudaStream_t work_stream = nullptr);
+// icy_mpm_create with the allocation work queued on `stream` (not waited for;
+// nullptr: the instance's own stream, waited for)
+int icy_mpm_create_on(const icy_sim_params *p, int device, unsigned capacity, int precision, cudaStream_t stream,
+                      icy_mpm **out);
+// trim: give unused pool memory back; wait = false: the memory is freed in
+// the order of h->stream only (the caller knows that nothing on another stream
+// still uses it)
+void icy_instance_free(icy_mpm *h, bool trim = false, bool wait = true);
+// Grows the device's instance memory pool to hold at least `bytes` (kept).
+int icy_instance_pool_reserve(int device, size_t bytes);
 int icy_instance_upload(icy_mpm *h, const double *hssoa, unsigned cap, unsigned size);
 int icy_instance_download(icy_mpm *h, double *hssoa, unsigned cap);
 int icy_phase_reset_grid(icy_mpm *h);

@@ -81,8 +81,14 @@ class Server:
     (faster steps)."""
 
     def __init__(self, budget_bytes=150e9, max_instances=128, round_steps=50, device=0, keep_results=True,
-                 keep_inputs=True):
+                 keep_inputs=True, reserve_bytes=None):
         self.batch = Batch(max_instances, device=device)
+        # device memory for the admitted requests, mapped up front (up to 24 GB by
+        # default): an admission then takes its buffers from memory the pool holds
+        if reserve_bytes is None:
+            reserve_bytes = min(float(budget_bytes), 24e9)
+        if reserve_bytes > 0:
+            self.batch.reserve(reserve_bytes)
         self.keep_inputs = keep_inputs   # False: release each request's initial state once uploaded
         self.budget = float(budget_bytes)
         self.round_steps = int(round_steps)
@@ -98,6 +104,9 @@ class Server:
         self.peak_live = 0
         self.peak_bytes = 0.0
         self._scratch = {}      # free page-locked download buffers by capacity, when results are not kept
+        # uploaded inputs released while rounds are in flight: freeing page-locked
+        # memory synchronises the device, so they are freed when it is idle
+        self._released = []
 
     def close(self):
         self.batch.close()
@@ -234,14 +243,18 @@ class Server:
             if not self.keep_inputs:
                 for r in self.running.values():
                     if r.soa is not None and 0 <= r.upload_round < self.rounds:
+                        self._released.append(r.soa)
                         r.soa = None
             self.retired = finished
             if stepped and on_round is not None:
                 on_round(self, self.rounds)
-            if not self.running and not self.retired and not self.queue and pi < len(pending):
-                time.sleep(max(0.0, min(0.01, pending[pi].arrival - (time.perf_counter() - t0))))
+            if not self.running and not self.retired and not self.queue:
+                self._released.clear()   # nothing in flight: freeing costs no stall
+                if pi < len(pending):
+                    time.sleep(max(0.0, min(0.01, pending[pi].arrival - (time.perf_counter() - t0))))
         self.batch.wait_steps(0)
         makespan = time.perf_counter() - t0
+        self._released.clear()
         lat = np.array([r.done - r.arrival for r in self.completed]) if self.completed else np.zeros(1)
         return {
             "requests": len(self.completed),

@@ -376,6 +376,11 @@ int icy_batch_info(icy_batch *b, int *live, int64_t *points, int64_t *kernel_lau
 int64_t icy_batch_device_bytes(icy_batch *b, int slot);
 /* Device bytes an instance of this size and precision allocates. */
 int64_t icy_mpm_device_bytes(const icy_sim_params *p, unsigned capacity, int precision);
+/* Grows the memory pool that instances and batch members of `device` allocate
+   from to at least `bytes`, kept for them (no counterpart in the reference).
+   A server that reserves its budget up front admits requests without mapping
+   new device memory while rounds run (about 9 ms per admission otherwise). */
+int icy_mpm_reserve(int device, int64_t bytes);
 
 /* ------------------------------------------------------------------ */
 /* one instance in slabs of grid columns (partitions)                   */

@@ -70,6 +70,9 @@ class FakeBatch:
     def wait_steps(self, in_flight):
         pass
 
+    def reserve(self, nbytes):
+        pass
+
     def close(self):
         pass
 
