@@ -568,9 +568,9 @@ def main():
             try:
                 out["batched"] = measure_batch()
                 out["served"] = measure_serve()
-                # the same kind of trace at four times the arrival rate: more than the GPU
+                # the same kind of trace at six times the arrival rate: more than the GPU
                 # can take, so throughput shows the serving capacity and latency the queueing
-                out["served_overload"] = measure_serve(rate=40.0, duration=4.0)
+                out["served_overload"] = measure_serve(rate=60.0, duration=4.0)
                 # over capacity with a budget the admitted scenarios fill: admission is
                 # held back by device memory, not by slots (at these request sizes the
                 # 150 GB budget would need about 1,300 resident requests to bind)

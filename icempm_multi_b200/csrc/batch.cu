@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstring>
 #include <map>
 #include <vector>
@@ -83,6 +84,12 @@ struct icy_batch {
     cudaEvent_t ev_args[NARGS] = {};
     bool args_used[NARGS] = {};
     int args_next = 0;
+    // the members' re-binning tables (batched binning), staged the same way
+    BinMember *d_bin = nullptr;
+    BinMember *h_bin[NARGS] = {};
+    cudaEvent_t ev_bin[NARGS] = {};
+    bool bin_used[NARGS] = {};
+    int bin_next = 0;
 };
 
 // A member's device memory back to the pool in the order of the batch's second
@@ -173,14 +180,65 @@ static int rebuild(icy_batch *b)
     return ICY_OK;
 }
 
+// Every member with points binned again (icy_instance_bin's work), all
+// members in four launches on the batch stream.
 static int rebin_members(icy_batch *b)
 {
-    for (icy_mpm *h : b->members)
-        if (h && h->n) {
-            const int64_t l0 = h->launches;
-            if (int rc = icy_instance_bin(h)) return rc;
-            b->launches += h->launches - l0;
+    const int k = b->bin_next;
+    b->bin_next = (k + 1) % icy_batch::NARGS;
+    if (b->bin_used[k]) CKB(cudaEventSynchronize(b->ev_bin[k]));
+    BinMember *tab = b->h_bin[k];
+    int nm = 0;
+    long blocks = 0;
+    for (icy_mpm *h : b->members) {
+        if (!h || !h->n) continue;
+        BinMember &m = tab[nm++];
+        m.st = h->d_st;
+        m.st_alt = h->d_st_alt;
+        m.pitch = h->pitch;
+        m.n = (int)h->n;
+        m.blk0 = (int)blocks;
+        m.halo = h->prm.GridHaloSize;
+        m.gridx = h->prm.GridXTotal;
+        m.gridy = h->prm.GridY;
+        m.G = TileGeom{h->ntx, h->nty, h->ntiles};
+        m.keys = h->d_keys;
+        m.ranks = h->d_ranks;
+        m.counts = h->d_counts;
+        m.start = h->d_start;
+        m.active = h->d_active;
+        m.nactive = h->d_nactive;
+        m.nexp = h->d_nexp;
+        m.ncnt = h->d_ncnt;
+        m.unsafe = h->d_unsafe;
+        m.status = h->d_status;
+        m.oidx = h->d_oidx;
+        m.oidx_alt = h->d_oidx_alt;
+        blocks += (h->n + 255) / 256;
+    }
+    if (blocks > INT_MAX) return ICY_ERR_INVALID_ARGUMENT;
+    if (nm > 0) {
+        CKB(cudaMemcpyAsync(b->d_bin, tab, sizeof(BinMember) * nm, cudaMemcpyHostToDevice, b->stream));
+        CKB(cudaEventRecord(b->ev_bin[k], b->stream));
+        b->bin_used[k] = true;
+        with_shape(b->shape, [&](auto sh) {
+            using S = decltype(sh);
+            k_bin_clear_batch<S><<<dim3(64, nm), 256, 0, b->stream>>>(b->d_bin);
+            k_bin_count_batch<S><<<(int)blocks, 256, 0, b->stream>>>(b->d_bin, nm);
+            k_bin_scan_batch<S><<<nm, 1024, 0, b->stream>>>(b->d_bin);
+            k_bin_scatter_batch<<<(int)blocks, 256, 0, b->stream>>>(b->d_bin, nm);
+        });
+        CKB(cudaGetLastError());
+        b->launches += 4;
+        for (icy_mpm *h : b->members) {
+            if (!h || !h->n) continue;
+            std::swap(h->d_st, h->d_st_alt);
+            std::swap(h->d_oidx, h->d_oidx_alt);
+            h->binned = h->permuted = true;
+            h->steps_since_bin = 0;
+            h->fuse_seq = 0;
         }
+    }
     b->steps_since_bin = 0;
     b->dirty = true;
     return ICY_OK;
@@ -299,9 +357,14 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
         if (max_instances <= batch_const_slots() &&
             (e = cudaMallocHost(&b->h_mem[k], sizeof(SplitMember) * max_instances)) != cudaSuccess)
             return fail(e, "cudaMallocHost(batch arguments)");
-        if ((e = cudaEventCreateWithFlags(&b->ev_args[k], cudaEventDisableTiming)) != cudaSuccess)
+        if ((e = cudaEventCreateWithFlags(&b->ev_args[k], cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&b->ev_bin[k], cudaEventDisableTiming)) != cudaSuccess)
             return fail(e, "event");
+        if ((e = cudaMallocHost(&b->h_bin[k], sizeof(BinMember) * max_instances)) != cudaSuccess)
+            return fail(e, "cudaMallocHost(batch binning)");
     }
+    if ((e = cudaMalloc(&b->d_bin, sizeof(BinMember) * max_instances)) != cudaSuccess)
+        return fail(e, "cudaMalloc(batch binning)");
     if ((e = cudaMalloc(&b->d_args, sizeof(SplitArgs) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_clk, sizeof(BatchClock) * max_instances)) != cudaSuccess ||
         (e = cudaMalloc(&b->d_rec, sizeof(int) * max_instances)) != cudaSuccess ||
@@ -365,7 +428,10 @@ int icy_batch_destroy(icy_batch *b)
         if (b->h_args[k]) cudaFreeHost(b->h_args[k]);
         if (b->h_mem[k]) cudaFreeHost(b->h_mem[k]);
         if (b->ev_args[k]) cudaEventDestroy(b->ev_args[k]);
+        if (b->h_bin[k]) cudaFreeHost(b->h_bin[k]);
+        if (b->ev_bin[k]) cudaEventDestroy(b->ev_bin[k]);
     }
+    cudaFree(b->d_bin);
     for (cudaEvent_t ev : b->ev_steps)
         if (ev) cudaEventDestroy(ev);
     if (b->ev_join) cudaEventDestroy(b->ev_join);

@@ -1091,12 +1091,15 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
                                                                 double ind_x, double ind_y);
 
 // ---------------------------------------------------------------- binning / conversion
-template <class S>
-static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__restrict__ st, int n, int *keys,
-                                       int *ranks, int *counts, int *status)
+// Binning key and rank of point i of the blocked state st (n points): its
+// tile cell (or the disabled / out-of-grid bucket), its place among the
+// points of that cell (warp-aggregated atomics on counts).  P: any block of
+// the ints halo, gridx, gridy.
+template <class S, class PT>
+__device__ __forceinline__ void bin_count_point(const PT &P, const TileGeom &G, const unsigned *__restrict__ st, int n,
+                                                int i, int *keys, int *ranks, int *counts, int *status)
 {
     ICY_TILE_SHAPE(S);
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool in = i < n;
     int key = G.ntiles * TT;
     if (in) {
@@ -1120,13 +1123,20 @@ static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned 
     ranks[i] = base + __popc(peers & ((1u << lane) - 1u));
 }
 
-static __global__ void k_bin_scatter_f32(const unsigned *__restrict__ src, unsigned *__restrict__ dst, long pitch, int n,
-                                         const int *__restrict__ keys, const int *__restrict__ ranks,
-                                         const int *__restrict__ start, const int *__restrict__ oidx_src,
-                                         int *__restrict__ oidx_dst)
+template <class S>
+static __global__ void k_bin_count_f32(StepParams P, TileGeom G, const unsigned *__restrict__ st, int n, int *keys,
+                                       int *ranks, int *counts, int *status)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    bin_count_point<S>(P, G, st, n, blockIdx.x * blockDim.x + threadIdx.x, keys, ranks, counts, status);
+}
+
+// point i of src to its binned place start[keys[i]] + ranks[i] in dst, with its
+// upload index
+__device__ __forceinline__ void bin_scatter_point(const unsigned *__restrict__ src, unsigned *__restrict__ dst,
+                                                  long pitch, int i, const int *__restrict__ keys,
+                                                  const int *__restrict__ ranks, const int *__restrict__ start,
+                                                  const int *__restrict__ oidx_src, int *__restrict__ oidx_dst)
+{
     const long d = start[keys[i]] + ranks[i];
     *reinterpret_cast<uint4 *>(hot_vec(dst, d)) = *reinterpret_cast<const uint4 *>(hot_vec(src, i));
     *reinterpret_cast<uint4 *>(hot_vec(dst, d) + 128) = *reinterpret_cast<const uint4 *>(hot_vec(src, i) + 128);
@@ -1135,6 +1145,15 @@ static __global__ void k_bin_scatter_f32(const unsigned *__restrict__ src, unsig
     *reinterpret_cast<uint4 *>(dst + cold_vec(pitch, d) + 128) =
         *reinterpret_cast<const uint4 *>(src + cold_vec(pitch, i) + 128);
     oidx_dst[d] = oidx_src[i];
+}
+
+static __global__ void k_bin_scatter_f32(const unsigned *__restrict__ src, unsigned *__restrict__ dst, long pitch, int n,
+                                         const int *__restrict__ keys, const int *__restrict__ ranks,
+                                         const int *__restrict__ start, const int *__restrict__ oidx_src,
+                                         int *__restrict__ oidx_dst)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) bin_scatter_point(src, dst, pitch, i, keys, ranks, start, oidx_src, oidx_dst);
 }
 
 // FP64 HSSOA chunk (16 lines, stride cpitch) -> FP32 state slots [first, first+count)
@@ -1223,6 +1242,121 @@ static __global__ void k_node_tile_expect(TileGeom G, const int *__restrict__ ce
             e += cell_start[(t + 1) * TT] > cell_start[t * TT];
         }
     nexp[X] = e;
+}
+
+// ---------------------------------------------------------------- batched re-binning
+// The binning of every member of a batch in four launches (clear, count, scan,
+// scatter) instead of about ten per member: with a hundred members the
+// per-member launches cost the serving loop 30 ms of host time per re-binning.
+// Member m's points are blocks [blk0, blk0 + ceil(n / 256)) of the count and
+// scatter grids.
+struct BinMember {
+    const unsigned *st;
+    unsigned *st_alt;
+    long pitch;
+    int n, blk0;
+    int halo, gridx, gridy;   // for base_error
+    TileGeom G;
+    int *keys, *ranks, *counts, *start, *active, *nactive, *nexp, *ncnt, *unsafe, *status;
+    const int *oidx;
+    int *oidx_alt;
+};
+
+// the member whose block range holds block b (members in ascending blk0)
+__device__ __forceinline__ int bin_member_of(const BinMember *mem, int nmem, int b)
+{
+    int lo = 0, hi = nmem;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (mem[mid].blk0 <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// counts of every member to zero (grid: 64 CTAs per member)
+template <class S>
+static __global__ void k_bin_clear_batch(const BinMember *__restrict__ mem)
+{
+    ICY_TILE_SHAPE(S);
+    const BinMember &M = mem[blockIdx.y];
+    const long nkeys = (long)M.G.ntiles * TT + 1;
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < nkeys; k += (long)gridDim.x * blockDim.x)
+        M.counts[k] = 0;
+}
+
+template <class S>
+static __global__ void k_bin_count_batch(const BinMember *__restrict__ mem, int nmem)
+{
+    const BinMember &M = mem[bin_member_of(mem, nmem, blockIdx.x)];
+    bin_count_point<S>(M, M.G, M.st, M.n, (blockIdx.x - M.blk0) * blockDim.x + threadIdx.x, M.keys, M.ranks,
+                       M.counts, M.status);
+}
+
+// one CTA of 1024 threads per member: cell starts (exclusive scan of the
+// counts, start[nkeys] = total), the list of tiles with points, the
+// contributors per node tile, and the fused update's counters reset
+template <class S>
+static __global__ void __launch_bounds__(1024) k_bin_scan_batch(const BinMember *__restrict__ mem)
+{
+    ICY_TILE_SHAPE(S);
+    constexpr int PER = 8, CHUNK = 1024 * PER;
+    __shared__ int s_warp[32];
+    const BinMember &M = mem[blockIdx.x];
+    const long nkeys = (long)M.G.ntiles * TT + 1;
+    int carry = 0;
+    for (long c0 = 0; c0 < nkeys; c0 += CHUNK) {
+        const long b = c0 + (long)threadIdx.x * PER;
+        int v[PER], sum = 0;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            v[k] = b + k < nkeys ? M.counts[b + k] : 0;
+            sum += v[k];
+        }
+        int total;
+        int run = block_exclusive_scan<1024>(sum, s_warp, total) + carry;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            if (b + k < nkeys) M.start[b + k] = run;
+            run += v[k];
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0) M.start[nkeys] = carry;
+    __syncthreads();   // the block's start[] writes are visible to the block
+    const int nt = M.G.ntiles;
+    const int per = (nt + 1023) / 1024;
+    const int t0 = min((int)threadIdx.x * per, nt), t1 = min(t0 + per, nt);
+    int s = 0;
+    for (int t = t0; t < t1; t++) s += M.start[(long)(t + 1) * TT] > M.start[(long)t * TT];
+    int total;
+    int run = block_exclusive_scan<1024>(s, s_warp, total);
+    for (int t = t0; t < t1; t++)
+        if (M.start[(long)(t + 1) * TT] > M.start[(long)t * TT]) M.active[run++] = t;
+    if (threadIdx.x == 0) {
+        *M.nactive = total;
+        M.unsafe[0] = M.unsafe[1] = -1;
+    }
+    for (int X = threadIdx.x; X < nt; X += blockDim.x) {
+        const int x = X % M.G.ntx, y = X / M.G.ntx;
+        int e = 0;
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                const int tx = x + dx, ty = y + dy;
+                if (tx < 0 || tx >= M.G.ntx || ty < 0 || ty >= M.G.nty) continue;
+                const long t = (long)ty * M.G.ntx + tx;
+                e += M.start[(t + 1) * TT] > M.start[t * TT];
+            }
+        M.nexp[X] = e;
+        M.ncnt[X] = 0;
+    }
+}
+
+static __global__ void k_bin_scatter_batch(const BinMember *__restrict__ mem, int nmem)
+{
+    const BinMember &M = mem[bin_member_of(mem, nmem, blockIdx.x)];
+    const int i = (blockIdx.x - M.blk0) * blockDim.x + threadIdx.x;
+    if (i < M.n) bin_scatter_point(M.st, M.st_alt, M.pitch, i, M.keys, M.ranks, M.start, M.oidx, M.oidx_alt);
 }
 
 }  // namespace icy_dev

@@ -174,3 +174,26 @@ def test_batch_beyond_the_constant_bank(oracle):
         one, _ = single_f32(p, soa, 60, 30)
         assert field_errors(out, one)["pos"] <= 1e-6
     b.close()
+
+
+@pytest.mark.parametrize("shape", [0, 1])
+def test_batch_rebinning_matches_single(oracle, shape):
+    """All members re-binned together on the device every 20 steps (one
+    launch per phase for the whole batch): each member still matches its
+    single-instance run and the oracle, after six re-binnings."""
+    sc = scenarios()
+    b = Batch(8)
+    b.set_option("tile_shape", shape)
+    b.set_option("resort_every", 20)
+    slots = [b.add(p, soa) for p, soa in sc]
+    for _ in range(6):
+        b.step(20)
+    for (p, soa), s in zip(sc, slots):
+        out = soa.clone()
+        assert b.download(s, out)[1] == 120
+        one, _ = single_f32(p, soa, 120, 40)
+        assert field_errors(out, one)["pos"] <= 1e-6
+        ref = soa.clone()
+        assert oracle.run(p, ref, 0, 120)[0] == 0
+        assert field_errors(out, ref)["pos"] <= POS_TOL
+    b.close()
