@@ -181,7 +181,7 @@ static int rebuild(icy_batch *b)
 }
 
 // Every member with points binned again (icy_instance_bin's work), all
-// members in four launches on the batch stream.
+// members in seven launches on the batch stream.
 static int rebin_members(icy_batch *b)
 {
     const int k = b->bin_next;
@@ -189,7 +189,7 @@ static int rebin_members(icy_batch *b)
     if (b->bin_used[k]) CKB(cudaEventSynchronize(b->ev_bin[k]));
     BinMember *tab = b->h_bin[k];
     int nm = 0;
-    long blocks = 0;
+    long blocks = 0, sblocks = 0;
     for (icy_mpm *h : b->members) {
         if (!h || !h->n) continue;
         BinMember &m = tab[nm++];
@@ -198,6 +198,7 @@ static int rebin_members(icy_batch *b)
         m.pitch = h->pitch;
         m.n = (int)h->n;
         m.blk0 = (int)blocks;
+        m.sblk0 = (int)sblocks;
         m.halo = h->prm.GridHaloSize;
         m.gridx = h->prm.GridXTotal;
         m.gridy = h->prm.GridY;
@@ -206,6 +207,7 @@ static int rebin_members(icy_batch *b)
         m.ranks = h->d_ranks;
         m.counts = h->d_counts;
         m.start = h->d_start;
+        m.block_sums = h->d_block_sums;
         m.active = h->d_active;
         m.nactive = h->d_nactive;
         m.nexp = h->d_nexp;
@@ -215,8 +217,9 @@ static int rebin_members(icy_batch *b)
         m.oidx = h->d_oidx;
         m.oidx_alt = h->d_oidx_alt;
         blocks += (h->n + 255) / 256;
+        sblocks += h->scan_blocks;
     }
-    if (blocks > INT_MAX) return ICY_ERR_INVALID_ARGUMENT;
+    if (blocks > INT_MAX || sblocks > INT_MAX) return ICY_ERR_INVALID_ARGUMENT;
     if (nm > 0) {
         CKB(cudaMemcpyAsync(b->d_bin, tab, sizeof(BinMember) * nm, cudaMemcpyHostToDevice, b->stream));
         CKB(cudaEventRecord(b->ev_bin[k], b->stream));
@@ -225,11 +228,14 @@ static int rebin_members(icy_batch *b)
             using S = decltype(sh);
             k_bin_clear_batch<S><<<dim3(64, nm), 256, 0, b->stream>>>(b->d_bin);
             k_bin_count_batch<S><<<(int)blocks, 256, 0, b->stream>>>(b->d_bin, nm);
-            k_bin_scan_batch<S><<<nm, 1024, 0, b->stream>>>(b->d_bin);
+            k_bin_scan_reduce_batch<S><<<(int)sblocks, SCAN_NT, 0, b->stream>>>(b->d_bin, nm);
+            k_bin_scan_blocks_batch<S><<<nm, 1024, 0, b->stream>>>(b->d_bin);
+            k_bin_scan_apply_batch<S><<<(int)sblocks, SCAN_NT, 0, b->stream>>>(b->d_bin, nm);
+            k_bin_tiles_batch<S><<<nm, 1024, 0, b->stream>>>(b->d_bin);
             k_bin_scatter_batch<<<(int)blocks, 256, 0, b->stream>>>(b->d_bin, nm);
         });
         CKB(cudaGetLastError());
-        b->launches += 4;
+        b->launches += 7;
         for (icy_mpm *h : b->members) {
             if (!h || !h->n) continue;
             std::swap(h->d_st, h->d_st_alt);

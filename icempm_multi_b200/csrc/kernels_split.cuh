@@ -938,28 +938,37 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
         __syncthreads();
         const int next = BATCH ? s_claim : ti + (int)gridDim.x;
         const int ps = s_cs[0], pe = s_cs[TT];
-        // the 3 x 3 node velocities of a stencil: from the staged region (one check
-        // per point), else from the grid
-        auto vsrc = [&](int bx, int by, float2 *nv) {
-            const int lx = bx - RX0, ly = by - RY0;
-            if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
-                const float2 *r = s_v + lx * RY + ly;
-#pragma unroll
-                for (int a = 0; a < 3; a++)
-#pragma unroll
-                    for (int b = 0; b < 3; b++) nv[a * 3 + b] = r[a * RY + b];
-            } else {
-#pragma unroll
-                for (int a = 0; a < 3; a++)
-#pragma unroll
-                    for (int b = 0; b < 3; b++) nv[a * 3 + b] = A.g.vel<BATCH>(A.g.idx(bx + a, by + b));
-            }
-        };
         unsigned touch = 0;
         for (int cs = ps; cs < pe; cs += CAPF) {
             const int ce = min(cs + CAPF, pe);
             for (int j = tid; j < ce - cs; j += blockDim.x) {
                 const long i = cs + j;
+                // a batch member's arguments read from the constant bank again in
+                // every iteration (the index is opaque to the compiler) instead of
+                // held in registers across the loop: fewer spills (batched step
+                // -2.5 %); alone they are constant-bank operands either way
+                int inst_o = w.inst;
+                if (BATCH) asm volatile("" : "+r"(inst_o));
+                const auto &A = member_at<BATCH>(A1, tab, inst_o);
+                const auto &P = A.P;
+                // the 3 x 3 node velocities of a stencil: from the staged region (one
+                // check per point), else from the grid
+                auto vsrc = [&](int bx, int by, float2 *nv) {
+                    const int lx = bx - RX0, ly = by - RY0;
+                    if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
+                        const float2 *r = s_v + lx * RY + ly;
+#pragma unroll
+                        for (int a = 0; a < 3; a++)
+#pragma unroll
+                            for (int b = 0; b < 3; b++) nv[a * 3 + b] = r[a * RY + b];
+                    } else {
+#pragma unroll
+                        for (int a = 0; a < 3; a++)
+#pragma unroll
+                            for (int b = 0; b < 3; b++)
+                                nv[a * 3 + b] = A.g.template vel<BATCH>(A.g.idx(bx + a, by + b));
+                    }
+                };
                 PointF s;
                 if (!load_point_f32(A.st, i, s)) {
                     if (DO_P2G) MomF(s_momf).none(j);
@@ -1245,30 +1254,32 @@ static __global__ void k_node_tile_expect(TileGeom G, const int *__restrict__ ce
 }
 
 // ---------------------------------------------------------------- batched re-binning
-// The binning of every member of a batch in four launches (clear, count, scan,
-// scatter) instead of about ten per member: with a hundred members the
-// per-member launches cost the serving loop 30 ms of host time per re-binning.
-// Member m's points are blocks [blk0, blk0 + ceil(n / 256)) of the count and
-// scatter grids.
+// The binning of every member of a batch in seven launches (clear, count, the
+// three phases of the scan, active tiles, scatter) instead of about ten per
+// member: with a hundred members the per-member launches cost the serving
+// loop 30 ms of host time per re-binning.  Member m's points are blocks
+// [blk0, blk0 + ceil(n / 256)) of the count and scatter grids, its keys scan
+// blocks [sblk0, sblk0 + ceil(nkeys / SCAN_BLOCK)) of the scan grids.
 struct BinMember {
     const unsigned *st;
     unsigned *st_alt;
     long pitch;
-    int n, blk0;
+    int n, blk0, sblk0;
     int halo, gridx, gridy;   // for base_error
     TileGeom G;
-    int *keys, *ranks, *counts, *start, *active, *nactive, *nexp, *ncnt, *unsafe, *status;
+    int *keys, *ranks, *counts, *start, *block_sums, *active, *nactive, *nexp, *ncnt, *unsafe, *status;
     const int *oidx;
     int *oidx_alt;
 };
 
-// the member whose block range holds block b (members in ascending blk0)
+// the member whose block range holds block b (members in ascending blk0, sblk0)
+template <bool SCAN>
 __device__ __forceinline__ int bin_member_of(const BinMember *mem, int nmem, int b)
 {
     int lo = 0, hi = nmem;
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
-        if (mem[mid].blk0 <= b) lo = mid;
+        if ((SCAN ? mem[mid].sblk0 : mem[mid].blk0) <= b) lo = mid;
         else hi = mid;
     }
     return lo;
@@ -1288,42 +1299,85 @@ static __global__ void k_bin_clear_batch(const BinMember *__restrict__ mem)
 template <class S>
 static __global__ void k_bin_count_batch(const BinMember *__restrict__ mem, int nmem)
 {
-    const BinMember &M = mem[bin_member_of(mem, nmem, blockIdx.x)];
+    const BinMember &M = mem[bin_member_of<false>(mem, nmem, blockIdx.x)];
     bin_count_point<S>(M, M.G, M.st, M.n, (blockIdx.x - M.blk0) * blockDim.x + threadIdx.x, M.keys, M.ranks,
                        M.counts, M.status);
 }
 
-// one CTA of 1024 threads per member: cell starts (exclusive scan of the
-// counts, start[nkeys] = total), the list of tiles with points, the
-// contributors per node tile, and the fused update's counters reset
+// the scan of each member's counts (k_scan_reduce / k_scan_blocks /
+// k_scan_apply over every member): start[i] = exclusive prefix, start[nkeys] = total
 template <class S>
-static __global__ void __launch_bounds__(1024) k_bin_scan_batch(const BinMember *__restrict__ mem)
+static __global__ void __launch_bounds__(SCAN_NT) k_bin_scan_reduce_batch(const BinMember *__restrict__ mem, int nmem)
 {
     ICY_TILE_SHAPE(S);
-    constexpr int PER = 8, CHUNK = 1024 * PER;
+    __shared__ int s_warp[SCAN_NT / 32];
+    const BinMember &M = mem[bin_member_of<true>(mem, nmem, blockIdx.x)];
+    const long nkeys = (long)M.G.ntiles * TT + 1;
+    const int blk = blockIdx.x - M.sblk0;
+    const long base = (long)blk * SCAN_BLOCK;
+    int s = 0;
+    for (int k = 0; k < SCAN_PER; k++) {
+        const long i = base + (long)k * SCAN_NT + threadIdx.x;
+        if (i < nkeys) s += M.counts[i];
+    }
+    int total;
+    block_exclusive_scan<SCAN_NT>(s, s_warp, total);
+    if (threadIdx.x == 0) M.block_sums[blk] = total;
+}
+
+template <class S>
+static __global__ void __launch_bounds__(1024) k_bin_scan_blocks_batch(const BinMember *__restrict__ mem)
+{
+    ICY_TILE_SHAPE(S);
     __shared__ int s_warp[32];
     const BinMember &M = mem[blockIdx.x];
-    const long nkeys = (long)M.G.ntiles * TT + 1;
-    int carry = 0;
-    for (long c0 = 0; c0 < nkeys; c0 += CHUNK) {
-        const long b = c0 + (long)threadIdx.x * PER;
-        int v[PER], sum = 0;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            v[k] = b + k < nkeys ? M.counts[b + k] : 0;
-            sum += v[k];
-        }
-        int total;
-        int run = block_exclusive_scan<1024>(sum, s_warp, total) + carry;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            if (b + k < nkeys) M.start[b + k] = run;
-            run += v[k];
-        }
-        carry += total;
+    const int nb = (int)(((long)M.G.ntiles * TT + 1 + SCAN_BLOCK - 1) / SCAN_BLOCK);
+    const int per = (nb + 1023) / 1024;
+    const int b = min((int)threadIdx.x * per, nb), e = min(b + per, nb);
+    int s = 0;
+    for (int k = b; k < e; k++) s += M.block_sums[k];
+    int total;
+    int run = block_exclusive_scan<1024>(s, s_warp, total);
+    for (int k = b; k < e; k++) {
+        const int c = M.block_sums[k];
+        M.block_sums[k] = run;
+        run += c;
     }
-    if (threadIdx.x == 0) M.start[nkeys] = carry;
-    __syncthreads();   // the block's start[] writes are visible to the block
+}
+
+template <class S>
+static __global__ void __launch_bounds__(SCAN_NT) k_bin_scan_apply_batch(const BinMember *__restrict__ mem, int nmem)
+{
+    ICY_TILE_SHAPE(S);
+    __shared__ int s_warp[SCAN_NT / 32];
+    const BinMember &M = mem[bin_member_of<true>(mem, nmem, blockIdx.x)];
+    const long n = (long)M.G.ntiles * TT + 1;
+    const int blk = blockIdx.x - M.sblk0;
+    const long base = (long)blk * SCAN_BLOCK + (long)threadIdx.x * SCAN_PER;
+    int v[SCAN_PER], s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; k++) {
+        v[k] = (base + k < n) ? M.counts[base + k] : 0;
+        s += v[k];
+    }
+    int total;
+    int run = block_exclusive_scan<SCAN_NT>(s, s_warp, total) + M.block_sums[blk];
+#pragma unroll
+    for (int k = 0; k < SCAN_PER; k++) {
+        if (base + k < n) M.start[base + k] = run;
+        run += v[k];
+    }
+    if (base + SCAN_PER >= n && base < n) M.start[n] = run;   // the thread holding the last item
+}
+
+// one CTA of 1024 threads per member: the list of tiles with points, the
+// contributors per node tile, and the fused update's counters reset
+template <class S>
+static __global__ void __launch_bounds__(1024) k_bin_tiles_batch(const BinMember *__restrict__ mem)
+{
+    ICY_TILE_SHAPE(S);
+    __shared__ int s_warp[32];
+    const BinMember &M = mem[blockIdx.x];
     const int nt = M.G.ntiles;
     const int per = (nt + 1023) / 1024;
     const int t0 = min((int)threadIdx.x * per, nt), t1 = min(t0 + per, nt);
@@ -1354,7 +1408,7 @@ static __global__ void __launch_bounds__(1024) k_bin_scan_batch(const BinMember 
 
 static __global__ void k_bin_scatter_batch(const BinMember *__restrict__ mem, int nmem)
 {
-    const BinMember &M = mem[bin_member_of(mem, nmem, blockIdx.x)];
+    const BinMember &M = mem[bin_member_of<false>(mem, nmem, blockIdx.x)];
     const int i = (blockIdx.x - M.blk0) * blockDim.x + threadIdx.x;
     if (i < M.n) bin_scatter_point(M.st, M.st_alt, M.pitch, i, M.keys, M.ranks, M.start, M.oidx, M.oidx_alt);
 }
