@@ -24,7 +24,7 @@ CLI = os.path.join(HERE, "icy_cli")
 HOST_SOURCES = ["h5lite.cpp", "icy_host.cpp", "capi_host.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["capi.cu", "instance.cu", "noalloc.cu", "batch.cu", "batch_cargs.cu", "partition.cu"]
+CUDA_SOURCES = ["capi.cu", "instance.cu", "noalloc.cu", "batch.cu", "batch_cargs.cu", "batch_uargs.cu", "partition.cu"]
 CXX_SOURCES = ["params.cpp", "scene.cpp"]
 
 

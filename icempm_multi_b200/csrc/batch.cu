@@ -27,6 +27,9 @@ void batch_const_release(int device, const void *batch);
 cudaError_t batch_const_upload(const SplitArgs *args, const SplitArgs *d_args, int n, SplitMember *staging,
                                cudaStream_t s);
 cudaError_t batch_const_setup();
+cudaError_t batch_upd_const_upload(const SplitArgs *args, int n, UpdMember *staging, cudaStream_t s);
+void batch_upd_const_launch(int shape, int grid, cudaStream_t s, const BatchClock *clk, const int2 *tlist,
+                            unsigned *tlist_n);
 void batch_const_launch_tile(int kind, int shape, int grid, cudaStream_t s, const SplitArgs &none, const SplitArgs *args,
                              const BatchItem *work, const int *nwork, const int *rec);
 }
@@ -81,6 +84,7 @@ struct icy_batch {
     static constexpr int NARGS = 3;
     SplitArgs *h_args[NARGS] = {};
     SplitMember *h_mem[NARGS] = {};
+    UpdMember *h_upd[NARGS] = {};
     cudaEvent_t ev_args[NARGS] = {};
     bool args_used[NARGS] = {};
     int args_next = 0;
@@ -169,7 +173,10 @@ static int rebuild(icy_batch *b)
     }
     for (int s = 0; s < b->nslots; s++) args[s] = b->members[s] ? member_args(b, b->members[s], s) : SplitArgs{};
     CKB(cudaMemcpyAsync(b->d_args, args, sizeof(SplitArgs) * b->nslots, cudaMemcpyHostToDevice, b->stream));
-    if (b->cargs) CKB(batch_const_upload(args, b->d_args, b->nslots, b->h_mem[k], b->stream));
+    if (b->cargs) {
+        CKB(batch_const_upload(args, b->d_args, b->nslots, b->h_mem[k], b->stream));
+        CKB(batch_upd_const_upload(args, b->nslots, b->h_upd[k], b->stream));
+    }
     CKB(cudaEventRecord(b->ev_args[k], b->stream));
     b->args_used[k] = true;
     k_batch_work_offsets<<<1, 1024, 0, b->stream>>>(b->d_args, b->d_clk, b->nslots, b->d_woff, b->d_nwork);
@@ -277,10 +284,13 @@ static int capture(icy_batch *b, int nsteps, cudaGraphExec_t *out, int *nlaunch)
     n++;
     for (int k = 0; k < nsteps; k++) {
         k_batch_advance<<<(b->nslots + 127) / 128, 128, 0, b->stream>>>(b->d_clk, b->d_rec, b->nslots);
-        with_shape(b->shape, [&](auto sh) {
-            k_update_list_f32<true, decltype(sh)><<<b->update_grid, 256, 0, b->stream>>>(
-                SplitArgs{}, b->d_args, b->d_clk, b->d_tlist, b->d_tlist_n, 0.0, 0.0);
-        });
+        if (b->cargs)
+            batch_upd_const_launch(b->shape, b->update_grid, b->stream, b->d_clk, b->d_tlist, b->d_tlist_n);
+        else
+            with_shape(b->shape, [&](auto sh) {
+                k_update_list_f32<decltype(sh), GlobalMembers><<<b->update_grid, 256, 0, b->stream>>>(
+                    GlobalMembers{b->d_args}, b->d_clk, b->d_tlist, b->d_tlist_n);
+            });
         if (k + 1 < nsteps)
             launch_tile_batch<true, true, false>(b, none, MOMF_BYTES, 1);
         else
@@ -361,7 +371,8 @@ int icy_batch_create(int device, int max_instances, icy_batch **out)
         if ((e = cudaMallocHost(&b->h_args[k], sizeof(SplitArgs) * max_instances)) != cudaSuccess)
             return fail(e, "cudaMallocHost(batch arguments)");
         if (max_instances <= batch_const_slots() &&
-            (e = cudaMallocHost(&b->h_mem[k], sizeof(SplitMember) * max_instances)) != cudaSuccess)
+            ((e = cudaMallocHost(&b->h_mem[k], sizeof(SplitMember) * max_instances)) != cudaSuccess ||
+             (e = cudaMallocHost(&b->h_upd[k], sizeof(UpdMember) * max_instances)) != cudaSuccess))
             return fail(e, "cudaMallocHost(batch arguments)");
         if ((e = cudaEventCreateWithFlags(&b->ev_args[k], cudaEventDisableTiming)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&b->ev_bin[k], cudaEventDisableTiming)) != cudaSuccess)
@@ -433,6 +444,7 @@ int icy_batch_destroy(icy_batch *b)
     for (int k = 0; k < icy_batch::NARGS; k++) {
         if (b->h_args[k]) cudaFreeHost(b->h_args[k]);
         if (b->h_mem[k]) cudaFreeHost(b->h_mem[k]);
+        if (b->h_upd[k]) cudaFreeHost(b->h_upd[k]);
         if (b->ev_args[k]) cudaEventDestroy(b->ev_args[k]);
         if (b->h_bin[k]) cudaFreeHost(b->h_bin[k]);
         if (b->ev_bin[k]) cudaEventDestroy(b->ev_bin[k]);

@@ -771,7 +771,10 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, in
 // Grid update of one node in FP32 (simulation/kernels.cuh:175-300) from its
 // mass and momentum, the indenter geometry and the force in FP64: the new
 // velocity, and the force bin of a contact node (-1 if none).
-__device__ __forceinline__ int node_velocity_f32(const StepParams &P, const SplitConsts &Q, int gx, int gy, float mass,
+// (P: h, dt, ind_rsq, ind_v, nsub, gridx, gridy as in StepParams; Q: h, dtg,
+// vmax, vmax_sq as in SplitConsts)
+template <class PT, class QT>
+__device__ __forceinline__ int node_velocity_f32(const PT &P, const QT &Q, int gx, int gy, float mass,
                                                  float px, float py, double ind_x, double ind_y, float &vx, float &vy,
                                                  double &fxd, double &fyd)
 {
@@ -1116,13 +1119,6 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
 struct BatchClock;
 constexpr int UPD_TILES = 4;
 
-// Grid update of a batch's listed node tiles, defined after BatchClock below.
-template <bool BATCH, class S = Shape32x8>
-static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_constant__ SplitArgs A1,
-                                                                const SplitArgs *__restrict__ Aarr,
-                                                                const BatchClock *__restrict__ clk,
-                                                                const int2 *__restrict__ tlist, unsigned *tlist_n,
-                                                                double ind_x, double ind_y);
 
 // ---------------------------------------------------------------- binning / conversion
 // Binning key and rank of point i of the blocked state st (n points): its
@@ -1525,35 +1521,68 @@ static __global__ void __launch_bounds__(S::TT) k_update_tiles_f32(const __grid_
     }
 }
 
-// Grid update of a batch's listed node tiles: each group of TT threads takes
-// one TX x TY node tile (one thread per node), clears its mark, and the last
-// CTA empties the list.  Every entry names its member, whose arguments are
-// looked up once per tile group, whose indenter position comes from the
-// member's clock and whose force bins take the force directly (for batches
-// this is faster than a batch form of k_update_tiles_f32 measured: its
-// per-entry lookups of member arguments cost more than its extra loads in
-// flight gain).  BATCH = false sums the forces per CTA in shared memory (no
-// caller: a single instance uses k_update_tiles_f32).
-template <bool BATCH, class S>
-static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_constant__ SplitArgs A1,
-                                                                const SplitArgs *__restrict__ Aarr,
-                                                                const BatchClock *__restrict__ clk,
-                                                                const int2 *__restrict__ tlist, unsigned *tlist_n,
-                                                                double ind_x, double ind_y)
+// The arguments a batch member's grid update reads: 104 of SplitArgs' bytes,
+// so that 300 members' fit the constant bank beside nothing else
+// (batch_uargs.cu); field names as in SplitArgs.
+struct UpdMember {
+    struct {
+        double h, dt, ind_rsq, ind_v;
+        int nsub, gridx, gridy, halo;
+    } P;
+    struct {
+        float h, dtg, vmax, vmax_sq;
+    } Q;
+    TileGeom G;
+    GridViewB g;
+    unsigned *flags;
+    double *acc;
+};
+static_assert(sizeof(UpdMember) * 300 <= 64000, "300 members' update arguments fit the constant bank");
+
+inline UpdMember upd_member(const SplitArgs &a)
+{
+    UpdMember m{};
+    m.P.h = a.P.h;
+    m.P.dt = a.P.dt;
+    m.P.ind_rsq = a.P.ind_rsq;
+    m.P.ind_v = a.P.ind_v;
+    m.P.nsub = a.P.nsub;
+    m.P.gridx = a.P.gridx;
+    m.P.gridy = a.P.gridy;
+    m.P.halo = a.P.halo;
+    m.Q.h = a.Q.h;
+    m.Q.dtg = a.Q.dtg;
+    m.Q.vmax = a.Q.vmax;
+    m.Q.vmax_sq = a.Q.vmax_sq;
+    m.G = a.G;
+    m.g = GridViewB{a.g.mp, a.g.v, a.g.ny, a.g.halo};
+    m.flags = a.flags;
+    m.acc = a.acc;
+    return m;
+}
+
+#ifdef ICY_BATCH_UPD_CONST_ARGS
+static __constant__ UpdMember c_upd_mem[BATCH_CONST_SLOTS];
+struct ConstUpdMembers {
+    __device__ __forceinline__ const UpdMember &operator[](int i) const { return c_upd_mem[i]; }
+};
+#endif
+
+// Grid update of a batch's listed node tiles (all members): UPD_TILES node
+// tiles per pass, their loads issued together; each member's velocities are
+// updated in place (the next launch reads them) and its accumulators
+// cleared; contact forces go to the member's bins.  TAB: where the members'
+// arguments are (the global table, or the constant-bank copy of batch_uargs.cu).
+template <class S, class TAB>
+static __global__ void __launch_bounds__(256, 4) k_update_list_f32(TAB tab, const BatchClock *__restrict__ clk,
+                                                                const int2 *__restrict__ tlist, unsigned *tlist_n)
 {
     ICY_TILE_SHAPE(S);
-    extern __shared__ double s_acc[];   // 2*nsub (alone only)
     const unsigned n = *(volatile unsigned *)tlist_n;
-    if (!BATCH) {
-        for (int k = threadIdx.x; k < 2 * A1.P.nsub; k += blockDim.x) s_acc[k] = 0;
-        __syncthreads();
-    }
-    bool any = false;
     constexpr int TPC = 256 / TT;   // node tiles per CTA pass
     static_assert(256 % TT == 0, "whole node tiles per 256-thread CTA");
     const int l = threadIdx.x % TT;
     const unsigned stride = gridDim.x * TPC;
-    // UPD_TILES tiles per pass, their loads issued together
     for (unsigned e0 = blockIdx.x * TPC + threadIdx.x / TT; e0 < n; e0 += stride * UPD_TILES) {
         long q[UPD_TILES];
         int inst[UPD_TILES], gx[UPD_TILES], gy[UPD_TILES];
@@ -1565,59 +1594,35 @@ static __global__ void __launch_bounds__(256, 4) k_update_list_f32(const __grid_
             if (e >= n) continue;
             const int2 it = tlist[e];
             inst[u] = it.x;
-            const SplitArgs &A = BATCH ? Aarr[it.x] : A1;
+            const auto &A = tab[it.x];
             const int tx = it.y & 0xffff, ty = it.y >> 16;
             if (l == 0) A.flags[ty * A.G.ntx + tx] = 0u;
             gx[u] = tx * TX + l / TY - A.P.halo;
             gy[u] = ty * TY + (l & (TY - 1));
             if (gx[u] >= A.P.gridx + A.P.halo || gy[u] >= A.P.gridy) continue;   // past the grid edge
             q[u] = A.g.idx(gx[u], gy[u]);
-            if constexpr (BATCH) {
-                const float4 a = A.g.mp[q[u]];
-                m[u] = a.x;
-                px[u] = a.y;
-                py[u] = a.z;
-            } else {
-                m[u] = A.g.m[q[u]];
-                px[u] = A.g.px[q[u]];
-                py[u] = A.g.py[q[u]];
-            }
+            const float4 a = A.g.mp[q[u]];
+            m[u] = a.x;
+            px[u] = a.y;
+            py[u] = a.z;
         }
 #pragma unroll
         for (int u = 0; u < UPD_TILES; u++) {
             if (q[u] < 0) continue;
-            const SplitArgs &A = BATCH ? Aarr[inst[u]] : A1;
+            const auto &A = tab[inst[u]];
             float vx, vy;
             double fx = 0, fy = 0;
-            const int bin = node_velocity_f32(A.P, A.Q, gx[u], gy[u], m[u], px[u], py[u],
-                                              BATCH ? clk[inst[u]].ind_x : ind_x, BATCH ? clk[inst[u]].y0 : ind_y,
-                                              vx, vy, fx, fy);
-            if constexpr (BATCH) {
-                A.g.v[q[u]] = make_float2(vx, vy);
-                A.g.mp[q[u]] = make_float4(0.f, 0.f, 0.f, 0.f);
-            } else {
-                A.g.nvx[q[u]] = vx;   // the velocities the next G2P reads
-                A.g.nvx[q[u] + A.n_nodes] = vy;
-                A.g.m[q[u]] = 0.f;
-                A.g.px[q[u]] = 0.f;
-                A.g.py[q[u]] = 0.f;
-            }
+            const int bin = node_velocity_f32(A.P, A.Q, gx[u], gy[u], m[u], px[u], py[u], clk[inst[u]].ind_x,
+                                              clk[inst[u]].y0, vx, vy, fx, fy);
+            A.g.v[q[u]] = make_float2(vx, vy);
+            A.g.mp[q[u]] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (bin >= 0) {
-                if (BATCH) {
-                    atomicAdd(A.acc + 2 * bin, fx);
-                    atomicAdd(A.acc + 2 * bin + 1, fy);
-                } else {
-                    atomicAdd(&s_acc[2 * bin], fx);
-                    atomicAdd(&s_acc[2 * bin + 1], fy);
-                    any = true;
-                }
+                atomicAdd(A.acc + 2 * bin, fx);
+                atomicAdd(A.acc + 2 * bin + 1, fy);
             }
         }
     }
-    if (!BATCH && __syncthreads_or(any))
-        for (int k = threadIdx.x; k < 2 * A1.P.nsub; k += blockDim.x)
-            if (s_acc[k] != 0.0) atomicAdd(A1.acc + k, s_acc[k]);
-    if (BATCH) __syncthreads();
+    __syncthreads();
     if (threadIdx.x == 0) tile_list_done(tlist_n);
 }
 
