@@ -660,11 +660,14 @@ __device__ __forceinline__ void cell_order_build(int (&hist)[CNT_BUCKETS], const
 }
 
 // phases 2 and 3 (see p2g_cells_and_flush in kernels_tiled.cuh), in FP32
-template <int NT, bool AOS, bool FUSE, class S, class AT, typename Sync>
+// `nxt`: the next work item's prologue, overlapped with this tile's node
+// phase (nxt.load() issues its global loads before the node loop, nxt.store()
+// puts the values into shared memory after it).
+template <int NT, bool AOS, bool FUSE, class S, class AT, typename Sync, class Next>
 __device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, int tx, int ty, int cs, int ce,
                                                         const int *s_cs, const int *s_perm, float *mom,
                                                         float (*s_odd)[S::RN], unsigned &touch, unsigned &moved,
-                                                        bool fused, Sync &&sync)
+                                                        bool fused, Sync &&sync, Next &&nxt)
 {
     ICY_TILE_SHAPE(S);
     const auto &P = A.P;
@@ -736,6 +739,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, in
         for (int q = 0; q < 9; q++) part[q * TT + cell] = make_float4(acc[3 * q], acc[3 * q + 1], acc[3 * q + 2], 0.f);
     }
     sync();
+    nxt.load();
     for (int k = tid; k < RN; k += NT) {
         const int i = k / RY, jj = k % RY;
         const int nx = i - RM, ny = jj - RM;
@@ -765,6 +769,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, in
             }
         }
     }
+    nxt.store();
     sync();
 }
 
@@ -860,6 +865,20 @@ __device__ __forceinline__ void update_node_tile_f32(const SplitArgs &A, int ntx
 // Threads and resident CTAs per SM of the FP32 tile kernel.
 constexpr int TILE_THREADS_F32 = 256, TILE_CTAS_F32 = 3;
 
+// The next work item's prologue run inside a tile's node phase (see
+// p2g_cells_and_flush_f32), or nothing.
+struct NoNext {
+    __device__ __forceinline__ void load() const {}
+    __device__ __forceinline__ void store() const {}
+};
+template <class L, class St>
+struct NextOps {
+    L l;
+    St st;
+    __device__ __forceinline__ void load() const { l(); }
+    __device__ __forceinline__ void store() const { st(); }
+};
+
 // Work items of a batch: (instance, tile) pairs over all instances.
 struct BatchItem { int inst, tile; };
 
@@ -931,6 +950,9 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
     __syncthreads();
     int ti = BATCH ? s_claim : (int)blockIdx.x;
     __syncthreads();   // everybody has read s_claim; later reads of it come before the item's last barrier
+    // the current item's prologue (cell ranges and order counts, staged node
+    // velocities) was done during the previous item's node phase
+    bool staged = false;
     while (ti < na) {
         const BatchItem w = BATCH ? work[ti] : BatchItem{0, A1.active[ti]};
         if (BATCH && tid == 0) s_claim = atomicAdd(A1.claim, 1);
@@ -946,7 +968,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
         const int t = w.tile;
         const int tx = t % A.G.ntx, ty = t / A.G.ntx;
         const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
-        {
+        if (!staged) {
             // cell ranges; each thread counts its own cell's points for the cell order
             const int *cst = A.cell_start + (long)t * TT;
             if (tid < TT) {
@@ -955,18 +977,19 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                 if (tid == TT - 1) s_cs[TT] = c1;
                 if (DO_P2G) cell_order_count(s_hist, s_rank, tid, c1 - c0);
             }
-        }
-        if (tid == 0) s_touch = 0;
-        if (DO_G2P) {
-            for (int k = tid; k < RN; k += blockDim.x) {
-                const int gx = RX0 + k / RY, gy = RY0 + k % RY;
-                s_v[k] = node_in_grid(P, gx, gy) ? A.g.vel<BATCH>(A.g.idx(gx, gy)) : make_float2(0.f, 0.f);
+            if (DO_G2P) {
+                for (int k = tid; k < RN; k += blockDim.x) {
+                    const int gx = RX0 + k / RY, gy = RY0 + k % RY;
+                    s_v[k] = node_in_grid(P, gx, gy) ? A.g.vel<BATCH>(A.g.idx(gx, gy)) : make_float2(0.f, 0.f);
+                }
             }
         }
+        if (tid == 0) s_touch = 0;
         __syncthreads();
         const int next = BATCH ? s_claim : ti + (int)gridDim.x;
         const int ps = s_cs[0], pe = s_cs[TT];
         unsigned touch = 0;
+        bool next_staged = false;
         for (int cs = ps; cs < pe; cs += CAPF) {
             const int ce = min(cs + CAPF, pe);
             for (int j = tid; j < ce - cs; j += blockDim.x) {
@@ -1043,8 +1066,57 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                     if (tid < 32) cell_order_build(s_hist, s_rank, s_perm, tid);
                     __syncthreads();
                 }
-                p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH, FUSE, S>(A, tid, tx, ty, cs, ce, s_cs, s_perm, s_momf, s_odd,
-                                                                 touch, moved, fused, [] { __syncthreads(); });
+                auto sync = [] { __syncthreads(); };
+                if (ce == pe && next < na) {
+                    // the last chunk: the next item's prologue during this node phase
+                    // (its global loads into registers before the node loop, into
+                    // shared memory after it; the staging pass cost 7 % when alone)
+                    constexpr int NV = (RN + TILE_THREADS_F32 - 1) / TILE_THREADS_F32;
+                    int nc0 = 0, nc1 = 0;
+                    float2 nvel[NV];
+                    auto ld = [&] {
+                        const BatchItem wn = BATCH ? work[next] : BatchItem{0, A1.active[next]};
+                        const auto &An = member_at<BATCH>(A1, tab, wn.inst);
+                        const int tn = wn.tile;
+                        if (tid < TT) {
+                            const int *cst = An.cell_start + (long)tn * TT;
+                            nc0 = cst[tid];
+                            nc1 = cst[tid + 1];
+                        }
+                        if (DO_G2P) {
+                            const int rx0 = (tn % An.G.ntx) * TX - An.P.halo - RM, ry0 = (tn / An.G.ntx) * TY - RM;
+#pragma unroll
+                            for (int u = 0; u < NV; u++) {
+                                const int k = tid + u * TILE_THREADS_F32;
+                                const int gx = rx0 + k / RY, gy = ry0 + k % RY;
+                                nvel[u] = k < RN && node_in_grid(An.P, gx, gy)
+                                              ? An.g.template vel<BATCH>(An.g.idx(gx, gy))
+                                              : make_float2(0.f, 0.f);
+                            }
+                        }
+                    };
+                    auto st = [&] {
+                        if (tid < TT) {
+                            s_cs[tid] = nc0;
+                            if (tid == TT - 1) s_cs[TT] = nc1;
+                            cell_order_count(s_hist, s_rank, tid, nc1 - nc0);
+                        }
+                        if (DO_G2P) {
+#pragma unroll
+                            for (int u = 0; u < NV; u++) {
+                                const int k = tid + u * TILE_THREADS_F32;
+                                if (k < RN) s_v[k] = nvel[u];
+                            }
+                        }
+                    };
+                    p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH, FUSE, S>(
+                        A, tid, tx, ty, cs, ce, s_cs, s_perm, s_momf, s_odd, touch, moved, fused, sync,
+                        NextOps<decltype(ld), decltype(st)>{ld, st});
+                    next_staged = true;
+                } else {
+                    p2g_cells_and_flush_f32<TILE_THREADS_F32, BATCH, FUSE, S>(
+                        A, tid, tx, ty, cs, ce, s_cs, s_perm, s_momf, s_odd, touch, moved, fused, sync, NoNext{});
+                }
             }
         }
         bool tail_done = false;
@@ -1102,6 +1174,7 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
             if ((tid & 31) == 0 && moved) atomicAdd(A.moved, (unsigned long long)moved);
         }
         if (FUSE || !DO_P2G) __syncthreads();   // the fused path reads s_touch; G2P only: s_v, s_cs reused
+        staged = next_staged;
         ti = next;
     }
     // the last CTA to finish resets the counters for the next launch: every
