@@ -219,6 +219,7 @@ class Server:
         pending = sorted(requests, key=lambda r: r.arrival)
         pi = 0
         work = 0.0
+        sat = []                # (time, work) of the rounds queued while requests waited for admission
         t0 = time.perf_counter()
         while pi < len(pending) or self.queue or self.running or self.retired:
             now = time.perf_counter() - t0
@@ -231,9 +232,13 @@ class Server:
                 self.batch.step(self.round_steps)
                 stepped = True
                 self.rounds += 1
+                rw = 0.0
                 for r in self.running.values():
                     r.steps_done += self.round_steps
-                    work += r.points * self.round_steps
+                    rw += r.points * self.round_steps
+                work += rw
+                if self.queue:
+                    sat.append((time.perf_counter() - t0, rw))
             finished = self._retire_finished()
             # at most this round in flight; the previous round's results are copied by now
             self.batch.wait_steps(1)
@@ -256,6 +261,11 @@ class Server:
         makespan = time.perf_counter() - t0
         self._released.clear()
         lat = np.array([r.done - r.arrival for r in self.completed]) if self.completed else np.zeros(1)
+        # the device's rate while the server was saturated (requests waiting): the
+        # rounds queued then, over the time between the first and the last (the host
+        # queues a round only when the one before the last has finished)
+        sat_s = sat[-1][0] - sat[0][0] if len(sat) > 2 else 0.0
+        sat_rate = sum(w for _, w in sat[1:]) / sat_s if sat_s > 0 else None
         return {
             "requests": len(self.completed),
             "budget_bytes": self.budget,
@@ -265,6 +275,8 @@ class Server:
             "makespan_s": makespan,
             "particle_steps": work,
             "particle_steps_per_s": work / makespan if makespan > 0 else 0.0,
+            "saturated_particle_steps_per_s": sat_rate,
+            "saturated_s": sat_s,
             "latency_p50_s": float(np.percentile(lat, 50)),
             "latency_p99_s": float(np.percentile(lat, 99)),
             "latency_mean_s": float(lat.mean()),
