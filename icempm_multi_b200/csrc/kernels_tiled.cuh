@@ -470,11 +470,25 @@ __device__ __forceinline__ void mom_none(double *mom, int j)
 // threads (tid < TT) sum their points' contributions in registers, then every
 // region node adds its 9 cell partials in a fixed order plus the off-cell
 // contributions and flushes to the global grid.  `sync` is a barrier over
-// the NT participating threads.
-template <int NT, typename Sync>
+// the NT participating threads.  `nxt`: the next tile's prologue, overlapped
+// with the node phase (nxt.load() before the node loop issues its global
+// loads, nxt.store() after it puts them into shared memory).
+struct NoNextTile {
+    __device__ __forceinline__ void load() const {}
+    __device__ __forceinline__ void store() const {}
+};
+template <class L, class St>
+struct NextTileOps {
+    L l;
+    St st;
+    __device__ __forceinline__ void load() const { l(); }
+    __device__ __forceinline__ void store() const { st(); }
+};
+template <int NT, typename Sync, class Next = NoNextTile>
 __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, int tx, int ty, int cs, int ce,
                                                     const int *s_cs, double *mom, double (*s_odd)[RN],
-                                                    unsigned &touch, unsigned &moved, Sync &&sync)
+                                                    unsigned &touch, unsigned &moved, Sync &&sync,
+                                                    Next &&nxt = NoNextTile{})
 {
     const StepParams &P = A.P;
     const int X0 = tx * TX - P.halo, Y0 = ty * TY;
@@ -536,6 +550,7 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
         }
     }
     sync();
+    nxt.load();
     for (int k = tid; k < RN; k += NT) {
         const int i = k / RY, jj = k % RY;        // region coordinates
         const int nx = i - RM, ny = jj - RM;       // node relative to the tile's first base
@@ -567,6 +582,7 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
             touch |= 1u << (dy * 3 + dx);
         }
     }
+    nxt.store();
     sync();   // partials consumed before the buffer is refilled
 }
 
@@ -638,24 +654,29 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_co
     const int tid = threadIdx.x;
     unsigned moved = 0;
     for (int k = tid; k < RN; k += blockDim.x) { s_odd[0][k] = 0; s_odd[1][k] = 0; s_odd[2][k] = 0; }
+    // the tile's prologue (cell ranges, staged node velocities) was done during
+    // the previous tile's node phase
+    bool staged = false;
     for (int ti = blockIdx.x; ti < na; ti += gridDim.x) {
         const int t = A.active[ti];
         const int tx = t % A.G.ntx, ty = t / A.G.ntx;
         const int RX0 = tx * TX - P.halo - RM, RY0 = ty * TY - RM;
-        for (int c = tid; c <= TT; c += blockDim.x) s_cs[c] = A.cell_start[(long)t * TT + c];
-        if (tid == 0) s_touch = 0;
-        if (DO_G2P) {
-            for (int k = tid; k < RN; k += blockDim.x) {
-                const int gx = RX0 + k / RY, gy = RY0 + k % RY;
-                double vx = 0, vy = 0;
-                if (node_in_grid(P, gx, gy)) {
-                    const long q = A.g.idx(gx, gy);
-                    vx = A.g.vx[q];
-                    vy = A.g.vy[q];
+        if (!staged) {
+            for (int c = tid; c <= TT; c += blockDim.x) s_cs[c] = A.cell_start[(long)t * TT + c];
+            if (DO_G2P) {
+                for (int k = tid; k < RN; k += blockDim.x) {
+                    const int gx = RX0 + k / RY, gy = RY0 + k % RY;
+                    double vx = 0, vy = 0;
+                    if (node_in_grid(P, gx, gy)) {
+                        const long q = A.g.idx(gx, gy);
+                        vx = A.g.vx[q];
+                        vy = A.g.vy[q];
+                    }
+                    s_v[k] = make_double2(vx, vy);
                 }
-                s_v[k] = make_double2(vx, vy);
             }
         }
+        if (tid == 0) s_touch = 0;
         __syncthreads();
         const int ps = s_cs[0], pe = s_cs[TT];
         // the 3 x 3 node velocities of a stencil: from the staged region (one check
@@ -679,6 +700,7 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_co
             }
         };
         unsigned touch = 0;
+        bool next_staged = false;
         for (int cs = ps; cs < pe; cs += CAP) {
             const int ce = min(cs + CAP, pe);
             for (int j = tid; j < ce - cs; j += blockDim.x) {
@@ -713,9 +735,56 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_co
             // the last threads start the next tile's loads during the cell phase
             if (DO_P2G && cs == ps && tid >= TILE_THREADS - TILE_PREFETCHES)
                 prefetch_next_tile(A, ti + gridDim.x, na, tid - (TILE_THREADS - TILE_PREFETCHES));
-            if (DO_P2G)
+            const int nti = ti + gridDim.x;
+            if (DO_P2G && ce == pe && nti < na) {
+                // the last chunk: the next tile's prologue during this node phase
+                constexpr int NC = (TT + 1 + TILE_THREADS - 1) / TILE_THREADS, NV = (RN + TILE_THREADS - 1) / TILE_THREADS;
+                int ncs[NC];
+                double2 nvel[NV];
+                auto ld = [&] {
+                    const int tn = A.active[nti];
+#pragma unroll
+                    for (int u = 0; u < NC; u++) {
+                        const int c = tid + u * TILE_THREADS;
+                        ncs[u] = c <= TT ? A.cell_start[(long)tn * TT + c] : 0;
+                    }
+                    if (DO_G2P) {
+                        const int rx0 = (tn % A.G.ntx) * TX - P.halo - RM, ry0 = (tn / A.G.ntx) * TY - RM;
+#pragma unroll
+                        for (int u = 0; u < NV; u++) {
+                            const int k = tid + u * TILE_THREADS;
+                            const int gx = rx0 + k / RY, gy = ry0 + k % RY;
+                            double vx = 0, vy = 0;
+                            if (k < RN && node_in_grid(P, gx, gy)) {
+                                const long q = A.g.idx(gx, gy);
+                                vx = A.g.vx[q];
+                                vy = A.g.vy[q];
+                            }
+                            nvel[u] = make_double2(vx, vy);
+                        }
+                    }
+                };
+                auto st = [&] {
+#pragma unroll
+                    for (int u = 0; u < NC; u++) {
+                        const int c = tid + u * TILE_THREADS;
+                        if (c <= TT) s_cs[c] = ncs[u];
+                    }
+                    if (DO_G2P) {
+#pragma unroll
+                        for (int u = 0; u < NV; u++) {
+                            const int k = tid + u * TILE_THREADS;
+                            if (k < RN) s_v[k] = nvel[u];
+                        }
+                    }
+                };
+                p2g_cells_and_flush<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_mom, s_odd, touch, moved,
+                                                  [] { __syncthreads(); }, NextTileOps<decltype(ld), decltype(st)>{ld, st});
+                next_staged = true;
+            } else if (DO_P2G) {
                 p2g_cells_and_flush<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_mom, s_odd, touch, moved,
                                                   [] { __syncthreads(); });
+            }
         }
         if (DO_P2G) {
             touch = __reduce_or_sync(0xffffffffu, touch);
@@ -724,6 +793,7 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_co
             mark_node_tiles(A, tx, ty, s_touch, tid);
         }
         __syncthreads();
+        staged = next_staged;
     }
     if (DO_P2G) {
         moved = __reduce_add_sync(0xffffffffu, moved);
