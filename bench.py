@@ -452,6 +452,33 @@ def measure_serve(rate=10.0, duration=12.0, seed=11, budget=150e9, max_instances
     return st
 
 
+def measure_slabs(p, soa, parts=(1, 2, 4), steps=50, warmup=5):
+    """One instance in slabs of grid columns on this GPU (icy_part_*, the
+    reference's multi-partition layout): the same instance split 1, 2 and 4
+    ways, FP64 one-thread-per-item kernels, boundary columns added between
+    neighbours at every step and points handed over every
+    UpdateEveryNthStep / PointTransferFrequency steps.  Wall time of `steps`
+    steps between device synchronisations."""
+    import time
+    import torch
+    from icempm_multi_b200.partition import Partitioned
+    out = {}
+    for n in parts:
+        part = Partitioned(p, n, size_hint=soa.size)
+        part.upload(soa)
+        t = part.run_steps(0, warmup, 0.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        part.run_steps(warmup, steps, t)
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+        part.close()
+        out[f"{n}"] = {"value": soa.size * steps / secs, "ms_per_step": secs * 1e3 / steps}
+    return {"unit": METRIC, "steps": steps, "partitions": out,
+            "workload": "the single-instance workload in 1, 2 and 4 slabs on one GPU, FP64, one thread per "
+                        "point / node (the reference's kernel structure)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -577,6 +604,10 @@ def main():
                 out["served_budget"] = measure_serve(rate=20.0, duration=6.0, budget=2.5e9, max_instances=300)
             except Exception as e:
                 out["batched_or_served_error"] = str(e)[:300]
+            try:
+                out["slabs"] = measure_slabs(p, soa)
+            except Exception as e:
+                out["slabs"] = {"unavailable": str(e)[:200]}
         # ---- CPU baseline ------------------------------------------------------------------
         if not args.no_cpu_baseline:
             try:
