@@ -197,3 +197,22 @@ def test_batch_rebinning_matches_single(oracle, shape):
         assert oracle.run(p, ref, 0, 120)[0] == 0
         assert field_errors(out, ref)["pos"] <= POS_TOL
     b.close()
+
+
+def test_reserved_pool_serves_members(oracle):
+    """icy_mpm_reserve maps device memory into the instance pool up front
+    (a negative size is refused); members admitted afterwards still match
+    their single-instance runs."""
+    import ctypes as C
+    from icempm_multi_b200._lib import ICY_ERR_INVALID_ARGUMENT, lib
+    assert lib().icy_mpm_reserve(0, C.c_int64(-1)) == ICY_ERR_INVALID_ARGUMENT
+    b = Batch(4)
+    b.reserve(256 << 20)
+    p, soa = standard(seed=47)
+    s = b.add_async(p, soa)
+    b.step(40)
+    out = soa.clone()
+    assert b.download(s, out)[1] == 40
+    one, _ = single_f32(p, soa, 40, 40)
+    assert field_errors(out, one)["pos"] <= 1e-6
+    b.close()

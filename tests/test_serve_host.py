@@ -191,3 +191,16 @@ def test_late_arrival_joins_a_running_batch(fake):
     assert both, "the second request never ran beside the first"
     done = {r.rid: r for r in srv.completed}
     assert done[1].admitted < done[0].done
+
+
+def test_saturated_rate_is_reported_when_requests_wait(fake):
+    """With more requests than slots, rounds run while requests wait: the
+    stats carry the rate over those rounds (and None when nothing waited)."""
+    reqs = _requests(9, [40] * 9)
+    srv = S.Server(budget_bytes=1e12, max_instances=3, round_steps=20)
+    stats = srv.run(reqs)
+    assert stats["saturated_s"] >= 0.0
+    assert stats["saturated_particle_steps_per_s"] is None or stats["saturated_particle_steps_per_s"] > 0
+    srv2 = S.Server(budget_bytes=1e12, max_instances=16, round_steps=20)
+    stats2 = srv2.run(_requests(3, [40] * 3))
+    assert stats2["saturated_particle_steps_per_s"] is None and stats2["saturated_s"] == 0.0
