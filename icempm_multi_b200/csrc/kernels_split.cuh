@@ -4,12 +4,12 @@
 // `pitch` points of capacity (a multiple of 32), 17 words per point:
 //   hot part, read and written at every step, 288 words per block:
 //     words [0, 128)    one 16-byte vector per point: (base word, gx, gy, utility)
-//     words [128, 256)  one 16-byte vector per point: De = Fe - I (d00, d01, d10, d11)
+//     words [128, 256)  one 16-byte vector per point: De = Fe - I by columns (d00, d10, d01, d11)
 //     words [256, 288)  Jp_inv per point
 //   cold part (from word 9 * pitch on), written on the last step of a call
 //   and on record steps only, 256 words per block:
 //     words [0, 128)    (vx, vy, P, Q) per point
-//     words [128, 256)  Bp (b00, b01, b10, b11) per point
+//     words [128, 256)  Bp by columns (b00, b10, b01, b11) per point
 // so that a thread reads and writes a point's step state with two 128-bit
 // and one 32-bit access, a warp's accesses are contiguous, and a tile's
 // points (consecutive after binning) are one contiguous range of the hot part.
@@ -136,32 +136,48 @@ __device__ __forceinline__ bool split_rebase(int &b, float &g)
     return true;
 }
 
+// Paired FP32 arithmetic of sm_100 (the FFMA2 / FADD2 / FMUL2 instructions):
+// two independent operations in one instruction, each component rounded as
+// the scalar __fmaf_rn / __fadd_rn / __fmul_rn.  A pair holds the two
+// components of a vector (a velocity, a momentum, a column of De, Bp or the
+// affine moment), or one value twice (p_dup: a weight scaling both).
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_dup(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 p_neg(float2 a) { return make_float2(-a.x, -a.y); }
+
 // quadratic B-spline weights of the stencil columns 0, 1, 2 (simulation/kernels.cuh:100-103)
-// with fx = 1 + g
-__device__ __forceinline__ void weights_g(float g, float w[3])
+// with fx = 1 + g, for the two offsets of g at once: 0.5 (0.5 - g)^2,
+// 0.75 - g^2, 0.5 (0.5 + g)^2 (g = (t, t) gives each weight twice)
+__device__ __forceinline__ void weights_g2(float2 g, float2 w[3])
 {
-    const float a0 = 0.5f - g, a2 = 0.5f + g;
-    w[0] = (0.5f * a0) * a0;
-    w[1] = 0.75f - g * g;
-    w[2] = (0.5f * a2) * a2;
+    const float2 h = p_dup(0.5f);
+    const float2 a0 = p_add(h, p_neg(g)), a2 = p_add(h, g);
+    w[0] = p_mul(p_mul(h, a0), a0);
+    w[1] = p_fma(p_neg(g), g, p_dup(0.75f));
+    w[2] = p_mul(p_mul(h, a2), a2);
 }
 
-// dev(Fe Fe^T) and J = det Fe from De = Fe - I, without cancellation:
+// dev(Fe Fe^T) and J = det Fe from De = Fe - I, given by its columns
+// d0 = (d00, d10), d1 = (d01, d11), without cancellation:
 // Fe Fe^T - I = De + De^T + De De^T, J - 1 = tr De + det De.
-__device__ __forceinline__ void split_dev(const M2<float> &D, float &jm1, float &d00, float &d01)
+__device__ __forceinline__ void split_dev(float2 d0, float2 d1, float &jm1, float &d00, float &d01)
 {
-    jm1 = (D.a00 + D.a11) + (D.a00 * D.a11 - D.a10 * D.a01);
-    const float b00 = 2.f * D.a00 + D.a00 * D.a00 + D.a01 * D.a01;
-    const float b11 = 2.f * D.a11 + D.a10 * D.a10 + D.a11 * D.a11;
+    const float a00 = d0.x, a10 = d0.y, a01 = d1.x, a11 = d1.y;
+    jm1 = (a00 + a11) + (a00 * a11 - a10 * a01);
+    const float b00 = 2.f * a00 + a00 * a00 + a01 * a01;
+    const float b11 = 2.f * a11 + a10 * a10 + a11 * a11;
     d00 = 0.5f * (b00 - b11);
-    d01 = D.a01 + D.a10 + D.a00 * D.a10 + D.a01 * D.a11;
+    d01 = a01 + a10 + a00 * a10 + a01 * a11;
 }
 
 struct PointF {
     unsigned util, bw;   // utility (low 32 bits), base word
     int bx, by;
-    float gx, gy, Jp, vx, vy, ptr, qtr;
-    M2<float> D, B;
+    float gx, gy, Jp, ptr, qtr;
+    float2 v;            // (vx, vy)
+    float2 d0, d1, b0, b1;   // columns of De = Fe - I and of Bp: (a00, a10), (a01, a11)
     // J and dev(Fe Fe^T) of the current D from ComputePQ, reused by P2G's stress
     // (dev_ok: D unchanged since, i.e. no return mapping)
     float je, dv0, dv1;
@@ -231,50 +247,51 @@ __device__ __forceinline__ bool g2p_update_f32(const PT &P, const SplitConsts &Q
 {
     const int e = split_base_error(P, s.bw, s.bx, s.by);
     if (e) { *status = e; return false; }
-    float wx[3], wy[3];
-    weights_g(s.gx, wx);
-    weights_g(s.gy, wy);
+    // the weights of each axis, each held twice: it scales both velocity components
+    float2 wx[3], wy[3];
+    weights_g2(p_dup(s.gx), wx);
+    weights_g2(p_dup(s.gy), wy);
     // v = sum W v_i and Bp = 4/h sum W v_i (i - f)^T (kernels.cuh:357-372),
     // separably: sums over b with wy per column a, then over a with wx;
-    // sum W v_i (i - f) = sum W v_i (i - 1) - g v
+    // sum W v_i (i - f) = sum W v_i (i - 1) - g v; (vx, vy) paired throughout
     float2 nv[9];
     vsrc(s.bx, s.by, nv);
-    float cvx[3], cvy[3], cbx[3], cby[3];
+    float2 cv[3], cb[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         const float2 n0 = nv[a * 3], n1 = nv[a * 3 + 1], n2 = nv[a * 3 + 2];
-        cvx[a] = wy[0] * n0.x + wy[1] * n1.x + wy[2] * n2.x;
-        cvy[a] = wy[0] * n0.y + wy[1] * n1.y + wy[2] * n2.y;
-        cbx[a] = wy[2] * n2.x - wy[0] * n0.x;
-        cby[a] = wy[2] * n2.y - wy[0] * n0.y;
+        cv[a] = p_fma(wy[2], n2, p_fma(wy[1], n1, p_mul(wy[0], n0)));
+        cb[a] = p_fma(wy[2], n2, p_neg(p_mul(wy[0], n0)));
     }
-    const float vx = wx[0] * cvx[0] + wx[1] * cvx[1] + wx[2] * cvx[2];
-    const float vy = wx[0] * cvy[0] + wx[1] * cvy[1] + wx[2] * cvy[2];
-    const float sax = wx[2] * cvx[2] - wx[0] * cvx[0], say = wx[2] * cvy[2] - wx[0] * cvy[0];
-    const float sbx = wx[0] * cbx[0] + wx[1] * cbx[1] + wx[2] * cbx[2];
-    const float sby = wx[0] * cby[0] + wx[1] * cby[1] + wx[2] * cby[2];
-    const M2<float> B{Q.s4 * (sax - s.gx * vx), Q.s4 * (sbx - s.gy * vx), Q.s4 * (say - s.gx * vy),
-                      Q.s4 * (sby - s.gy * vy)};
+    const float2 v = p_fma(wx[2], cv[2], p_fma(wx[1], cv[1], p_mul(wx[0], cv[0])));
+    const float2 sa = p_fma(wx[2], cv[2], p_neg(p_mul(wx[0], cv[0])));
+    const float2 sb = p_fma(wx[2], cb[2], p_fma(wx[1], cb[1], p_mul(wx[0], cb[0])));
+    // the columns of Bp: (B00, B10) = 4/h (sa - gx v), (B01, B11) = 4/h (sb - gy v)
+    const float2 s4 = p_dup(Q.s4);
+    const float2 b0 = p_mul(s4, p_fma(p_dup(-s.gx), v, sa));
+    const float2 b1 = p_mul(s4, p_fma(p_dup(-s.gy), v, sb));
     // advection in cell units, x += v dt (kernels.cuh:375)
-    s.gx += vx * Q.dt_hinv;
-    s.gy += vy * Q.dt_hinv;
+    s.gx += v.x * Q.dt_hinv;
+    s.gy += v.y * Q.dt_hinv;
     const bool mx = split_rebase(s.bx, s.gx);
     const bool my = split_rebase(s.by, s.gy);
     if (mx || my) s.bw = split_pack(s.bx, s.by);
-    // Fe <- (I + dt Bp) Fe  as  De <- De + T + T De,  T = dt Bp (kernels.cuh:376)
-    const M2<float> T{Q.dt * B.a00, Q.dt * B.a01, Q.dt * B.a10, Q.dt * B.a11};
-    const M2<float> D = s.D;
-    s.D = {D.a00 + T.a00 + (T.a00 * D.a00 + T.a01 * D.a10), D.a01 + T.a01 + (T.a00 * D.a01 + T.a01 * D.a11),
-           D.a10 + T.a10 + (T.a10 * D.a00 + T.a11 * D.a10), D.a11 + T.a11 + (T.a10 * D.a01 + T.a11 * D.a11)};
+    // Fe <- (I + dt Bp) Fe  as  De <- De + T + T De,  T = dt Bp (kernels.cuh:376),
+    // by columns: column j of T De is T(:,0) De(0,j) + T(:,1) De(1,j)
+    const float2 dtp = p_dup(Q.dt);
+    const float2 t0 = p_mul(dtp, b0), t1 = p_mul(dtp, b1);
+    const float2 d0 = s.d0, d1 = s.d1;
+    s.d0 = p_add(p_add(d0, t0), p_fma(t1, p_dup(d0.y), p_mul(t0, p_dup(d0.x))));
+    s.d1 = p_add(p_add(d1, t1), p_fma(t1, p_dup(d1.y), p_mul(t0, p_dup(d1.x))));
     s.ptr = 0.f;
     s.qtr = 0.f;
     s.dev_ok = false;
     if (s.util & (unsigned)kLiquid) {
-        s.Jp *= (1.f + T.a00) * (1.f + T.a11) - T.a10 * T.a01;   // kernels.cuh:380
+        s.Jp *= (1.f + t0.x) * (1.f + t1.y) - t0.y * t1.x;   // kernels.cuh:380
     } else {
         // ComputePQ (kernels.cuh:547-557) from De
         float jm1, d00, d01;
-        split_dev(s.D, jm1, d00, d01);
+        split_dev(s.d0, s.d1, jm1, d00, d01);
         const float Je = 1.f + jm1;
         s.ptr = -(Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
         s.je = Je;
@@ -295,15 +312,16 @@ __device__ __forceinline__ bool g2p_update_f32(const PT &P, const SplitConsts &Q
             if (crushed) s.util |= (unsigned)kCrushed;
         }
         if (s.util & (unsigned)kCrushed) {
-            const SplitRm r = return_map_split(rare_params(P), s.D.a00, s.D.a01, s.D.a10, s.D.a11, s.Jp);
-            s.D = {r.d00, r.d01, r.d10, r.d11};
+            const SplitRm r = return_map_split(rare_params(P), s.d0.x, s.d1.x, s.d0.y, s.d1.y, s.Jp);
+            s.d0 = make_float2(r.d00, r.d10);
+            s.d1 = make_float2(r.d01, r.d11);
             s.Jp = r.jp;
             s.dev_ok = false;
         }
     }
-    s.vx = vx;
-    s.vy = vy;
-    s.B = B;
+    s.v = v;
+    s.b0 = b0;
+    s.b1 = b1;
     return true;
 }
 
@@ -312,13 +330,13 @@ __device__ __forceinline__ void store_point_f32(unsigned *__restrict__ st, long 
 {
     unsigned *v = hot_vec(st, i);
     *reinterpret_cast<uint4 *>(v) = make_uint4(s.bw, __float_as_uint(s.gx), __float_as_uint(s.gy), s.util);
-    *reinterpret_cast<float4 *>(v + 128) = make_float4(s.D.a00, s.D.a01, s.D.a10, s.D.a11);
+    *reinterpret_cast<float4 *>(v + 128) = make_float4(s.d0.x, s.d0.y, s.d1.x, s.d1.y);
     reinterpret_cast<float *>(st)[hot_jp(i)] = s.Jp;
     if (write_vb || record_pq) {
         float *c = reinterpret_cast<float *>(st) + cold_vec(pitch, i);
         if (write_vb) {
-            *reinterpret_cast<float2 *>(c) = make_float2(s.vx, s.vy);
-            *reinterpret_cast<float4 *>(c + 128) = make_float4(s.B.a00, s.B.a01, s.B.a10, s.B.a11);
+            *reinterpret_cast<float2 *>(c) = s.v;
+            *reinterpret_cast<float4 *>(c + 128) = make_float4(s.b0.x, s.b0.y, s.b1.x, s.b1.y);
         }
         if (record_pq) *reinterpret_cast<float2 *>(c + 2) = make_float2(s.ptr, s.qtr);
     }
@@ -335,7 +353,8 @@ __device__ __forceinline__ bool load_point_f32(const unsigned *__restrict__ st, 
     s.gx = __uint_as_float(a.y);
     s.gy = __uint_as_float(a.z);
     s.util = a.w;
-    s.D = {d.x, d.y, d.z, d.w};
+    s.d0 = make_float2(d.x, d.y);
+    s.d1 = make_float2(d.z, d.w);
     s.dev_ok = false;
     split_unpack(s.bw, s.bx, s.by);
     return !(s.util & (unsigned)kDisabled);
@@ -344,8 +363,9 @@ __device__ __forceinline__ bool load_point_f32(const unsigned *__restrict__ st, 
 // ---------------------------------------------------------------- P2G (FP32)
 // Moments of a point as three vectors in shared memory, one padding column
 // after every 4 points (the cell phase reads points about 4 apart per lane):
-//   m0 = (gx, gy, mass, m vx),  m1 = (m vy, S00, S01, S10),  m2 = (S11, base word)
-// with S = m Bp - dt vol Dp_inv tau (simulation/kernels.cuh:57-92).
+//   m0 = (gx, gy, m vx, m vy),  m1 = (S00, S10, S01, S11),  m2 = (mass, base word)
+// with S = m Bp - dt vol Dp_inv tau (simulation/kernels.cuh:57-92), so that
+// the momentum and the columns of S load as aligned pairs.
 constexpr int CAPF = 1280;                // points per chunk of the FP32 tile kernel
 constexpr int MOMF_N = CAPF + CAPF / 4;
 constexpr size_t MOMF_BYTES = (2 * sizeof(float4) + sizeof(float2)) * MOMF_N;
@@ -375,10 +395,11 @@ __device__ __forceinline__ void p2g_moments_f32(const PT &P, const SplitConsts &
         M.none(j);
         return;
     }
-    M2<float> tau;
+    float2 tau0, tau1;   // columns of tau
     if (liquid) {
         const float sw = (float)(rare_params(P).kappa * (1. - pow((double)s.Jp, -5.0)));   // Water (kernels.cuh:37-44)
-        tau = {sw, 0.f, 0.f, sw};
+        tau0 = make_float2(sw, 0.f);
+        tau1 = make_float2(0.f, sw);
     } else {
         // KirchhoffStress_Wolper (kernels.cuh:24-34) from De: mu/J dev(Fe Fe^T) +
         // kappa/2 (J^2 - 1) I, the second term -p of ComputePQ; J and the
@@ -391,18 +412,21 @@ __device__ __forceinline__ void p2g_moments_f32(const PT &P, const SplitConsts &
             s2 = -s.ptr;
         } else {
             float jm1;
-            split_dev(s.D, jm1, d00, d01);
+            split_dev(s.d0, s.d1, jm1, d00, d01);
             Je = 1.f + jm1;
             s2 = (Q.kappa * 0.5f) * (jm1 * (Je + 1.f));
         }
         const float s1 = __fdividef(Q.mu, Je);
-        tau = {s1 * d00 + s2, s1 * d01, s1 * d01, -s1 * d00 + s2};
+        tau0 = make_float2(s1 * d00 + s2, s1 * d01);
+        tau1 = make_float2(s1 * d01, -s1 * d00 + s2);
     }
     const int c = momf_col(j);
-    M.m0[c] = make_float4(s.gx, s.gy, mass, s.vx * mass);
-    M.m1[c] = make_float4(s.vy * mass, mass * s.B.a00 - Q.dtvd * tau.a00, mass * s.B.a01 - Q.dtvd * tau.a01,
-                          mass * s.B.a10 - Q.dtvd * tau.a10);
-    M.m2[c] = make_float2(mass * s.B.a11 - Q.dtvd * tau.a11, __uint_as_float(s.bw));
+    const float2 mp = p_dup(mass), ndt = p_dup(-Q.dtvd);
+    const float2 mv = p_mul(mp, s.v);
+    const float2 S0 = p_fma(mp, s.b0, p_mul(ndt, tau0)), S1 = p_fma(mp, s.b1, p_mul(ndt, tau1));
+    M.m0[c] = make_float4(s.gx, s.gy, mv.x, mv.y);
+    M.m1[c] = make_float4(S0.x, S0.y, S1.x, S1.y);
+    M.m2[c] = make_float2(mass, __uint_as_float(s.bw));
 }
 
 // (m, px, py) += (dm, dpx, dpy) on a float4 node with one vector reduction
@@ -576,17 +600,27 @@ __device__ __forceinline__ decltype(auto) member_at(const SplitArgs &A1, const T
 // 100-120): node (a, b) gets W m and W (m v + S d) with W = wx[a] wy[b] and
 // d = ((a - fx) h, (b - fy) h) = ((a - 1 - gx) h, (b - 1 - gy) h).  S d is
 // affine in (a, b), so it is evaluated as c + (a - 1) S(:,0) h + (b - 1) S(:,1) h:
-// per node one product for W and one addition per component.
+// per node one product for W and one addition per component.  In scalar
+// arithmetic: the paired form of this loop (W twice, (tx, ty) and the
+// momentum sums as pairs) needs aligned register pairs for the 9 momentum
+// sums of the cell phase, and at 80 registers the tile kernel then spills
+// four times as much.
+__device__ __forceinline__ void weights_g(float g, float w[3])
+{
+    const float a0 = 0.5f - g, a2 = 0.5f + g;
+    w[0] = (0.5f * a0) * a0;
+    w[1] = 0.75f - g * g;
+    w[2] = (0.5f * a2) * a2;
+}
 template <typename Sink>
-__device__ __forceinline__ void point_contributions_f32(float h, float gx, float gy, float mass, float mvx,
-                                                        float mvy, float s00, float s01, float s10, float s11,
-                                                        Sink &&sink)
+__device__ __forceinline__ void point_contributions_f32(float h, float gx, float gy, float mass, float2 mv,
+                                                        float2 S0, float2 S1, Sink &&sink)
 {
     float wx[3], wy[3];
     weights_g(gx, wx);
     weights_g(gy, wy);
-    const float s00h = s00 * h, s01h = s01 * h, s10h = s10 * h, s11h = s11 * h;
-    const float cx = mvx - (s00h * gx + s01h * gy), cy = mvy - (s10h * gx + s11h * gy);
+    const float s00h = S0.x * h, s01h = S1.x * h, s10h = S0.y * h, s11h = S1.y * h;
+    const float cx = mv.x - (s00h * gx + s01h * gy), cy = mv.y - (s10h * gx + s11h * gy);
 #pragma unroll
     for (int a = 0; a < 3; a++) {
         const float ax = a == 0 ? cx - s00h : a == 1 ? cx : cx + s00h;
@@ -604,14 +638,12 @@ __device__ __forceinline__ void point_contributions_f32(float h, float gx, float
 template <bool AOS, class S, class GV>
 static __device__ __noinline__ void p2g_global_f32(GV g, unsigned *flags, int2 *tlist, unsigned *tlist_n,
                                                    int inst, int ntx, int halo, float h, int bx, int by, float gx,
-                                                   float gy, float mass, float mvx, float mvy, float s00, float s01,
-                                                   float s10, float s11)
+                                                   float gy, float mass, float2 mv, float2 S0, float2 S1)
 {
     ICY_TILE_SHAPE(S);
-    point_contributions_f32(h, gx, gy, mass, mvx, mvy, s00, s01, s10, s11,
-                            [&](int a, int b, float W, float dm, float tx, float ty) {
-                                g.add<AOS>(g.idx(bx + a, by + b), dm, W * tx, W * ty);
-                            });
+    point_contributions_f32(h, gx, gy, mass, mv, S0, S1, [&](int a, int b, float W, float dm, float tx, float ty) {
+        g.add<AOS>(g.idx(bx + a, by + b), dm, W * tx, W * ty);
+    });
     const int t0x = (bx + halo) / TX, t1x = (bx + 2 + halo) / TX;
     const int t0y = by / TY, t1y = (by + 2) / TY;
     mark_tile(flags, tlist, tlist_n, inst, t0x, t0y, ntx);
@@ -673,9 +705,13 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, in
     const auto &P = A.P;
     const int X0 = tx * TX - P.halo, Y0 = ty * TY;
     const int RX0 = X0 - RM, RY0 = Y0 - RM;
-    float acc[27];
+    float accm[9];     // per node of the stencil: mass and momentum
+    float2 accp[9];
 #pragma unroll
-    for (int q = 0; q < 27; q++) acc[q] = 0.f;
+    for (int q = 0; q < 9; q++) {
+        accm[q] = 0.f;
+        accp[q] = make_float2(0.f, 0.f);
+    }
     if (tid < TT) {
         const int cell = s_perm[tid];
         const unsigned pbc = split_pack(X0 + cell / TY, Y0 + cell % TY);
@@ -687,15 +723,15 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, in
             const unsigned pb = __float_as_uint(q2.y);
             if (pb == (unsigned)BASE_NONE) continue;
             const float4 q0 = M.m0[c], q1 = M.m1[c];
-            const float gx = q0.x, gy = q0.y, mass = q0.z, mvx = q0.w, mvy = q1.x;
-            const float s00 = q1.y, s01 = q1.z, s10 = q1.w, s11 = q2.x;
+            const float gx = q0.x, gy = q0.y, mass = q2.x;
+            const float2 mv = make_float2(q0.z, q0.w), S0 = make_float2(q1.x, q1.y), S1 = make_float2(q1.z, q1.w);
             if (pb == pbc) {
-                point_contributions_f32(A.Q.h, gx, gy, mass, mvx, mvy, s00, s01, s10, s11,
+                point_contributions_f32(A.Q.h, gx, gy, mass, mv, S0, S1,
                                         [&](int a, int b, float W, float dm, float tx, float ty) {
-                                            const int q = (a * 3 + b) * 3;
-                                            acc[q] += dm;
-                                            acc[q + 1] += W * tx;
-                                            acc[q + 2] += W * ty;
+                                            const int q = a * 3 + b;
+                                            accm[q] += dm;
+                                            accp[q].x += W * tx;
+                                            accp[q].y += W * ty;
                                         });
             } else {
                 moved++;
@@ -716,7 +752,7 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, in
                 }
                 const int lx = bx - RX0, ly = by - RY0;
                 if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
-                    point_contributions_f32(A.Q.h, gx, gy, mass, mvx, mvy, s00, s01, s10, s11,
+                    point_contributions_f32(A.Q.h, gx, gy, mass, mv, S0, S1,
                                             [&](int a, int b, float W, float dm, float tx, float ty) {
                                                 const int k = (lx + a) * RY + (ly + b);
                                                 atomicAdd(&s_odd[0][k], dm);
@@ -726,24 +762,26 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, in
                 } else {
                     if (FUSE && fused) *A.status = ICY_DRIFT_CODE;   // excluded by the margin test of the last launch
                     p2g_global_f32<AOS, S>(A.g, A.flags, A.tlist, A.tlist_n, A.inst, A.G.ntx, P.halo, A.Q.h, bx, by,
-                                        gx, gy, mass, mvx, mvy, s00, s01, s10, s11);
+                                        gx, gy, mass, mv, S0, S1);
                 }
             }
         }
     }
     sync();
-    float4 *part = reinterpret_cast<float4 *>(mom);   // [9 node offsets][TT cells], aliasing the moments
+    // [9 node offsets][TT cells] of (px, py, m, -), aliasing the moments
+    float4 *part = reinterpret_cast<float4 *>(mom);
     if (tid < TT) {
         const int cell = s_perm[tid];
 #pragma unroll
-        for (int q = 0; q < 9; q++) part[q * TT + cell] = make_float4(acc[3 * q], acc[3 * q + 1], acc[3 * q + 2], 0.f);
+        for (int q = 0; q < 9; q++) part[q * TT + cell] = make_float4(accp[q].x, accp[q].y, accm[q], 0.f);
     }
     sync();
     nxt.load();
     for (int k = tid; k < RN; k += NT) {
         const int i = k / RY, jj = k % RY;
         const int nx = i - RM, ny = jj - RM;
-        float m = 0.f, px = 0.f, py = 0.f;
+        float m = 0.f;
+        float2 pp = make_float2(0.f, 0.f);
 #pragma unroll
         for (int a = 0; a < 3; a++) {
             const int cx = nx - a;
@@ -753,11 +791,11 @@ __device__ __forceinline__ void p2g_cells_and_flush_f32(const AT &A, int tid, in
                 const int cy = ny - b;
                 if (cy < 0 || cy >= TY) continue;
                 const float4 v = part[(a * 3 + b) * TT + cx * TY + cy];
-                m += v.x;
-                px += v.y;
-                py += v.z;
+                pp = p_add(pp, make_float2(v.x, v.y));
+                m += v.z;
             }
         }
+        float px = pp.x, py = pp.y;
         m += s_odd[0][k]; px += s_odd[1][k]; py += s_odd[2][k];
         s_odd[0][k] = 0.f; s_odd[1][k] = 0.f; s_odd[2][k] = 0.f;
         if (m != 0.f || px != 0.f || py != 0.f) {
@@ -1035,9 +1073,9 @@ static __global__ void __launch_bounds__(TILE_THREADS_F32, TILE_CTAS_F32)
                     const float *c = reinterpret_cast<const float *>(A.st) + cold_vec(A.pitch, i);
                     const float4 v = *reinterpret_cast<const float4 *>(c);
                     const float4 b = *reinterpret_cast<const float4 *>(c + 128);
-                    s.vx = v.x;
-                    s.vy = v.y;
-                    s.B = {b.x, b.y, b.z, b.w};
+                    s.v = make_float2(v.x, v.y);
+                    s.b0 = make_float2(b.x, b.y);
+                    s.b1 = make_float2(b.z, b.w);
                 }
                 if (DO_P2G) p2g_moments_f32<BATCH>(P, A.Q, s, s_momf, j, A.status);
             }
@@ -1279,11 +1317,12 @@ static __global__ void k_split_from_hssoa(const double *__restrict__ chunk, long
     s.gx = g[0];
     s.gy = g[1];
     s.util = (unsigned)(unsigned long long)__double_as_longlong(L(0));
-    s.D = {(float)(L(8) - 1.0), (float)L(9), (float)L(10), (float)(L(11) - 1.0)};
+    s.d0 = make_float2((float)(L(8) - 1.0), (float)L(10));   // columns of Fe - I
+    s.d1 = make_float2((float)L(9), (float)(L(11) - 1.0));
     s.Jp = (float)L(3);
-    s.vx = (float)L(6);
-    s.vy = (float)L(7);
-    s.B = {(float)L(12), (float)L(13), (float)L(14), (float)L(15)};
+    s.v = make_float2((float)L(6), (float)L(7));
+    s.b0 = make_float2((float)L(12), (float)L(14));            // columns of Bp
+    s.b1 = make_float2((float)L(13), (float)L(15));
     s.ptr = (float)L(1);
     s.qtr = (float)L(2);
     store_point_f32(st, pitch, i, s, true, true);
@@ -1306,16 +1345,16 @@ static __global__ void k_split_to_hssoa(const unsigned *__restrict__ st, long pi
     W(0, __longlong_as_double((long long)s.util));
     W(4, ((double)s.bx + 1.0 + (double)s.gx) * h);
     W(5, ((double)s.by + 1.0 + (double)s.gy) * h);
-    W(8, 1.0 + (double)s.D.a00);
-    W(9, (double)s.D.a01);
-    W(10, (double)s.D.a10);
-    W(11, 1.0 + (double)s.D.a11);
+    W(8, 1.0 + (double)s.d0.x);
+    W(9, (double)s.d1.x);
+    W(10, (double)s.d0.y);
+    W(11, 1.0 + (double)s.d1.y);
     W(3, (double)s.Jp);
     W(6, (double)v.x);
     W(7, (double)v.y);
-    W(12, (double)bp.x);
-    W(13, (double)bp.y);
-    W(14, (double)bp.z);
+    W(12, (double)bp.x);   // Bp by columns: (b00, b10, b01, b11)
+    W(13, (double)bp.z);
+    W(14, (double)bp.y);
     W(15, (double)bp.w);
     W(1, (double)v.z);
     W(2, (double)v.w);
