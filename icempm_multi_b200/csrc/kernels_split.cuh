@@ -3,7 +3,9 @@
 // Device state, in blocks of 32 points (point i: block i / 32, lane i % 32),
 // `pitch` points of capacity (a multiple of 32), 17 words per point:
 //   hot part, read and written at every step, 288 words per block:
-//     words [0, 128)    one 16-byte vector per point: (base word, gx, gy, utility)
+//     words [0, 128)    one 16-byte vector per point: (base word, gx, gy, utility),
+//                       the utility word's bits 19-30 holding the point's
+//                       failure-surface table entry where the input left them clear
 //     words [128, 256)  one 16-byte vector per point: De = Fe - I by columns (d00, d10, d01, d11)
 //     words [256, 288)  Jp_inv per point
 //   cold part (from word 9 * pitch on), written on the last step of a call
@@ -108,6 +110,15 @@ __device__ __forceinline__ int grain_entry_f32(unsigned util)
 {
     const short g = (short)util;
     return g >= 0 ? GRAIN_TAB + (int)((unsigned)g % GRAIN_PERIOD) : grain_slot(g);
+}
+// Bits 19-29 of a point's utility word in the FP32 state hold its table entry
+// (cached at upload, with bit 30 set) where the input word leaves bits 19-31
+// clear; the download clears them again.
+constexpr unsigned GE_SHIFT = 19, GE_MASK = 0x7ffu, GE_CACHED = 1u << 30;
+static_assert(GRAIN_TAB_F32 <= (int)GE_MASK + 1, "table entries fit the cached field");
+__device__ __forceinline__ int grain_entry_cached(unsigned util)
+{
+    return (util & GE_CACHED) ? (int)((util >> GE_SHIFT) & GE_MASK) : grain_entry_f32(util);
 }
 
 // base word: 16 bits per axis, each offset by 32768
@@ -304,7 +315,7 @@ __device__ __forceinline__ bool g2p_update_f32(const PT &P, const SplitConsts &Q
         asm("sqrt.approx.f32 %0, %1;" : "=f"(sq) : "f"(d00 * d00 + d01 * d01));
         s.qtr = __fdividef(2.f * Q.mu, Je) * sq;   // sqrt(2) mu/J |dev|, |dev| = sqrt(2(d00^2+d01^2))
         if (!(s.util & (unsigned)kCrushed)) {
-            const float4 gc = __ldg(reinterpret_cast<const float4 *>(tab) + grain_entry_f32(s.util));
+            const float4 gc = __ldg(reinterpret_cast<const float4 *>(tab) + grain_entry_cached(s.util));
             const float pmin2 = gc.x, k = gc.y, msq = gc.z;
             bool crushed;
             if (s.ptr < 0.f) crushed = s.ptr < pmin2 || s.qtr > k * (s.ptr - pmin2);
@@ -1343,6 +1354,7 @@ static __global__ void k_split_from_hssoa(const double *__restrict__ chunk, long
     s.gx = g[0];
     s.gy = g[1];
     s.util = (unsigned)(unsigned long long)__double_as_longlong(L(0));
+    if ((s.util >> GE_SHIFT) == 0u) s.util |= GE_CACHED | ((unsigned)grain_entry_f32(s.util) << GE_SHIFT);
     s.d0 = make_float2((float)(L(8) - 1.0), (float)L(10));   // columns of Fe - I
     s.d1 = make_float2((float)L(9), (float)(L(11) - 1.0));
     s.Jp = (float)L(3);
@@ -1368,7 +1380,8 @@ static __global__ void k_split_to_hssoa(const unsigned *__restrict__ st, long pi
     const float *c = reinterpret_cast<const float *>(st) + cold_vec(pitch, i);
     const float4 v = *reinterpret_cast<const float4 *>(c);
     const float4 bp = *reinterpret_cast<const float4 *>(c + 128);
-    W(0, __longlong_as_double((long long)s.util));
+    const unsigned u = (s.util & GE_CACHED) ? s.util & ~(GE_CACHED | (GE_MASK << GE_SHIFT)) : s.util;
+    W(0, __longlong_as_double((long long)u));
     W(4, ((double)s.bx + 1.0 + (double)s.gx) * h);
     W(5, ((double)s.by + 1.0 + (double)s.gy) * h);
     W(8, 1.0 + (double)s.d0.x);

@@ -61,6 +61,35 @@ def test_split_roundtrip(built):
     assert np.allclose(out.vel[:, m], soa.vel[:, m], rtol=1e-7, atol=1e-7)
 
 
+def test_split_utility_words_beyond_the_flags(built):
+    """The FP32 state caches each point's failure-surface table entry in
+    bits 19-30 of its utility word when the uploaded word leaves bits 19-31
+    clear; a word that uses them keeps them, and its entry is looked up at
+    every step instead.  Both give the same steps (up to the order of the
+    atomic node sums, which differs from run to run), and every word comes
+    back as uploaded, apart from the crushed flag the steps set."""
+    from icempm_multi_b200.hssoa import STATUS_CRUSHED
+    p, soa = stress(seed=3)
+    high = soa.clone()
+    u = high.utility
+    u |= np.int64(1 << 24)
+    back, _, _ = run_split(p, high, 0)
+    assert np.array_equal(back.utility, high.utility)
+    a, _, _ = run_split(p, soa, 40)
+    b, _, _ = run_split(p, high, 40)
+    assert np.mean(a.crushed() != soa.crushed()) > 0.5   # the steps crushed points
+    keep = ~np.int64(STATUS_CRUSHED)
+    assert np.all(b.utility & np.int64(1 << 24))
+    assert np.array_equal(b.utility & keep & ~np.int64(1 << 24), soa.utility & keep)
+    assert np.array_equal(a.utility & keep, soa.utility & keep)
+    bu = b.utility
+    bu &= ~np.int64(1 << 24)
+    e = field_errors(b, a)
+    assert e["status"] <= 0.01, e
+    for k, v in TOL32.items():
+        assert e[k] <= v, (k, e)
+
+
 def displacement_errors(p, x0, a, b):
     """Error of run a against run b relative to b's displacement from the
     common start x0, and the largest position difference in cells."""
