@@ -4,8 +4,9 @@
 // `pitch` points of capacity (a multiple of 32), 17 words per point:
 //   hot part, read and written at every step, 288 words per block:
 //     words [0, 128)    one 16-byte vector per point: (base word, gx, gy, utility),
-//                       the utility word's bits 19-30 holding the point's
-//                       failure-surface table entry where the input left them clear
+//                       the utility word's bits 19-29 holding the point's
+//                       failure-surface table entry, marked by bit 30, where
+//                       the input left bits 19-31 clear
 //     words [128, 256)  one 16-byte vector per point: De = Fe - I by columns (d00, d10, d01, d11)
 //     words [256, 288)  Jp_inv per point
 //   cold part (from word 9 * pitch on), written on the last step of a call
