@@ -484,10 +484,13 @@ struct NextTileOps {
     __device__ __forceinline__ void load() const { l(); }
     __device__ __forceinline__ void store() const { st(); }
 };
+// `s_oddf` (or nullptr: always the full region): set when a point of the
+// chunk added to the drift buffer s_odd; without one the node phase walks only
+// the (TX + 2) x (TY + 2) nodes that cell sums reach and leaves s_odd alone.
 template <int NT, typename Sync, class Next = NoNextTile>
 __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, int tx, int ty, int cs, int ce,
                                                     const int *s_cs, double *mom, double (*s_odd)[RN],
-                                                    unsigned &touch, unsigned &moved, Sync &&sync,
+                                                    int *s_oddf, unsigned &touch, unsigned &moved, Sync &&sync,
                                                     Next &&nxt = NoNextTile{})
 {
     const StepParams &P = A.P;
@@ -524,6 +527,7 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
                 moved++;
                 const int lx = bx - RX0, ly = by - RY0;
                 if (lx >= 0 && lx + 2 < RX && ly >= 0 && ly + 2 < RY) {
+                    if (s_oddf) *s_oddf = 1;
                     point_contributions(P.h, fx, fy, mass, mvx, mvy, s00, s01, s10, s11,
                                         [&](int a, int b, double W, double dm, double tx, double ty) {
                                             const int k = (lx + a) * RY + (ly + b);
@@ -551,8 +555,19 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
     }
     sync();
     nxt.load();
-    for (int k = tid; k < RN; k += NT) {
-        const int i = k / RY, jj = k % RY;        // region coordinates
+    const bool odd = !s_oddf || *s_oddf != 0;
+    constexpr int CY = TY + 2;
+    const int kn = odd ? RN : (TX + 2) * CY;
+    for (int k = tid; k < kn; k += NT) {
+        int i, jj;                                 // region coordinates
+        if (odd) {
+            i = k / RY;
+            jj = k % RY;
+        } else {
+            i = RM + k / CY;
+            jj = RM + k % CY;
+        }
+        const int kk = i * RY + jj;
         const int nx = i - RM, ny = jj - RM;       // node relative to the tile's first base
         double m = 0, px = 0, py = 0;
 #pragma unroll
@@ -570,8 +585,10 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
                 py += ppy[q * TT + c];
             }
         }
-        m += s_odd[0][k]; px += s_odd[1][k]; py += s_odd[2][k];
-        s_odd[0][k] = 0; s_odd[1][k] = 0; s_odd[2][k] = 0;
+        if (odd) {
+            m += s_odd[0][kk]; px += s_odd[1][kk]; py += s_odd[2][kk];
+            s_odd[0][kk] = 0; s_odd[1][kk] = 0; s_odd[2][kk] = 0;
+        }
         if (m != 0.0 || px != 0.0 || py != 0.0) {
             const int gx = RX0 + i, gy = RY0 + jj;   // inside the grid: only valid bases scatter
             const long q = A.g.idx(gx, gy);
@@ -584,6 +601,7 @@ __device__ __forceinline__ void p2g_cells_and_flush(const TileArgs &A, int tid, 
     }
     nxt.store();
     sync();   // partials consumed before the buffer is refilled
+    if (s_oddf && tid == 0) *s_oddf = 0;   // the next chunk's cell phase sets it after a barrier
 }
 
 __device__ __forceinline__ void mark_node_tiles(const TileArgs &A, int tx, int ty, unsigned touch, int lane9)
@@ -647,6 +665,7 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_co
     __shared__ double s_odd[3][RN];    // contributions of points off their sorted cell
     __shared__ int s_cs[TT + 1];       // cell ranges of the tile
     __shared__ unsigned s_touch;
+    __shared__ int s_oddf;             // a point of the chunk used s_odd
     extern __shared__ double2 s_mom2[];   // moments | 27 x TT cell partials
     double *const s_mom = reinterpret_cast<double *>(s_mom2);
     const StepParams &P = A.P;
@@ -654,6 +673,7 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_co
     const int tid = threadIdx.x;
     unsigned moved = 0;
     for (int k = tid; k < RN; k += blockDim.x) { s_odd[0][k] = 0; s_odd[1][k] = 0; s_odd[2][k] = 0; }
+    if (tid == 0) s_oddf = 0;
     // the tile's prologue (cell ranges, staged node velocities) was done during
     // the previous tile's node phase
     bool staged = false;
@@ -778,11 +798,11 @@ static __global__ void __launch_bounds__(TILE_THREADS, 2) k_tile(const __grid_co
                         }
                     }
                 };
-                p2g_cells_and_flush<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_mom, s_odd, touch, moved,
+                p2g_cells_and_flush<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_mom, s_odd, &s_oddf, touch, moved,
                                                   [] { __syncthreads(); }, NextTileOps<decltype(ld), decltype(st)>{ld, st});
                 next_staged = true;
             } else if (DO_P2G) {
-                p2g_cells_and_flush<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_mom, s_odd, touch, moved,
+                p2g_cells_and_flush<TILE_THREADS>(A, tid, tx, ty, cs, ce, s_cs, s_mom, s_odd, &s_oddf, touch, moved,
                                                   [] { __syncthreads(); });
             }
         }
@@ -967,7 +987,8 @@ static __global__ void __launch_bounds__(PIPE_THREADS, 1) k_tile_pipe(const __gr
                 p2g_moments(P, s, S.mom, j, A.status);
             }
             csync();
-            p2g_cells_and_flush<PIPE_CONS>(A, tid, tx, ty, cs, ce, S.cs[st], S.mom, S.odd, touch, moved, csync);
+            p2g_cells_and_flush<PIPE_CONS>(A, tid, tx, ty, cs, ce, S.cs[st], S.mom, S.odd, nullptr, touch, moved,
+                                           csync);
             // the stage (lines, velocities, cell ranges) is no longer read: release it
             if (tid == 0) mbar_arrive(reinterpret_cast<uint64_t *>(&S.empty[st]));
         }
